@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark of the delta-SPH single-GPU step on the 3-D dam break at scale:
+dx = 0.005 m, 3,456,000 fluid + 765,468 wall particles (4,221,468), one step =
+predictor + corrector sub-step (single_gpu_sph_src/deltasph/main.cu:58-90).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  `value` is whole-job particle-steps/s with
+the state resident in HBM (CUDA-event time of K steps replayed from a CUDA
+graph, max over ranks); `e2e` is the same metric through the C ABI from
+pinned host buffers (upload, K steps with a per-step status read, download).
+With N > 1 (torchrun) every rank runs an independent replica of the case:
+the path does not shard (replicas only), so there is no collective on the
+data path; only the barrier and the max-over-ranks timing reduction.
+
+--impl reference times the reference solver's equations on the host cores
+(the CPU oracle, an OpenMP restatement of the reference's CUDA kernels; the
+reference has no CPU path of its own) and, beside it, the reference's own
+CUDA kernels compiled for sm_100a (key `reference_cuda`).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = ("dam break dx=0.005 m: water 0.6x0.6x1.2 m in a 1.6x0.6x1.2 m tank, 3,456,000 fluid + 765,468 "
+            "dummy-wall particles (3 layers), 500-step case, 1 step = predictor + corrector")
+BYTES_PER_PARTICLE_SEARCH = 188  # hash 20 + sort 16 + cell bounds 4 + reorder 148
+BYTES_PER_CELL_SEARCH = 8
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["config1", "config0"], default="config1")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample duration")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_case(name):
+    from zsph_b200 import cases
+    return cases.config1() if name == "config1" else cases.config0()
+
+
+# ---------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = False
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        import torch.distributed as dist
+        dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        sm, smmax = [], []
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smmax.append(float(r[2]))
+            except ValueError:
+                pass
+            for k, nm in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        load = [s for s in sm if smmax and s > 0.5 * max(smmax)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(smmax) if smmax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic(kernel_group: str):
+    """Per-launch DRAM bytes of a kernel group from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(kernel_group)
+
+
+# ---------------------------------------------------------------- CPU baseline
+def cpu_baseline(case, target_s: float) -> dict:
+    """The FP32 CPU oracle (OpenMP restatement of the reference's kernels) on
+    a bounded sample of the same workload: whole steps of the full case,
+    as many as fit in about target_s seconds (at least one)."""
+    import numpy as np
+    from oracle import pyoracle as po
+    threads = os.cpu_count() or 1
+    po.set_threads(threads)
+    o = po.Oracle(case.json, case.state, np.float32)
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter()
+    steps, dt = 1, t1 - t0
+    while dt < target_s and steps < 3:
+        s0 = time.perf_counter()
+        o.step(1)
+        dt += time.perf_counter() - s0
+        steps += 1
+    return {"value": case.n * steps / dt, "unit": "particle-steps/s", "cores": po.max_threads(), "kind": "port",
+            "sample": f"{steps} full step(s) of the {case.n:,}-particle case (FP32 CPU oracle, OpenMP, "
+                      f"{dt:.1f} s)"}
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, dist: Dist):
+    import ctypes
+    import numpy as np
+    import torch
+    import zsph_b200 as z
+
+    dev = dist.local if torch.cuda.device_count() > 1 else 0
+    torch.cuda.set_device(dev)
+    case = make_case(args.workload)
+    cp, gp = z.params_from_json(case.json)
+    n, G = case.n, cp.grid_num
+    sol = z.Solver(gp, G)
+    sol.upload(case.state)
+    stream = torch.cuda.Stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    K, W = args.steps, args.warmup
+
+    # warm-up (captures the CUDA graph), then K steps timed with CUDA events
+    with torch.cuda.stream(stream):
+        sol.run(W, sptr)
+    torch.cuda.synchronize()
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(dev)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sol.run(K, sptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    dist.barrier()
+    ms_local = e0.elapsed_time(e1)
+    ms = dist.max(ms_local)
+    flags = sol.status()
+    if flags & z.FLAG_NAN:
+        raise SystemExit("non-finite state during the timed steps")
+    value = dist.world * n * K / (ms / 1e3)
+
+    # per-launch durations (3 profiled steps, events on the launching stream)
+    prof = [sol.step_profiled(sptr) for _ in range(3)]
+    per = {}
+    for step in prof:
+        for name, t in step:
+            per.setdefault(name, []).append(t)
+    launches = len(prof[0])
+    step_ms_prof = sum(t for _, t in prof[-1])
+    kern = {k: {"launches_per_step": len(v) // 3, "ms_per_step": sum(v) / 3,
+                "share": (sum(v) / 3) / step_ms_prof} for k, v in per.items()}
+    search_names = ("hash_count", "scan_reduce", "scan_cells", "scatter", "sort_big_cells", "rank_gather")
+    search_ms_sub = sum(kern[k]["ms_per_step"] for k in search_names if k in kern) / 2  # per sub-step
+    search_bytes = BYTES_PER_PARTICLE_SEARCH * n + BYTES_PER_CELL_SEARCH * G
+    peaks = measured_peaks()
+    ach = search_bytes / (search_ms_sub / 1e3) / 1e9
+    dom = max(kern.items(), key=lambda kv: kv[1]["ms_per_step"])
+    nb_b, nb_g = sol.neighbor_counts("new")
+    pairs_gov = float(np.mean(nb_g[nb_g >= 0]))
+    roofline = {"bound": "hbm", "kernel": "search+sort group: " + ", ".join(search_names),
+                "algorithmic_bytes": search_bytes, "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": ach / peaks["hbm_gbs"] if peaks["hbm_gbs"] else None,
+                "peak_source": f"{peaks['source']} hbm_gbs (copy test)",
+                "traffic": ncu_traffic("search_group")}
+    gov_ms = kern.get("governing", {}).get("ms_per_step", 0) / 2
+    dominant = {"kernel": dom[0], "ms_per_step": dom[1]["ms_per_step"], "share": dom[1]["share"],
+                "bound": "fp32 pair arithmetic / latency (not hbm, no tensor-core work on the pair path)",
+                "interacting_pairs_per_particle": pairs_gov,
+                "governing_pair_evals_per_s": pairs_gov * n / (gov_ms / 1e3) if gov_ms else None,
+                "traffic": ncu_traffic(dom[0])}
+
+    # end to end through the C ABI from pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    hp = {k: pin(getattr(case.state, k)) for k in ("pos", "vel", "rhop", "type", "table")}
+    hout = {k: torch.empty_like(v).pin_memory() for k, v in hp.items()}
+    ptr = lambda t: ctypes.c_void_p(t.data_ptr())
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    z.check(z.lib.zsph_cpu_to_gpu(ctypes.byref(sol.old), ctypes.byref(sol.tmp), ptr(hp["pos"]), ptr(hp["vel"]),
+                                  ptr(hp["rhop"]), ptr(hp["type"]), ptr(hp["table"]), None, n, sptr))
+    flag = ctypes.c_int(0)
+    for _ in range(K):
+        sol.run(1, sptr)
+        z.check(z.lib.zsph_status(sol.h, ctypes.byref(flag), 0), sol.h)
+    z.check(z.lib.zsph_gpu_to_cpu(ctypes.byref(sol.old), ctypes.byref(sol.tmp), ptr(hout["pos"]), ptr(hout["vel"]),
+                                  ptr(hout["rhop"]), ptr(hout["type"]), ptr(hout["table"]), None, None, n, sptr))
+    t_e2e = dist.max(time.perf_counter() - t0)
+    h2d = 40 * n  # pos 12, vel 12, rhop 8, type 4, table 4 (acc_drhodt is zero-filled on the device)
+    d2h = 40 * n + 4 * K
+    e2e = {"value": dist.world * n * K / t_e2e, "unit": "particle-steps/s",
+           "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+           "what": "zsph_cpu_to_gpu of the case from pinned host memory, K x (zsph_run 1 step + zsph_status "
+                   "read of the 4-byte device status word), zsph_gpu_to_cpu of pos/vel/rhop/type/table; "
+                   "host wall clock, max over ranks"}
+
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(case, args.cpu_seconds)
+
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": dist.world,
+        "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (lattice dam break, no randomness)",
+        "config": {"workload": WORKLOAD, "ptc_num": n, "fluid": case.n_fluid, "wall": case.n_wall,
+                   "grid_num": G, "dt": float(cp.dt), "parallelism": f"replicas x{dist.world}",
+                   "l2": "inputs larger than L2 (particle state 0.76 GB + scratch per step)",
+                   "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
+        "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
+        "roofline": roofline, "dominant_kernel": dominant, "kernels": kern, "cpu_baseline": cpu,
+        "status_flags": flags,
+    }
+    sol.close()
+    return line
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args, dist: Dist):
+    """Reference's equations on the host cores (CPU oracle = the port: the
+    reference has no CPU implementation) plus the reference's own CUDA build."""
+    if dist.rank != 0:
+        return None
+    from oracle import pyoracle as po
+    case = make_case(args.workload)
+    cpu = cpu_baseline(case, max(args.cpu_seconds, 30.0))
+    line = {"impl": "reference", "metric": "particle-steps/s", "value": cpu["value"], "unit": "particle-steps/s",
+            "n_gpus": 1, "steps": 0, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (lattice dam break, no randomness)",
+            "config": {"workload": WORKLOAD, "ptc_num": case.n},
+            "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "particle-steps/s",
+                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    line["steps"] = int(cpu["sample"].split()[0])
+    if po.ref_available():
+        try:
+            import torch
+            if torch.cuda.is_available():
+                _, _, ms = po.ref_run(case.json, case.state, args.steps, warmup=args.warmup)
+                line["reference_cuda"] = {"value": case.n / (ms / 1e3), "unit": "particle-steps/s",
+                                          "ms_per_step": ms, "steps": args.steps, "warmup": args.warmup,
+                                          "what": "the reference's own hash/sort/boundary/governing/time "
+                                                  "integration kernels (unmodified sources, -maxrregcount 64, "
+                                                  "sm_100a), Thrust sort, launch order of main.cu:63-88, CUDA "
+                                                  "events"}
+        except Exception as e:  # keep the CPU line even if the GPU leg fails
+            line["reference_cuda"] = {"unavailable": str(e)[:200]}
+    else:
+        line["reference_cuda"] = {"unavailable": "oracle/_ref/libzsph_ref.so not built"}
+    return line
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    try:
+        line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)
+        if dist.rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/*
+ * zsph.h -- C ABI of the B200-native delta-SPH single-GPU step.
+ *
+ * The entry points replace the reference solver's single-GPU hot path
+ * (ZSPH, single_gpu_sph_src/) for a caller that drives it the way
+ * single_gpu_sph_src/deltasph/main.cu does.  All structs are plain C; every
+ * device pointer is caller-owned; every call returns a ZSPH_* status and
+ * never exits the process.  `stream` is a cudaStream_t passed as void*
+ * (NULL = the legacy default stream).
+ *
+ * Particle layout (unchanged from the reference, data_structure.cuh:158-182):
+ * pos, vel, tmp_pos, tmp_vel hold 3 floats per particle (float3), rhop and
+ * tmp_rhop 2 floats (float2: density, pressure), acc_drhodt and
+ * dofv_grandrho 4 floats (float4), type/table/index/hash one int, and
+ * grid_start/grid_end one int per grid cell.  Particle type 1 is fluid,
+ * any other type a dummy wall, 100 a particle that left the grid.
+ */
+#ifndef ZSPH_H
+#define ZSPH_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  ZSPH_OK = 0,
+  ZSPH_EINVAL = 1,   /* bad argument, dt > dt_max, size mismatch, unsupported grid factor */
+  ZSPH_ECUDA = 2,    /* a CUDA runtime call failed; see zsph_last_error */
+  ZSPH_ENAN = 3,     /* a non-finite acceleration or density was produced */
+  ZSPH_ETIMEOUT = 4, /* a bounded device-side wait gave up */
+  ZSPH_EIO = 5,      /* file or JSON error */
+  ZSPH_ENOMEM = 6    /* device allocation failed */
+};
+
+/* Bits of the device status word (zsph_status). */
+enum {
+  ZSPH_FLAG_NAN = 1,         /* non-finite acc_drhodt or density */
+  ZSPH_FLAG_KILLED = 2,      /* a particle left the grid and became type 100 */
+  ZSPH_FLAG_NB_OVERFLOW = 4, /* a neighbour list overflowed (handled, slower path) */
+  ZSPH_FLAG_BAD_KEY = 8      /* zsph_sort_index got a hash outside [0, grid_num) */
+};
+
+/* cpu_json_t (single_gpu_sph_src/header/data_structure.cuh:6-51); the three
+ * std::string members become fixed char arrays. */
+typedef struct {
+  float g, m, rho0, dx, h_factor, r_factor, eta_factor, cs_factor, delta, alpha;
+  float xmin, xmax, ymin, ymax, zmin, zmax, grid_layer_factor, grid_size_factor;
+  float dt;
+  int start_step, current_step, end_step, output_step;
+  int ptc_num, water_ptc_num, air_ptc_num, wall_ptc_num, rigid_ptc_num;
+  int thread_num, gpu_id;
+  char input_path[256], output_path[256], git_hash[64];
+} zsph_json_t;
+
+/* cpu_param_t (data_structure.cuh:53-105), same fields and order. */
+typedef struct {
+  float g, m, rho0, dx, h, r, eta, cs, adh, delta, alpha;
+  float dt;
+  int start_step, current_step, end_step, output_step;
+  float xmin, xmax, ymin, ymax, zmin, zmax;
+  int grid_factor;
+  float grid_size;
+  float grid_xmin, grid_ymin, grid_zmin, grid_xmax, grid_ymax, grid_zmax;
+  int grid_xdim, grid_ydim, grid_zdim, grid_num, grid_hash_min, grid_hash_max;
+  int ptc_num, water_ptc_num, air_ptc_num, wall_ptc_num, rigid_ptc_num;
+  int thread_num, gpu_id;
+  char input_path[256], output_path[256], git_hash[64];
+} zsph_cpu_param_t;
+
+/* gpu_param_t (data_structure.cuh:107-134), field for field. */
+typedef struct {
+  float half_dt, h, g, m, rho0, adh, h2, eta2, cs2, alpha, delta_h_cs, h_cs_rho_m;
+  float grid_size;
+  int grid_factor;
+  float grid_xmin, grid_ymin, grid_zmin;
+  int grid_xdim, grid_ydim, grid_zdim, grid_hash_min, grid_hash_max;
+  int ptc_num;
+} zsph_gpu_param_t;
+
+/* gpu_ptc_t (data_structure.cuh:158-168): same layout (all members are pointers). */
+typedef struct {
+  float *pos, *vel, *rhop, *tmp_pos, *tmp_vel, *tmp_rhop;
+  int *type, *table;
+} zsph_ptc_t;
+
+/* gpu_tmp_t (data_structure.cuh:170-182): same layout. */
+typedef struct {
+  float *acc_drhodt, *dofv_grandrho, *dofv;
+  int *index, *hash, *grid_start, *grid_end;
+} zsph_tmp_t;
+
+typedef struct zsph_handle zsph_handle_t;
+
+/* ---- host-side case set-up -------------------------------------------- */
+
+/* read_json (single_gpu_sph_src/io/read_json.cu:5-51): reads the 33
+ * required keys; a missing or mistyped key is ZSPH_EIO with its name in err. */
+int zsph_read_json(const char* path, zsph_json_t* out, char* err, int errlen);
+
+/* set_cpu_param (single_gpu_sph_src/lib/init.cu:153-219), including the
+ * check_dt call of init.cu:218: returns ZSPH_EINVAL when dt > dt_max
+ * (the reference exits, check.cu:9-17). */
+int zsph_set_cpu_param(zsph_cpu_param_t* param, const zsph_json_t* jdata);
+
+/* set_gpu_param (single_gpu_sph_src/lib/init.cu:221-251). */
+int zsph_set_gpu_param(zsph_gpu_param_t* gparam, const zsph_cpu_param_t* cparam);
+
+/* check_dt (single_gpu_sph_src/lib/check.cu:3-18): ZSPH_OK when
+ * dt <= 0.25*h/sqrt(-g*(zmax-zmin)), else ZSPH_EINVAL; dt_max may be NULL. */
+int zsph_check_dt(const zsph_cpu_param_t* param, float* dt_max);
+
+/* ---- device buffers ----------------------------------------------------- */
+
+/* alloc_gpu_ptc_data / delete_gpu_ptc_data (lib/init.cu:38-80). */
+int zsph_alloc_ptc(zsph_ptc_t* ptc, int ptc_num);
+int zsph_free_ptc(zsph_ptc_t* ptc);
+/* alloc_gpu_tmp_data / delete_gpu_tmp_data (lib/init.cu:82-134); zero-filled. */
+int zsph_alloc_tmp(zsph_tmp_t* tmp, int ptc_num, int grid_num);
+int zsph_free_tmp(zsph_tmp_t* tmp);
+/* cpu_to_gpu (lib/init.cu:136-151): host pos/vel/rhop/type/table/acc_drhodt
+ * (acc_drhodt may be NULL: zero-filled) into the device buffers. */
+int zsph_cpu_to_gpu(const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, const float* pos, const float* vel,
+                    const float* rhop, const int* type, const int* table, const float* acc_drhodt,
+                    int ptc_num, void* stream);
+/* gpu_to_cpu (lib/gmemcpy.cu:3-36): device buffers to host arrays; any
+ * NULL host pointer is skipped. */
+int zsph_gpu_to_cpu(const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, float* pos, float* vel, float* rhop,
+                    int* type, int* table, float* acc_drhodt, int* hash, int ptc_num, void* stream);
+
+/* ---- solver handle -------------------------------------------------------- */
+
+/* Creates a solver for one case.  Owns only its scratch (counting-sort
+ * buckets, packed particle shadows, neighbour lists); allocates it here and
+ * never during a step.  grid_num = grid_xdim*grid_ydim*grid_zdim
+ * (cpu_param_t::grid_num).  Binds to the current CUDA device. */
+int zsph_create(const zsph_gpu_param_t* gparam, int grid_num, zsph_handle_t** out);
+void zsph_destroy(zsph_handle_t* h);
+/* Replaces the constants (dt and physics) of an existing handle; the grid
+ * and particle count must not change. */
+int zsph_set_params(zsph_handle_t* h, const zsph_gpu_param_t* gparam);
+
+/* cuda_ptc_hash (single_gpu_sph_src/lib/hash.cu:3-26): cell hash of every
+ * particle into tmp->hash, identity into tmp->index, out-of-grid particles
+ * become type 100 at the grid origin. */
+int zsph_hash(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream);
+/* cuda_sort_index (single_gpu_sph_src/lib/sort.cu:3-6): stable ascending
+ * sort of tmp->hash carrying tmp->index.  Keys must lie in [0, grid_num). */
+int zsph_sort_index(zsph_handle_t* h, const zsph_tmp_t* tmp, void* stream);
+/* cuda_sort_data (single_gpu_sph_src/lib/sort.cu:8-84): grid_start/grid_end
+ * from the sorted keys (with the reference's end-of-array rules) and the
+ * gather of all eight particle arrays from old_ into new_. */
+int zsph_sort_data(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+                   void* stream);
+/* hash + sort_index + sort_data in one fused pipeline (bit-identical result). */
+int zsph_neighbor_search(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_,
+                         const zsph_tmp_t* tmp, void* stream);
+/* cuda_boundary_ns (single_gpu_sph_src/equation/delta_ns.cu:5-177): wall
+ * pressure, renormalisation matrix, div(v) and renormalised grad(rho) into
+ * tmp->dofv_grandrho; new wall (rho, p) into ptc->rhop.  Wall densities are
+ * extrapolated before any neighbour reads them (deterministic). */
+int zsph_boundary(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream);
+/* cuda_govering_ns (delta_ns.cu:179-267): acc and drho/dt into tmp->acc_drhodt. */
+int zsph_governing(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream);
+/* cuda_prediction / cuda_correction (single_gpu_sph_src/lib/time_int.cu:3-92). */
+int zsph_prediction(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream);
+int zsph_correction(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream);
+
+/* One full time step (single_gpu_sph_src/deltasph/main.cu:63-88): predictor
+ * sub-step and corrector sub-step; the result is in old_ (sorted by the
+ * corrector's neighbour search), as in the reference.  new_ is scratch. */
+int zsph_step(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+              void* stream);
+/* nsteps calls of zsph_step, replayed from one captured CUDA graph. */
+int zsph_run(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+             int nsteps, void* stream);
+
+/* Per-particle neighbour counts of a sorted state (after a neighbour
+ * search): candidates that pass the reference's distance test
+ * (delta_ns.cu:67-68) in the boundary kernel's stencil rows (y < gf,
+ * delta_ns.cu:37) and in the governing kernel's rows (y <= gf, :206).
+ * Outputs are device int arrays of ptc_num entries (either may be NULL). */
+int zsph_neighbor_counts(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int* nb_boundary,
+                         int* nb_governing, void* stream);
+/* One zsph_step with a CUDA event after every kernel launch: writes each
+ * launch's duration in ms into ms[0..cap), their number into *count and the
+ * comma-separated kernel names into names (may be NULL). */
+int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+                       void* stream, float* ms, int cap, int* count, char* names, int names_len);
+/* Number of kernel launches one zsph_step issues. */
+int zsph_launches_per_step(zsph_handle_t* h);
+
+/* Synchronises the handle's last stream and returns the accumulated device
+ * status bits (ZSPH_FLAG_*), clearing them when clear != 0.  Returns
+ * ZSPH_ENAN if the NAN bit is set, else ZSPH_OK (or ZSPH_ECUDA). */
+int zsph_status(zsph_handle_t* h, int* flags, int clear);
+/* Copies the last error message of the handle (or of the library when h is
+ * NULL) into buf; returns its length. */
+int zsph_last_error(zsph_handle_t* h, char* buf, int len);
+/* Plain device-memory helpers for callers without their own CUDA runtime
+ * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,
+ * deltasph/main.cu:41-45).  kind: 1 host->device, 2 device->host,
+ * 3 device->device; the copy is complete on return. */
+int zsph_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream);
+int zsph_device_malloc(void** p, size_t bytes);
+int zsph_device_free(void* p);
+int zsph_device_synchronize(void);
+
+/* Library version string. */
+const char* zsph_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZSPH_H */

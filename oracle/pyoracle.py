@@ -1,0 +1,250 @@
+"""ctypes wrapper over the CPU oracle (liboracle.so) and the reference-build
+checker (_ref/libzsph_ref.so).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libzsph_ref.so")
+
+WALLS_FIRST, WALLS_OLD = 0, 1
+_F, _I, _VP = ctypes.c_float, ctypes.c_int, ctypes.c_void_p
+
+
+class OCase(ctypes.Structure):
+    _fields_ = [(n, _F) for n in ("g", "rho0", "dx", "h_factor", "r_factor", "eta_factor", "cs_factor", "delta",
+                                  "alpha", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax", "grid_layer_factor",
+                                  "grid_size_factor", "dt")] + [("ptc_num", _I)]
+
+
+class OParams(ctypes.Structure):
+    _fields_ = [(n, _F) for n in ("half_dt", "h", "g", "m", "rho0", "adh", "h2", "eta2", "cs2", "alpha",
+                                  "delta_h_cs", "h_cs_rho_m", "grid_size")] + \
+               [("grid_factor", _I)] + [(n, _F) for n in ("grid_xmin", "grid_ymin", "grid_zmin")] + \
+               [(n, _I) for n in ("grid_xdim", "grid_ydim", "grid_zdim", "grid_hash_min", "grid_hash_max",
+                                  "ptc_num", "grid_num")] + \
+               [(n, _F) for n in ("dt", "dt_max", "cs", "eta", "r")]
+
+
+class OState(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel", "tmp_rhop", "type", "table")]
+
+
+class OTmp(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("acc_drhodt", "dofv_grandrho", "index", "hash", "grid_start", "grid_end")]
+
+
+def build_oracle() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build_oracle()
+        _lib = ctypes.CDLL(ORACLE_SO)
+        _lib.oracle_params.argtypes = [ctypes.POINTER(OCase), ctypes.POINTER(OParams)]
+        _lib.oracle_params.restype = _I
+        _lib.oracle_sizeof_params.restype = _I
+        _lib.oracle_set_threads.argtypes = [_I]
+        _lib.oracle_max_threads.restype = _I
+        assert _lib.oracle_sizeof_params() == ctypes.sizeof(OParams), "oracle Params layout mismatch"
+    return _lib
+
+
+def case_of(json) -> OCase:
+    """OCase from a zsph_b200.JsonCase (or any object with the same fields)."""
+    c = OCase()
+    for name, _ in OCase._fields_:
+        setattr(c, name, getattr(json, name))
+    return c
+
+
+def params(json) -> tuple[int, OParams]:
+    p = OParams()
+    rc = lib().oracle_params(ctypes.byref(case_of(json)), ctypes.byref(p))
+    return rc, p
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_VP)
+
+
+class Oracle:
+    """One oracle run (FP32 or FP64) on host arrays in the reference layout."""
+
+    def __init__(self, json, state, dtype=np.float32):
+        self.dtype = np.dtype(dtype)
+        self.suf = "f32" if self.dtype == np.float32 else "f64"
+        rc, self.p = params(json)
+        if rc != 0:
+            raise ValueError("dt > dt_max")
+        n, G = self.p.ptc_num, self.p.grid_num
+        cv = lambda a, shape: (np.zeros(shape, self.dtype) if a is None else np.ascontiguousarray(a, self.dtype))
+        self.old = dict(pos=cv(state.pos, (n, 3)), vel=cv(state.vel, (n, 3)), rhop=cv(state.rhop, (n, 2)),
+                        tmp_pos=cv(state.tmp_pos, (n, 3)), tmp_vel=cv(state.tmp_vel, (n, 3)),
+                        tmp_rhop=cv(state.tmp_rhop, (n, 2)),
+                        type=np.ascontiguousarray(state.type, np.int32).copy(),
+                        table=np.ascontiguousarray(state.table, np.int32).copy())
+        self.new = {k: np.zeros_like(v) for k, v in self.old.items()}
+        self.tmp = dict(acc_drhodt=np.zeros((n, 4), self.dtype), dofv_grandrho=np.zeros((n, 4), self.dtype),
+                        index=np.zeros(n, np.int32), hash=np.zeros(n, np.int32),
+                        grid_start=np.zeros(G, np.int32), grid_end=np.zeros(G, np.int32))
+        self._mk()
+
+    def _mk(self):
+        self._so = OState(*[_p(self.old[k]) for k, _ in OState._fields_])
+        self._sn = OState(*[_p(self.new[k]) for k, _ in OState._fields_])
+        self._t = OTmp(*[_p(self.tmp[k]) for k, _ in OTmp._fields_])
+
+    def _s(self, which):
+        return self._so if which == "old" else self._sn
+
+    def _fn(self, name):
+        f = getattr(lib(), f"oracle_{name}_{self.suf}")
+        f.restype = None
+        return f
+
+    def hash(self, which="old"):
+        self._fn("hash")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t))
+
+    def sort_index(self):
+        self._fn("sort_index")(ctypes.byref(self.p), ctypes.byref(self._t))
+
+    def sort_data(self, src="old", dst="new"):
+        self._fn("sort_data")(ctypes.byref(self.p), ctypes.byref(self._s(src)), ctypes.byref(self._s(dst)),
+                              ctypes.byref(self._t))
+
+    def search(self, src="old", dst="new"):
+        self.hash(src)
+        self.sort_index()
+        self.sort_data(src, dst)
+
+    def boundary(self, which="new", wall_mode=WALLS_FIRST):
+        self._fn("boundary")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
+                             _I(wall_mode))
+
+    def governing(self, which="new"):
+        self._fn("governing")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t))
+
+    def prediction(self, which="new"):
+        self._fn("prediction")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t))
+
+    def correction(self, which="old"):
+        self._fn("correction")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t))
+
+    def step(self, nsteps=1, wall_mode=WALLS_FIRST):
+        self._fn("step")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
+                         ctypes.byref(self._t), _I(nsteps), _I(wall_mode))
+
+    def neighbor_count(self, which="new", stencil="governing") -> np.ndarray:
+        out = np.zeros(self.p.ptc_num, np.int32)
+        ylast = self.p.grid_factor if stencil == "governing" else self.p.grid_factor - 1
+        self._fn("neighbor_count")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
+                                   _I(ylast), _p(out))
+        return out
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().oracle_max_threads())
+
+
+# ---- the reference's own CUDA kernels (checker build in _ref/) ---------------
+
+class RState(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel", "tmp_rhop", "type", "table")]
+
+
+class RTmp(ctypes.Structure):
+    _fields_ = [(n, _VP) for n in ("acc_drhodt", "dofv_grandrho", "index", "hash", "grid_start", "grid_end",
+                                   "nb_boundary", "nb_governing")]
+
+
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        _ref = ctypes.CDLL(REF_SO)
+        _ref.ref_substep.restype = _I
+        _ref.ref_run.restype = _I
+        _ref.ref_params.restype = _I
+        _ref.ref_last_error.restype = ctypes.c_char_p
+    return _ref
+
+
+def ref_params(json):
+    from zsph_b200 import GpuParam  # same field layout as the reference's gpu_param_t
+    gp = GpuParam()
+    G = _I(0)
+    ref_lib().ref_params(ctypes.byref(case_of(json)), ctypes.byref(gp), ctypes.byref(G))
+    return gp, G.value
+
+
+def _rstate(st, n):
+    f = lambda a, s: np.ascontiguousarray(a if a is not None else np.zeros(s, np.float32), np.float32)
+    arrs = dict(pos=f(st.pos, (n, 3)), vel=f(st.vel, (n, 3)), rhop=f(st.rhop, (n, 2)),
+                tmp_pos=f(st.tmp_pos, (n, 3)), tmp_vel=f(st.tmp_vel, (n, 3)), tmp_rhop=f(st.tmp_rhop, (n, 2)),
+                type=np.ascontiguousarray(st.type, np.int32), table=np.ascontiguousarray(st.table, np.int32))
+    return arrs, RState(*[_p(arrs[k]) for k, _ in RState._fields_])
+
+
+def _rout(n, G):
+    out = dict(pos=np.zeros((n, 3), np.float32), vel=np.zeros((n, 3), np.float32), rhop=np.zeros((n, 2), np.float32),
+               tmp_pos=np.zeros((n, 3), np.float32), tmp_vel=np.zeros((n, 3), np.float32),
+               tmp_rhop=np.zeros((n, 2), np.float32), type=np.zeros(n, np.int32), table=np.zeros(n, np.int32))
+    tmp = dict(acc_drhodt=np.zeros((n, 4), np.float32), dofv_grandrho=np.zeros((n, 4), np.float32),
+               index=np.zeros(n, np.int32), hash=np.zeros(n, np.int32), grid_start=np.zeros(G, np.int32),
+               grid_end=np.zeros(G, np.int32), nb_boundary=np.zeros(n, np.int32),
+               nb_governing=np.zeros(n, np.int32))
+    return out, tmp, RState(*[_p(out[k]) for k, _ in RState._fields_]), RTmp(*[_p(tmp[k]) for k, _ in RTmp._fields_])
+
+
+def ref_substep(json, state, stage: int):
+    """Runs the reference's kernels of one predictor sub-step up to `stage`
+    (1 hash, 2 sort_index, 3 sort_data, 4 boundary, 5 governing, 6 prediction)."""
+    _, G = ref_params(json)
+    n = int(json.ptc_num)
+    arrs, rin = _rstate(state, n)
+    out, tmp, rout, rtmp = _rout(n, G)
+    c = case_of(json)
+    rc = ref_lib().ref_substep(ctypes.byref(c), ctypes.byref(rin), _I(stage), ctypes.byref(rout), ctypes.byref(rtmp))
+    if rc:
+        raise RuntimeError(ref_lib().ref_last_error().decode())
+    return out, tmp
+
+
+def ref_run(json, state, nsteps: int, warmup: int = 0):
+    """Runs `warmup + nsteps` full reference steps; returns (OLD state, tmp, ms/step of the last nsteps)."""
+    _, G = ref_params(json)
+    n = int(json.ptc_num)
+    arrs, rin = _rstate(state, n)
+    out, tmp, rout, rtmp = _rout(n, G)
+    ms = ctypes.c_float(0.0)
+    rc = ref_lib().ref_run(ctypes.byref(case_of(json)), ctypes.byref(rin), _I(warmup), _I(nsteps), ctypes.byref(rout),
+                           ctypes.byref(rtmp), ctypes.byref(ms))
+    if rc:
+        raise RuntimeError(ref_lib().ref_last_error().decode())
+    return out, tmp, float(ms.value)

@@ -1,0 +1,48 @@
+"""Shared helpers for the parity tests: numpy restatements used as
+independent cross-checks, case builders and error norms."""
+from __future__ import annotations
+
+import numpy as np
+
+
+def cell_bounds_closed_form(sorted_keys: np.ndarray, G: int, prev_start=None, prev_end=None):
+    """Cell bounds the reference's cuda_sort_data writes (single_gpu_sph_src/
+    lib/sort.cu:30-60) for sorted keys, computed from counts: with lb(c) the
+    number of keys below c, start = min(lb(c), N-1), end = min(lb(c+1), N-1),
+    except that a singleton last key leaves end[c >= k] and start[c > k]
+    untouched."""
+    n = len(sorted_keys)
+    start = np.zeros(G, np.int32) if prev_start is None else prev_start.copy()
+    end = np.zeros(G, np.int32) if prev_end is None else prev_end.copy()
+    if n == 0:
+        return start, end
+    cnt = np.bincount(sorted_keys, minlength=G)
+    lb = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int64)
+    klast = int(sorted_keys[-1])
+    single = cnt[klast] == 1
+    c = np.arange(G)
+    ws = ~(single & (c > klast))
+    we = ~(single & (c >= klast))
+    start[ws] = np.minimum(lb[:-1], n - 1)[ws]
+    end[we] = np.minimum(lb[1:], n - 1)[we]
+    return start, end
+
+
+def stable_sort_keys(keys: np.ndarray):
+    order = np.argsort(keys, kind="stable")
+    return keys[order], order.astype(np.int32)
+
+
+def err_norms(a: np.ndarray, b: np.ndarray) -> tuple[float, float]:
+    d = np.abs(np.asarray(a, np.float64) - np.asarray(b, np.float64))
+    return float(d.max()) if d.size else 0.0, float(np.sqrt((d * d).mean())) if d.size else 0.0
+
+
+def by_id(state, table=None):
+    """Particles re-indexed by identity: the reference keeps table[t] + t equal
+    to the particle's original index when the input table is zero
+    (single_gpu_sph_src/lib/sort.cu:82)."""
+    tab = state["table"] if isinstance(state, dict) else state.table
+    ids = tab + np.arange(len(tab), dtype=np.int32)
+    order = np.argsort(ids)
+    return order, ids

@@ -1,0 +1,139 @@
+"""GPU parity of the neighbour search (hash, stable sort, cell bounds,
+reorder) and of the neighbour counts: bit-exact against the FP32 oracle,
+through the C ABI, on lattices, random clouds and edge cases."""
+import numpy as np
+import pytest
+
+import zsph_b200 as z
+from oracle import pyoracle as po
+from zsph_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    return {
+        "small_dam": lambda: cases.small(0.04),
+        "config0_dam": cases.config0,
+        "cloud_killed": lambda: cases.random_cloud(5000, 1, kill_frac=0.02),
+        "cloud_crowded_cell0": lambda: cases.random_cloud(6000, 3, kill_frac=0.3),  # >256 in cell 0
+        "cloud_257": lambda: cases.random_cloud(257, 4),
+        "cloud_1": lambda: cases.random_cloud(1, 5),
+        "cloud_2": lambda: cases.random_cloud(2, 6),
+    }
+
+
+def _oracle_search(c):
+    o = po.Oracle(c.json, c.state, np.float32)
+    o.search()
+    return o
+
+
+def _assert_same(sol, o, tag=""):
+    tmp = sol.download_tmp()
+    for k in ("hash", "index", "grid_start", "grid_end"):
+        assert np.array_equal(tmp[k], o.tmp[k]), f"{tag}{k}"
+    new = sol.download("new")
+    for k in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel", "tmp_rhop", "type", "table"):
+        assert np.array_equal(getattr(new, k), o.new[k].reshape(getattr(new, k).shape)), f"{tag}new.{k}"
+    old = sol.download("old")  # out-of-grid particles are killed in place in the source buffer
+    for k in ("pos", "vel", "rhop", "type"):
+        assert np.array_equal(getattr(old, k), o.old[k].reshape(getattr(old, k).shape)), f"{tag}old.{k}"
+
+
+@pytest.mark.parametrize("name", list(_cases().keys()))
+def test_fused_search_bit_exact(name):
+    c = _cases()[name]()
+    sol = z.Solver.from_case(c)
+    sol.neighbor_search("old", "new")
+    sol.sync()
+    _assert_same(sol, _oracle_search(c), "fused ")
+    sol.close()
+
+
+@pytest.mark.parametrize("name", ["small_dam", "cloud_killed", "cloud_crowded_cell0", "cloud_1"])
+def test_dropin_hash_sort_index_sort_data_bit_exact(name):
+    c = _cases()[name]()
+    sol = z.Solver.from_case(c)
+    sol.hash("old")
+    sol.sort_index()
+    sol.sort_data("old", "new")
+    sol.sync()
+    _assert_same(sol, _oracle_search(c), "drop-in ")
+    sol.close()
+
+
+def test_sort_index_carries_arbitrary_values_stably():
+    c = cases.random_cloud(20000, 9)
+    sol = z.Solver.from_case(c)
+    rng = np.random.default_rng(0)
+    keys = rng.integers(0, sol.G, size=c.n).astype(np.int32)
+    keys[::7] = keys[0]  # many ties
+    vals = rng.integers(-10**6, 10**6, size=c.n).astype(np.int32)
+    sol.upload_tmp(hash=keys, index=vals)
+    sol.sort_index()
+    t = sol.download_tmp()
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(t["hash"], keys[order])
+    assert np.array_equal(t["index"], vals[order])
+    assert sol.status() & z.FLAG_BAD_KEY == 0
+    sol.close()
+
+
+def test_singleton_last_cell_keeps_stale_bounds():
+    c = cases.random_cloud(3000, 7)
+    c.state.pos[-1] = [0.2, 0.15, 0.36]
+    sol = z.Solver.from_case(c)
+    G = sol.G
+    sol.upload_tmp(grid_start=np.full(G, -7, np.int32), grid_end=np.full(G, -9, np.int32))
+    sol.neighbor_search("old", "new")
+    o = po.Oracle(c.json, c.state, np.float32)
+    o.tmp["grid_start"][:] = -7
+    o.tmp["grid_end"][:] = -9
+    o.search()
+    t = sol.download_tmp()
+    assert np.array_equal(t["grid_start"], o.tmp["grid_start"])
+    assert np.array_equal(t["grid_end"], o.tmp["grid_end"])
+    k = t["hash"][-1]
+    assert t["grid_end"][k] == -9
+    sol.close()
+
+
+def test_killed_flag_and_type100():
+    c = cases.random_cloud(4000, 11, kill_frac=0.05)
+    sol = z.Solver.from_case(c)
+    sol.neighbor_search("old", "new")
+    f = sol.status()
+    assert f & z.FLAG_KILLED
+    assert (sol.download("new").type == 100).sum() > 0
+    sol.close()
+
+
+@pytest.mark.parametrize("name", ["small_dam", "config0_dam", "cloud_killed"])
+def test_neighbor_counts_bit_exact(name):
+    c = _cases()[name]()
+    sol = z.Solver.from_case(c)
+    sol.neighbor_search("old", "new")
+    nb_b, nb_g = sol.neighbor_counts("new")
+    o = _oracle_search(c)
+    assert np.array_equal(nb_b, o.neighbor_count("new", "boundary"))
+    assert np.array_equal(nb_g, o.neighbor_count("new", "governing"))
+    sol.close()
+
+
+def test_search_twice_reuses_scratch():
+    # the counting-sort buckets must be left zeroed between searches
+    c = cases.small(0.04)
+    sol = z.Solver.from_case(c)
+    for _ in range(3):
+        sol.neighbor_search("old", "new")
+        sol.neighbor_search("new", "old")
+    o = po.Oracle(c.json, c.state, np.float32)
+    for _ in range(3):
+        o.search("old", "new")
+        o.search("new", "old")
+    t = sol.download_tmp()
+    assert np.array_equal(t["index"], o.tmp["index"])
+    assert np.array_equal(t["grid_end"], o.tmp["grid_end"])
+    assert np.array_equal(sol.download("old").pos, o.old["pos"])
+    sol.close()

@@ -1,0 +1,385 @@
+"""Python host bindings for the B200-native delta-SPH step (C ABI: include/zsph.h).
+
+The product is the CUDA library ``libzsph_b200.so`` built in this directory;
+this module only binds its C entry points with ctypes and offers a thin
+``Solver`` that owns device buffers in the reference solver's particle layout
+(single_gpu_sph_src/header/data_structure.cuh:158-182).  Importing it loads the
+library and fails loudly if it has not been built: there is no fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+__all__ = [
+    "ZsphError", "lib", "JsonCase", "CpuParam", "GpuParam", "Ptc", "Tmp", "Solver", "State",
+    "params_from_json", "LIB_PATH",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libzsph_b200.so")
+
+ZSPH_OK, ZSPH_EINVAL, ZSPH_ECUDA, ZSPH_ENAN, ZSPH_ETIMEOUT, ZSPH_EIO, ZSPH_ENOMEM = range(7)
+FLAG_NAN, FLAG_KILLED, FLAG_NB_OVERFLOW, FLAG_BAD_KEY = 1, 2, 4, 8
+_CODES = {0: "ZSPH_OK", 1: "ZSPH_EINVAL", 2: "ZSPH_ECUDA", 3: "ZSPH_ENAN", 4: "ZSPH_ETIMEOUT", 5: "ZSPH_EIO",
+          6: "ZSPH_ENOMEM"}
+
+
+class ZsphError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_CODES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make -C zsph_b200` or __graft_entry__.build(); "
+            "zsph_b200 has no CPU fallback")
+    return ctypes.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+_F = ctypes.c_float
+_I = ctypes.c_int
+_FP = ctypes.POINTER(ctypes.c_float)
+_IP = ctypes.POINTER(ctypes.c_int)
+_VP = ctypes.c_void_p
+
+
+class JsonCase(ctypes.Structure):
+    """zsph_json_t: the reference's cpu_json_t (data_structure.cuh:6-51)."""
+    _fields_ = [(n, _F) for n in ("g", "m", "rho0", "dx", "h_factor", "r_factor", "eta_factor", "cs_factor",
+                                  "delta", "alpha", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax",
+                                  "grid_layer_factor", "grid_size_factor", "dt")] + \
+              [(n, _I) for n in ("start_step", "current_step", "end_step", "output_step", "ptc_num",
+                                 "water_ptc_num", "air_ptc_num", "wall_ptc_num", "rigid_ptc_num", "thread_num",
+                                 "gpu_id")] + \
+              [("input_path", ctypes.c_char * 256), ("output_path", ctypes.c_char * 256),
+               ("git_hash", ctypes.c_char * 64)]
+
+
+class CpuParam(ctypes.Structure):
+    """zsph_cpu_param_t: the reference's cpu_param_t (data_structure.cuh:53-105)."""
+    _fields_ = [(n, _F) for n in ("g", "m", "rho0", "dx", "h", "r", "eta", "cs", "adh", "delta", "alpha", "dt")] + \
+              [(n, _I) for n in ("start_step", "current_step", "end_step", "output_step")] + \
+              [(n, _F) for n in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")] + \
+              [("grid_factor", _I), ("grid_size", _F)] + \
+              [(n, _F) for n in ("grid_xmin", "grid_ymin", "grid_zmin", "grid_xmax", "grid_ymax", "grid_zmax")] + \
+              [(n, _I) for n in ("grid_xdim", "grid_ydim", "grid_zdim", "grid_num", "grid_hash_min",
+                                 "grid_hash_max", "ptc_num", "water_ptc_num", "air_ptc_num", "wall_ptc_num",
+                                 "rigid_ptc_num", "thread_num", "gpu_id")] + \
+              [("input_path", ctypes.c_char * 256), ("output_path", ctypes.c_char * 256),
+               ("git_hash", ctypes.c_char * 64)]
+
+
+class GpuParam(ctypes.Structure):
+    """zsph_gpu_param_t: the reference's gpu_param_t (data_structure.cuh:107-134)."""
+    _fields_ = [(n, _F) for n in ("half_dt", "h", "g", "m", "rho0", "adh", "h2", "eta2", "cs2", "alpha",
+                                  "delta_h_cs", "h_cs_rho_m", "grid_size")] + \
+              [("grid_factor", _I)] + [(n, _F) for n in ("grid_xmin", "grid_ymin", "grid_zmin")] + \
+              [(n, _I) for n in ("grid_xdim", "grid_ydim", "grid_zdim", "grid_hash_min", "grid_hash_max",
+                                 "ptc_num")]
+
+
+class Ptc(ctypes.Structure):
+    """zsph_ptc_t: the reference's gpu_ptc_t (data_structure.cuh:158-168)."""
+    _fields_ = [(n, _VP) for n in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel", "tmp_rhop", "type", "table")]
+
+
+class Tmp(ctypes.Structure):
+    """zsph_tmp_t: the reference's gpu_tmp_t (data_structure.cuh:170-182)."""
+    _fields_ = [(n, _VP) for n in ("acc_drhodt", "dofv_grandrho", "dofv", "index", "hash", "grid_start",
+                                   "grid_end")]
+
+
+_HP = ctypes.c_void_p
+_sig = {
+    "zsph_read_json": (_I, [ctypes.c_char_p, ctypes.POINTER(JsonCase), ctypes.c_char_p, _I]),
+    "zsph_set_cpu_param": (_I, [ctypes.POINTER(CpuParam), ctypes.POINTER(JsonCase)]),
+    "zsph_set_gpu_param": (_I, [ctypes.POINTER(GpuParam), ctypes.POINTER(CpuParam)]),
+    "zsph_check_dt": (_I, [ctypes.POINTER(CpuParam), _FP]),
+    "zsph_alloc_ptc": (_I, [ctypes.POINTER(Ptc), _I]),
+    "zsph_free_ptc": (_I, [ctypes.POINTER(Ptc)]),
+    "zsph_alloc_tmp": (_I, [ctypes.POINTER(Tmp), _I, _I]),
+    "zsph_free_tmp": (_I, [ctypes.POINTER(Tmp)]),
+    "zsph_cpu_to_gpu": (_I, [ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
+    "zsph_gpu_to_cpu": (_I, [ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _VP]),
+    "zsph_create": (_I, [ctypes.POINTER(GpuParam), _I, ctypes.POINTER(_HP)]),
+    "zsph_destroy": (None, [_HP]),
+    "zsph_set_params": (_I, [_HP, ctypes.POINTER(GpuParam)]),
+    "zsph_hash": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_sort_index": (_I, [_HP, ctypes.POINTER(Tmp), _VP]),
+    "zsph_sort_data": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_neighbor_search": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_boundary": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_governing": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_prediction": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_correction": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_step": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
+    "zsph_run": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _VP]),
+    "zsph_status": (_I, [_HP, _IP, _I]),
+    "zsph_neighbor_counts": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _VP, _VP]),
+    "zsph_launches_per_step": (_I, [_HP]),
+    "zsph_step_profiled": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _FP, _I,
+                                _IP, ctypes.c_char_p, _I]),
+    "zsph_last_error": (_I, [_HP, ctypes.c_char_p, _I]),
+    "zsph_version": (ctypes.c_char_p, []),
+    "zsph_memcpy": (_I, [_VP, _VP, ctypes.c_size_t, _I, _VP]),
+    "zsph_device_malloc": (_I, [ctypes.POINTER(_VP), ctypes.c_size_t]),
+    "zsph_device_free": (_I, [_VP]),
+    "zsph_device_synchronize": (_I, []),
+}
+for _name, (_res, _args) in _sig.items():
+    _fn = getattr(lib, _name)
+    _fn.restype = _res
+    _fn.argtypes = _args
+
+
+def last_error(handle=None) -> str:
+    buf = ctypes.create_string_buffer(1024)
+    lib.zsph_last_error(handle, buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(rc: int, handle=None) -> None:
+    if rc != ZSPH_OK:
+        raise ZsphError(rc, last_error(handle))
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def read_json(path: str) -> JsonCase:
+    """zsph_read_json (io/read_json.cu:5-51)."""
+    j = JsonCase()
+    err = ctypes.create_string_buffer(512)
+    rc = lib.zsph_read_json(path.encode(), ctypes.byref(j), err, len(err))
+    if rc != ZSPH_OK:
+        raise ZsphError(rc, err.value.decode())
+    return j
+
+
+def params_from_json(j: JsonCase) -> tuple[CpuParam, GpuParam]:
+    """set_cpu_param + set_gpu_param (lib/init.cu:153-251); raises on dt > dt_max."""
+    cp, gp = CpuParam(), GpuParam()
+    check(lib.zsph_set_cpu_param(ctypes.byref(cp), ctypes.byref(j)))
+    check(lib.zsph_set_gpu_param(ctypes.byref(gp), ctypes.byref(cp)))
+    return cp, gp
+
+
+@dataclass
+class State:
+    """Host copy of one particle buffer set in the reference layout."""
+    pos: np.ndarray
+    vel: np.ndarray
+    rhop: np.ndarray
+    type: np.ndarray
+    table: np.ndarray
+    tmp_pos: np.ndarray | None = None
+    tmp_vel: np.ndarray | None = None
+    tmp_rhop: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.type.shape[0])
+
+    def copy(self) -> "State":
+        c = lambda a: None if a is None else a.copy()
+        return State(c(self.pos), c(self.vel), c(self.rhop), c(self.type), c(self.table), c(self.tmp_pos),
+                     c(self.tmp_vel), c(self.tmp_rhop), dict(self.extra))
+
+
+class Solver:
+    """Owns a solver handle and two particle buffer sets plus tmp arrays on
+    the current CUDA device, in the reference's layout (the OLD/NEW/tmp
+    buffers of single_gpu_sph_src/deltasph/main.cu:32-45)."""
+
+    def __init__(self, gparam: GpuParam, grid_num: int):
+        self.gp = gparam
+        self.n = int(gparam.ptc_num)
+        self.G = int(grid_num)
+        self.old, self.new, self.tmp = Ptc(), Ptc(), Tmp()
+        check(lib.zsph_alloc_ptc(ctypes.byref(self.old), self.n))
+        check(lib.zsph_alloc_ptc(ctypes.byref(self.new), self.n))
+        check(lib.zsph_alloc_tmp(ctypes.byref(self.tmp), self.n, self.G))
+        h = _HP()
+        check(lib.zsph_create(ctypes.byref(gparam), self.G, ctypes.byref(h)))
+        self.h = h
+
+    @classmethod
+    def from_case(cls, case) -> "Solver":
+        _, gp = params_from_json(case.json)
+        cp, _ = params_from_json(case.json)
+        s = cls(gp, cp.grid_num)
+        s.upload(case.state)
+        return s
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib.zsph_destroy(self.h)
+            self.h = None
+            lib.zsph_free_ptc(ctypes.byref(self.old))
+            lib.zsph_free_ptc(ctypes.byref(self.new))
+            lib.zsph_free_tmp(ctypes.byref(self.tmp))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _buf(self, which: str) -> Ptc:
+        return self.old if which == "old" else self.new
+
+    # -- host <-> device -------------------------------------------------
+    def upload(self, st: State, which: str = "old", acc: np.ndarray | None = None, stream=None) -> None:
+        b = self._buf(which)
+        f = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        i = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        pos, vel, rhop, typ, tab = f(st.pos), f(st.vel), f(st.rhop), i(st.type), i(st.table)
+        a = None if acc is None else f(acc)
+        check(lib.zsph_cpu_to_gpu(ctypes.byref(b), ctypes.byref(self.tmp), _ptr(pos), _ptr(vel), _ptr(rhop),
+                                  _ptr(typ), _ptr(tab), _ptr(a), self.n, stream))
+        for name in ("tmp_pos", "tmp_vel", "tmp_rhop"):
+            arr = getattr(st, name)
+            if arr is not None:
+                self.copy_to_device(getattr(b, name), f(arr))
+
+    def copy_to_device(self, dptr, host: np.ndarray) -> None:
+        _cudart_memcpy(dptr, host.ctypes.data, host.nbytes, 1)
+
+    def copy_from_device(self, dptr, host: np.ndarray) -> np.ndarray:
+        _cudart_memcpy(host.ctypes.data, dptr, host.nbytes, 2)
+        return host
+
+    def download(self, which: str = "old") -> State:
+        b = self._buf(which)
+        n = self.n
+        st = State(np.empty((n, 3), np.float32), np.empty((n, 3), np.float32), np.empty((n, 2), np.float32),
+                   np.empty(n, np.int32), np.empty(n, np.int32), np.empty((n, 3), np.float32),
+                   np.empty((n, 3), np.float32), np.empty((n, 2), np.float32))
+        check(lib.zsph_gpu_to_cpu(ctypes.byref(b), ctypes.byref(self.tmp), _ptr(st.pos), _ptr(st.vel),
+                                  _ptr(st.rhop), _ptr(st.type), _ptr(st.table), None, None, n, None))
+        self.copy_from_device(b.tmp_pos, st.tmp_pos)
+        self.copy_from_device(b.tmp_vel, st.tmp_vel)
+        self.copy_from_device(b.tmp_rhop, st.tmp_rhop)
+        return st
+
+    def download_tmp(self) -> dict:
+        n, G = self.n, self.G
+        out = {
+            "acc_drhodt": np.empty((n, 4), np.float32), "dofv_grandrho": np.empty((n, 4), np.float32),
+            "index": np.empty(n, np.int32), "hash": np.empty(n, np.int32),
+            "grid_start": np.empty(G, np.int32), "grid_end": np.empty(G, np.int32),
+        }
+        for k, v in out.items():
+            self.copy_from_device(getattr(self.tmp, k), v)
+        return out
+
+    def upload_tmp(self, **arrays) -> None:
+        for k, v in arrays.items():
+            dt = np.int32 if k in ("index", "hash", "grid_start", "grid_end") else np.float32
+            self.copy_to_device(getattr(self.tmp, k), np.ascontiguousarray(v, dtype=dt))
+
+    # -- entry points ----------------------------------------------------
+    def _call(self, fn, *args):
+        check(fn(self.h, *args), self.h)
+
+    def hash(self, which="old", stream=None):
+        self._call(lib.zsph_hash, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), stream)
+
+    def sort_index(self, stream=None):
+        self._call(lib.zsph_sort_index, ctypes.byref(self.tmp), stream)
+
+    def sort_data(self, src="old", dst="new", stream=None):
+        self._call(lib.zsph_sort_data, ctypes.byref(self._buf(src)), ctypes.byref(self._buf(dst)),
+                   ctypes.byref(self.tmp), stream)
+
+    def neighbor_search(self, src="old", dst="new", stream=None):
+        self._call(lib.zsph_neighbor_search, ctypes.byref(self._buf(src)), ctypes.byref(self._buf(dst)),
+                   ctypes.byref(self.tmp), stream)
+
+    def boundary(self, which="new", stream=None):
+        self._call(lib.zsph_boundary, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), stream)
+
+    def governing(self, which="new", stream=None):
+        self._call(lib.zsph_governing, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), stream)
+
+    def prediction(self, which="new", stream=None):
+        self._call(lib.zsph_prediction, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), stream)
+
+    def correction(self, which="old", stream=None):
+        self._call(lib.zsph_correction, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), stream)
+
+    def step(self, stream=None):
+        self._call(lib.zsph_step, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp), stream)
+
+    def run(self, nsteps: int, stream=None):
+        self._call(lib.zsph_run, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+                   int(nsteps), stream)
+
+    def status(self, clear: bool = True) -> int:
+        f = ctypes.c_int(0)
+        rc = lib.zsph_status(self.h, ctypes.byref(f), 1 if clear else 0)
+        if rc not in (ZSPH_OK, ZSPH_ENAN, ZSPH_EINVAL):
+            check(rc, self.h)
+        return f.value
+
+    def sync(self) -> None:
+        _cudart_sync()
+
+    def neighbor_counts(self, which="new") -> tuple[np.ndarray, np.ndarray]:
+        nb_b = _DeviceInts(self.n)
+        nb_g = _DeviceInts(self.n)
+        self._call(lib.zsph_neighbor_counts, ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), nb_b.ptr,
+                   nb_g.ptr, None)
+        return nb_b.get(), nb_g.get()
+
+    def step_profiled(self, stream=None) -> list[tuple[str, float]]:
+        """One step with per-launch CUDA-event timing: [(kernel, ms), ...]."""
+        cap = 64
+        ms = (ctypes.c_float * cap)()
+        cnt = ctypes.c_int(0)
+        names = ctypes.create_string_buffer(4096)
+        self._call(lib.zsph_step_profiled, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+                   stream, ms, cap, ctypes.byref(cnt), names, len(names))
+        nm = names.value.decode().split(",")
+        return [(nm[k], float(ms[k])) for k in range(cnt.value)]
+
+    def launches_per_step(self) -> int:
+        return int(lib.zsph_launches_per_step(self.h))
+
+
+# ---- device-memory helpers through the library's own C ABI ----------------
+def _cudart_memcpy(dst, src, nbytes, kind):
+    check(lib.zsph_memcpy(dst, src, nbytes, kind, None))
+
+
+def _cudart_sync():
+    check(lib.zsph_device_synchronize())
+
+
+class _DeviceInts:
+    def __init__(self, n: int):
+        self.n = n
+        p = _VP()
+        check(lib.zsph_device_malloc(ctypes.byref(p), max(n, 1) * 4))
+        self.ptr = p
+
+    def get(self) -> np.ndarray:
+        out = np.empty(self.n, np.int32)
+        _cudart_memcpy(out.ctypes.data, self.ptr, out.nbytes, 2)
+        return out
+
+    def __del__(self):
+        try:
+            lib.zsph_device_free(self.ptr)
+        except Exception:
+            pass

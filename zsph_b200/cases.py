@@ -1,0 +1,142 @@
+"""Synthetic case generator: 3-D dam break in the reference's JSON schema and
+particle layout.
+
+The reference ships no input cases (its driver reads input/input.json and
+input/input.vtk, single_gpu_sph_src/deltasph/main.cu:13,17); these cases are
+seeded-free, lattice-built stand-ins with the shapes of the workloads the
+solver is measured on:
+
+* water column wx x wy x wz at the x = 0 end of a tank lx x wy x lz, fluid on
+  the cubic lattice ((i+1/2)dx, (j+1/2)dx, (k+1/2)dx), type 1, zero velocity;
+* ``layers`` layers of dummy wall particles (type 0) outside the tank's floor
+  and four sides, up to the tank top (open top);
+* hydrostatic initial pressure p = rho0*|g|*(H - z) with the reference's
+  linear equation of state rho = rho0 + p/c0^2 (time_int.cu:39-40), for
+  walls below the water level too (p = 0, rho = rho0 above it);
+* dt = cfl * h / c0.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import JsonCase, State
+
+
+@dataclass
+class Case:
+    json: JsonCase
+    state: State
+    n_fluid: int
+    n_wall: int
+    name: str
+
+    @property
+    def n(self) -> int:
+        return self.state.n
+
+
+def _json(dx, xmax, ymax, zmax, dt, n, nf, nw, end_step, g=-9.81, rho0=1000.0, h_factor=1.3, r_factor=2.0,
+          eta_factor=0.1, cs_factor=10.0, delta=0.1, alpha=0.02, grid_layer_factor=2.0, grid_size_factor=1.0):
+    j = JsonCase()
+    j.g, j.rho0, j.dx = g, rho0, dx
+    j.h_factor, j.r_factor, j.eta_factor, j.cs_factor = h_factor, r_factor, eta_factor, cs_factor
+    j.delta, j.alpha = delta, alpha
+    j.xmin, j.xmax, j.ymin, j.ymax, j.zmin, j.zmax = 0.0, xmax, 0.0, ymax, 0.0, zmax
+    j.grid_layer_factor, j.grid_size_factor = grid_layer_factor, grid_size_factor
+    j.dt = dt
+    j.start_step, j.current_step, j.end_step, j.output_step = 0, 0, end_step, max(end_step, 1)
+    j.ptc_num, j.water_ptc_num, j.air_ptc_num, j.wall_ptc_num, j.rigid_ptc_num = n, nf, 0, nw, 0
+    j.thread_num, j.gpu_id = 1, 0
+    j.input_path, j.output_path, j.git_hash = b"input", b"output", b"zsph-b200"
+    return j
+
+
+def dam_break(dx: float = 0.02, water=(0.6, 0.6, 1.2), tank=(1.6, 0.6, 1.2), layers: int = 3, cfl: float = 0.2,
+              end_step: int = 2000, order: str = "fluid_first", **phys) -> Case:
+    """Dam break of the measured workloads: dx = 0.02 gives 54,000 fluid +
+    51,048 wall particles, dx = 0.005 gives 3,456,000 + 765,468."""
+    g = phys.get("g", -9.81)
+    rho0 = phys.get("rho0", 1000.0)
+    cs_factor = phys.get("cs_factor", 10.0)
+    h_factor = phys.get("h_factor", 1.3)
+    lx, ly, lz = tank
+    wx, wy, wz = water
+    nx, ny, nz = (int(round(v / dx)) for v in (wx, wy, wz))
+    tx, ty, tz = (int(round(v / dx)) for v in (lx, ly, lz))
+    # fluid lattice
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    fl = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)
+    # wall lattice: the extended box minus the tank interior, up to the tank top
+    ii, jj, kk = np.meshgrid(np.arange(-layers, tx + layers), np.arange(-layers, ty + layers),
+                             np.arange(-layers, tz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    outside = (ii < 0) | (ii >= tx) | (jj < 0) | (jj >= ty) | (kk < 0)
+    wl = np.stack([ii[outside], jj[outside], kk[outside]], axis=1)
+    pos_f = ((fl.astype(np.float64) + 0.5) * dx)
+    pos_w = ((wl.astype(np.float64) + 0.5) * dx)
+    c0 = cs_factor * math.sqrt(abs(g) * lz)
+    H = nz * dx
+
+    def hydro(z):
+        p = rho0 * abs(g) * np.clip(H - z, 0.0, None)
+        return rho0 + p / (c0 * c0), p
+
+    rf, pf = hydro(pos_f[:, 2])
+    rw, pw = hydro(pos_w[:, 2])
+    if order == "fluid_first":
+        parts = [(pos_f, rf, pf, 1), (pos_w, rw, pw, 0)]
+    else:
+        parts = [(pos_w, rw, pw, 0), (pos_f, rf, pf, 1)]
+    pos = np.concatenate([p[0] for p in parts]).astype(np.float32)
+    rho = np.concatenate([p[1] for p in parts]).astype(np.float32)
+    prs = np.concatenate([p[2] for p in parts]).astype(np.float32)
+    typ = np.concatenate([np.full(len(p[0]), p[3], np.int32) for p in parts])
+    n = len(typ)
+    st = State(pos=pos, vel=np.zeros((n, 3), np.float32), rhop=np.stack([rho, prs], axis=1).astype(np.float32),
+               type=typ, table=np.zeros(n, np.int32), tmp_pos=np.zeros((n, 3), np.float32),
+               tmp_vel=np.zeros((n, 3), np.float32), tmp_rhop=np.zeros((n, 2), np.float32))
+    h = h_factor * dx
+    dt = cfl * h / c0
+    js = _json(dx, lx, ly, lz, dt, n, len(pos_f), len(pos_w), end_step, **phys)
+    return Case(js, st, len(pos_f), len(pos_w), f"dam_break_dx{dx:g}")
+
+
+def config0() -> Case:
+    """Plain dam break, dx = 0.02 m: 54,000 fluid + 51,048 wall particles, 2000 steps."""
+    return dam_break(0.02, end_step=2000)
+
+
+def config1() -> Case:
+    """Dam break at scale, dx = 0.005 m: 3,456,000 fluid + 765,468 wall particles, 500 steps."""
+    return dam_break(0.005, end_step=500)
+
+
+def small(dx: float = 0.04) -> Case:
+    """A small dam break of the same geometry for fast parity tests."""
+    return dam_break(dx, end_step=100)
+
+
+def random_cloud(n: int, seed: int, dx: float = 0.02, box=(0.4, 0.3, 0.3), kill_frac: float = 0.0) -> Case:
+    """Seeded random particle cloud in a closed box (every particle type 1
+    except a wall shell fraction), for hash / sort / neighbour edge cases.
+    With kill_frac > 0 some particles are placed outside the grid."""
+    rng = np.random.default_rng(seed)
+    lx, ly, lz = box
+    pos = rng.uniform([0, 0, 0], [lx, ly, lz], size=(n, 3)).astype(np.float32)
+    typ = (rng.uniform(size=n) < 0.8).astype(np.int32)
+    if kill_frac > 0:
+        m = rng.uniform(size=n) < kill_frac
+        pos[m] = (pos[m] + np.float32(10.0)).astype(np.float32)
+    rho = (1000.0 + rng.uniform(0, 5, size=n)).astype(np.float32)
+    prs = ((rho - 1000.0) * 34.310349 ** 2).astype(np.float32)
+    vel = rng.normal(0, 0.1, size=(n, 3)).astype(np.float32)
+    st = State(pos=pos, vel=vel, rhop=np.stack([rho, prs], 1).astype(np.float32), type=typ,
+               table=np.zeros(n, np.int32), tmp_pos=pos.copy(), tmp_vel=vel.copy(),
+               tmp_rhop=np.stack([rho, prs], 1).astype(np.float32))
+    c0 = 10.0 * math.sqrt(9.81 * lz)
+    dt = 0.2 * 1.3 * dx / c0
+    js = _json(dx, lx, ly, lz, dt, n, int(typ.sum()), int(n - typ.sum()), 10)
+    return Case(js, st, int(typ.sum()), int(n - typ.sum()), f"cloud_{n}_{seed}")

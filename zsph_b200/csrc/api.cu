@@ -1,0 +1,531 @@
+// C ABI of the delta-SPH step (include/zsph.h): handle, buffers, entry
+// points and the step driver.
+//
+// The step follows single_gpu_sph_src/deltasph/main.cu:63-88 (predictor
+// sub-step OLD -> NEW, corrector sub-step back into OLD) with two changes
+// that keep every result where the reference leaves it:
+//  * the integration of each sub-step runs in the epilogue of the governing
+//    kernel and writes the integrated particle into the other buffer, so the
+//    neighbours still read the unintegrated state;
+//  * hence sub-step 1 ends with the predicted state in OLD, and sub-step 2
+//    sorts OLD into NEW again and writes the corrected state into OLD.
+// After zsph_step, old_ holds exactly what the reference's OLD buffers hold
+// (state sorted by the corrector's search), tmp holds the corrector's hash,
+// index, cell bounds, acc_drhodt and dofv_grandrho; new_ is scratch.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "zsph_internal.cuh"
+
+using namespace zsph;
+
+struct zsph_handle : public zsph::Handle {};
+
+namespace {
+
+std::mutex g_err_mu;
+std::string g_err;
+
+int set_err(zsph_handle* h, int code, const std::string& msg) {
+  if (h) {
+    h->err = msg;
+  } else {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    g_err = msg;
+  }
+  return code;
+}
+
+int cuda_fail(zsph_handle* h, const char* where, cudaError_t e) {
+  return set_err(h, e == cudaErrorMemoryAllocation ? ZSPH_ENOMEM : ZSPH_ECUDA,
+                 std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define ZCHECK(h, where, expr)                       \
+  do {                                               \
+    cudaError_t e_ = (expr);                         \
+    if (e_ != cudaSuccess) return cuda_fail(h, where, e_); \
+  } while (0)
+
+int validate_gparam(const zsph_gpu_param_t* p, int grid_num, std::string& why) {
+  if (p->ptc_num < 0) { why = "ptc_num < 0"; return 1; }
+  if (p->grid_xdim <= 0 || p->grid_ydim <= 0 || p->grid_zdim <= 0) { why = "grid dimensions must be positive"; return 1; }
+  const long long g = (long long)p->grid_xdim * p->grid_ydim * p->grid_zdim;
+  if (g != grid_num || g > 0x7fffffffLL - 2) { why = "grid_num != grid_xdim*grid_ydim*grid_zdim"; return 1; }
+  if (p->grid_hash_min != 0 || p->grid_hash_max != grid_num - 1) { why = "grid_hash_min/max must be 0 and grid_num-1"; return 1; }
+  if (p->grid_factor != 1 && p->grid_factor != 2) { why = "grid_factor (grid_size_factor) must be 1 or 2"; return 1; }
+  if (!(p->h > 0.0f) || !(p->grid_size > 0.0f)) { why = "h and grid_size must be positive"; return 1; }
+  return 0;
+}
+
+void fill_kparams(KParams& kp, const zsph_gpu_param_t& p, int grid_num) {
+  kp.p = p;
+  kp.n = p.ptc_num;
+  kp.G = grid_num;
+  kp.XY = p.grid_xdim * p.grid_ydim;
+  const double R2 = 4.0 * (double)p.h * (double)p.h;
+  kp.r2lo = (float)(R2 * (1.0 - 1e-5));
+  kp.r2hi = (float)(R2 * (1.0 + 1e-5));
+  kp.inv_h = 1.0f / p.h;
+  kp.c_fr = -5.0f * p.adh / p.h2;
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int check_device(zsph_handle* h) {
+  int d = -1;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) return cuda_fail(h, "cudaGetDevice", e);
+  if (d != h->device) return set_err(h, ZSPH_EINVAL, "the handle's device is not the current CUDA device");
+  return ZSPH_OK;
+}
+
+int check_ptc(zsph_handle* h, const zsph_ptc_t* p) {
+  if (!p) return set_err(h, ZSPH_EINVAL, "null particle buffers");
+  if (h->kp.n > 0 && (!p->pos || !p->vel || !p->rhop || !p->tmp_pos || !p->tmp_vel || !p->tmp_rhop || !p->type ||
+                      !p->table))
+    return set_err(h, ZSPH_EINVAL, "a particle array pointer is null");
+  return ZSPH_OK;
+}
+
+int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
+  if (!t) return set_err(h, ZSPH_EINVAL, "null scratch buffers");
+  if (h->kp.n > 0 && (!t->acc_drhodt || !t->dofv_grandrho || !t->index || !t->hash || !t->grid_start || !t->grid_end))
+    return set_err(h, ZSPH_EINVAL, "a tmp array pointer is null");
+  return ZSPH_OK;
+}
+
+void free_scratch(Scratch& s) {
+  void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
+                  s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp, s.sh.type};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  std::memset(&s, 0, sizeof s);
+}
+
+template <class T> cudaError_t dalloc(T*& p, size_t count) {
+  return cudaMalloc(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T));
+}
+
+// One sub-step of the fused path: search `from` into `to`, boundary on `to`,
+// governing + integration of `to` written into `from`.
+cudaError_t substep(zsph_handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
+                    cudaStream_t st, Prof* pf) {
+  cudaError_t e = launch_search(h->kp, h->s, h->tiles, from, to, t, st, pf);
+  if (!e) e = launch_boundary(h->kp, h->s, to, t, st, pf);
+  if (!e) e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf);
+  return e;
+}
+
+cudaError_t step_launches(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, const zsph_tmp_t& t,
+                          cudaStream_t st, Prof* pf = nullptr) {
+  cudaError_t e = substep(h, o, w, t, 1, st, pf);
+  if (!e) e = substep(h, o, w, t, 2, st, pf);
+  return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zsph_version(void) { return "zsph-b200 0.1 (sm_100a)"; }
+
+int zsph_last_error(zsph_handle_t* h, char* buf, int len) {
+  std::string m;
+  if (h) {
+    m = h->err;
+  } else {
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    m = g_err;
+  }
+  if (buf && len > 0) std::snprintf(buf, (size_t)len, "%s", m.c_str());
+  return (int)m.size();
+}
+
+int zsph_alloc_ptc(zsph_ptc_t* p, int n) {
+  if (!p || n < 0) return set_err(nullptr, ZSPH_EINVAL, "zsph_alloc_ptc: bad argument");
+  std::memset(p, 0, sizeof *p);
+  const size_t N = (size_t)(n ? n : 1);
+  float** f3[] = {&p->pos, &p->vel, &p->tmp_pos, &p->tmp_vel};
+  for (float** q : f3) {
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMalloc(reinterpret_cast<void**>(q), N * 3 * sizeof(float)));
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMemset(*q, 0, N * 3 * sizeof(float)));
+  }
+  float** f2[] = {&p->rhop, &p->tmp_rhop};
+  for (float** q : f2) {
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMalloc(reinterpret_cast<void**>(q), N * 2 * sizeof(float)));
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMemset(*q, 0, N * 2 * sizeof(float)));
+  }
+  int** i1[] = {&p->type, &p->table};
+  for (int** q : i1) {
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMalloc(reinterpret_cast<void**>(q), N * sizeof(int)));
+    ZCHECK(nullptr, "zsph_alloc_ptc", cudaMemset(*q, 0, N * sizeof(int)));
+  }
+  return ZSPH_OK;
+}
+
+int zsph_free_ptc(zsph_ptc_t* p) {
+  if (!p) return ZSPH_EINVAL;
+  void* ptrs[] = {p->pos, p->vel, p->rhop, p->tmp_pos, p->tmp_vel, p->tmp_rhop, p->type, p->table};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  std::memset(p, 0, sizeof *p);
+  return ZSPH_OK;
+}
+
+int zsph_alloc_tmp(zsph_tmp_t* t, int n, int grid_num) {
+  if (!t || n < 0 || grid_num <= 0) return set_err(nullptr, ZSPH_EINVAL, "zsph_alloc_tmp: bad argument");
+  std::memset(t, 0, sizeof *t);
+  const size_t N = (size_t)(n ? n : 1), G = (size_t)grid_num;
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->acc_drhodt), N * 4 * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->dofv_grandrho), N * 4 * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->dofv), N * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->index), N * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->hash), N * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->grid_start), G * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMalloc(reinterpret_cast<void**>(&t->grid_end), G * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->acc_drhodt, 0, N * 4 * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->dofv_grandrho, 0, N * 4 * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->dofv, 0, N * sizeof(float)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->index, 0, N * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->hash, 0, N * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->grid_start, 0, G * sizeof(int)));
+  ZCHECK(nullptr, "zsph_alloc_tmp", cudaMemset(t->grid_end, 0, G * sizeof(int)));
+  return ZSPH_OK;
+}
+
+int zsph_free_tmp(zsph_tmp_t* t) {
+  if (!t) return ZSPH_EINVAL;
+  void* ptrs[] = {t->acc_drhodt, t->dofv_grandrho, t->dofv, t->index, t->hash, t->grid_start, t->grid_end};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  std::memset(t, 0, sizeof *t);
+  return ZSPH_OK;
+}
+
+int zsph_cpu_to_gpu(const zsph_ptc_t* p, const zsph_tmp_t* t, const float* pos, const float* vel, const float* rhop,
+                    const int* type, const int* table, const float* acc, int n, void* stream) {
+  if (!p || !t || n < 0) return set_err(nullptr, ZSPH_EINVAL, "zsph_cpu_to_gpu: bad argument");
+  cudaStream_t st = as_stream(stream);
+  const size_t N = (size_t)n;
+  if (pos) ZCHECK(nullptr, "cpu_to_gpu pos", cudaMemcpyAsync(p->pos, pos, N * 12, cudaMemcpyHostToDevice, st));
+  if (vel) ZCHECK(nullptr, "cpu_to_gpu vel", cudaMemcpyAsync(p->vel, vel, N * 12, cudaMemcpyHostToDevice, st));
+  if (rhop) ZCHECK(nullptr, "cpu_to_gpu rhop", cudaMemcpyAsync(p->rhop, rhop, N * 8, cudaMemcpyHostToDevice, st));
+  if (type) ZCHECK(nullptr, "cpu_to_gpu type", cudaMemcpyAsync(p->type, type, N * 4, cudaMemcpyHostToDevice, st));
+  if (table) ZCHECK(nullptr, "cpu_to_gpu table", cudaMemcpyAsync(p->table, table, N * 4, cudaMemcpyHostToDevice, st));
+  if (acc)
+    ZCHECK(nullptr, "cpu_to_gpu acc", cudaMemcpyAsync(t->acc_drhodt, acc, N * 16, cudaMemcpyHostToDevice, st));
+  else
+    ZCHECK(nullptr, "cpu_to_gpu acc", cudaMemsetAsync(t->acc_drhodt, 0, N * 16, st));
+  ZCHECK(nullptr, "cpu_to_gpu sync", cudaStreamSynchronize(st));
+  return ZSPH_OK;
+}
+
+int zsph_gpu_to_cpu(const zsph_ptc_t* p, const zsph_tmp_t* t, float* pos, float* vel, float* rhop, int* type,
+                    int* table, float* acc, int* hash, int n, void* stream) {
+  if (!p || !t || n < 0) return set_err(nullptr, ZSPH_EINVAL, "zsph_gpu_to_cpu: bad argument");
+  cudaStream_t st = as_stream(stream);
+  const size_t N = (size_t)n;
+  if (pos) ZCHECK(nullptr, "gpu_to_cpu pos", cudaMemcpyAsync(pos, p->pos, N * 12, cudaMemcpyDeviceToHost, st));
+  if (vel) ZCHECK(nullptr, "gpu_to_cpu vel", cudaMemcpyAsync(vel, p->vel, N * 12, cudaMemcpyDeviceToHost, st));
+  if (rhop) ZCHECK(nullptr, "gpu_to_cpu rhop", cudaMemcpyAsync(rhop, p->rhop, N * 8, cudaMemcpyDeviceToHost, st));
+  if (type) ZCHECK(nullptr, "gpu_to_cpu type", cudaMemcpyAsync(type, p->type, N * 4, cudaMemcpyDeviceToHost, st));
+  if (table) ZCHECK(nullptr, "gpu_to_cpu table", cudaMemcpyAsync(table, p->table, N * 4, cudaMemcpyDeviceToHost, st));
+  if (acc) ZCHECK(nullptr, "gpu_to_cpu acc", cudaMemcpyAsync(acc, t->acc_drhodt, N * 16, cudaMemcpyDeviceToHost, st));
+  if (hash) ZCHECK(nullptr, "gpu_to_cpu hash", cudaMemcpyAsync(hash, t->hash, N * 4, cudaMemcpyDeviceToHost, st));
+  ZCHECK(nullptr, "gpu_to_cpu sync", cudaStreamSynchronize(st));
+  return ZSPH_OK;
+}
+
+int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
+  if (!gp || !out) return set_err(nullptr, ZSPH_EINVAL, "zsph_create: null argument");
+  *out = nullptr;
+  std::string why;
+  if (validate_gparam(gp, grid_num, why)) return set_err(nullptr, ZSPH_EINVAL, "zsph_create: " + why);
+  zsph_handle* h = new zsph_handle();
+  std::memset(&h->s, 0, sizeof h->s);
+  fill_kparams(h->kp, *gp, grid_num);
+  cudaError_t e = cudaGetDevice(&h->device);
+  const size_t n = (size_t)gp->ptc_num, G = (size_t)grid_num;
+  h->tiles = (grid_num + kScanTile - 1) / kScanTile;
+  Scratch& s = h->s;
+  if (!e) e = dalloc(s.cnt, G);
+  if (!e) e = dalloc(s.cell_lb, G + 1);
+  if (!e) e = dalloc(s.key, n);
+  if (!e) e = dalloc(s.ticket, n);
+  if (!e) e = dalloc(s.perm, n);
+  if (!e) e = dalloc(s.val, n);
+  if (!e) e = dalloc(s.tile_sum, (size_t)h->tiles);
+  if (!e) e = dalloc(s.tile_off, (size_t)h->tiles);
+  if (!e) e = dalloc(s.tile_last, (size_t)h->tiles);
+  if (!e) e = dalloc(s.misc, 8);
+  if (!e) e = dalloc(s.big_list, (size_t)kBigListCap);
+  if (!e) e = dalloc(s.nb, (size_t)kMaxNb * n);
+  if (!e) e = dalloc(s.nb_cnt, n);
+  if (!e) e = dalloc(s.flags, 1);
+  if (!e) e = dalloc(s.sh.pr, n);
+  if (!e) e = dalloc(s.sh.vp, n);
+  if (!e) e = dalloc(s.sh.type, n);
+  if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
+  if (!e) e = cudaMemset(s.misc, 0, 8 * sizeof(int));
+  if (!e) e = cudaMemset(s.flags, 0, sizeof(int));
+  if (!e) e = cudaMemset(s.nb_cnt, 0, n ? n : 1);
+  if (!e) e = cudaDeviceSynchronize();
+  if (e) {
+    const int code = cuda_fail(nullptr, "zsph_create", e);
+    free_scratch(h->s);
+    delete h;
+    return code;
+  }
+  *out = h;
+  return ZSPH_OK;
+}
+
+void zsph_destroy(zsph_handle_t* h) {
+  if (!h) return;
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
+  free_scratch(h->s);
+  delete h;
+}
+
+int zsph_set_params(zsph_handle_t* h, const zsph_gpu_param_t* gp) {
+  if (!h || !gp) return set_err(h, ZSPH_EINVAL, "zsph_set_params: null argument");
+  std::string why;
+  if (validate_gparam(gp, h->kp.G, why)) return set_err(h, ZSPH_EINVAL, "zsph_set_params: " + why);
+  if (gp->ptc_num != h->kp.n || gp->grid_xdim != h->kp.p.grid_xdim || gp->grid_ydim != h->kp.p.grid_ydim ||
+      gp->grid_zdim != h->kp.p.grid_zdim)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_params: particle count and grid must not change");
+  fill_kparams(h->kp, *gp, h->kp.G);
+  if (h->graph) {  // kernel arguments changed: re-capture on the next zsph_run
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return ZSPH_OK;
+}
+
+#define ENTRY_CHECKS(h)                                         \
+  if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle"); \
+  if (int rc_ = check_device(h)) return rc_;
+
+int zsph_hash(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_hash", launch_hash(h->kp, h->s.flags, *ptc, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_sort_index(zsph_handle_t* h, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_sort_index", launch_sort_index(h->kp, h->s, h->tiles, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_sort_data(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_sort_data", launch_sort_data(h->kp, h->s, h->tiles, *o, *w, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_neighbor_search(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp,
+                         void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_neighbor_search", launch_search(h->kp, h->s, h->tiles, *o, *w, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_boundary(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_boundary pack", launch_pack(h->kp, h->s, *ptc, h->last_stream));
+  ZCHECK(h, "zsph_boundary", launch_boundary(h->kp, h->s, *ptc, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_governing(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_governing pack", launch_pack(h->kp, h->s, *ptc, h->last_stream));
+  ZCHECK(h, "zsph_governing list", launch_nblist(h->kp, h->s, *tmp, h->last_stream));
+  ZCHECK(h, "zsph_governing", launch_governing(h->kp, h->s, *ptc, *tmp, 0, *ptc, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_prediction(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_prediction", launch_integrate(h->kp, h->s, *ptc, *tmp, 0, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_correction(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_correction", launch_integrate(h->kp, h->s, *ptc, *tmp, 1, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_step(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_step", step_launches(h, *o, *w, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_run(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp, int nsteps,
+             void* stream) {
+  ENTRY_CHECKS(h);
+  if (nsteps < 0) return set_err(h, ZSPH_EINVAL, "zsph_run: nsteps < 0");
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  if (nsteps == 0 || h->kp.n == 0) return ZSPH_OK;
+  const bool same = h->graph && !std::memcmp(&h->graph_old, o, sizeof *o) &&
+                    !std::memcmp(&h->graph_new, w, sizeof *w) && !std::memcmp(&h->graph_tmp, tmp, sizeof *tmp);
+  if (!same) {
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    if (!h->graph_stream) ZCHECK(h, "zsph_run stream", cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    ZCHECK(h, "zsph_run capture", cudaStreamBeginCapture(h->graph_stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t le = step_launches(h, *o, *w, *tmp, h->graph_stream);
+    cudaError_t ce = cudaStreamEndCapture(h->graph_stream, &g);
+    if (le) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run launch", le); }
+    if (ce) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run end capture", ce); }
+    cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie) { h->graph = nullptr; return cuda_fail(h, "zsph_run instantiate", ie); }
+    h->graph_old = *o;
+    h->graph_new = *w;
+    h->graph_tmp = *tmp;
+  }
+  for (int k = 0; k < nsteps; ++k) ZCHECK(h, "zsph_run launch", cudaGraphLaunch(h->graph, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_status(zsph_handle_t* h, int* flags, int clear) {
+  if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle");
+  if (int rc = check_device(h)) return rc;
+  ZCHECK(h, "zsph_status sync", cudaStreamSynchronize(h->last_stream));
+  ZCHECK(h, "zsph_status last error", cudaGetLastError());
+  int f = 0;
+  ZCHECK(h, "zsph_status read", cudaMemcpy(&f, h->s.flags, sizeof f, cudaMemcpyDeviceToHost));
+  if (clear) ZCHECK(h, "zsph_status clear", cudaMemset(h->s.flags, 0, sizeof(int)));
+  if (flags) *flags = f;
+  if (f & ZSPH_FLAG_NAN) return set_err(h, ZSPH_ENAN, "non-finite acceleration or density");
+  if (f & ZSPH_FLAG_BAD_KEY) return set_err(h, ZSPH_EINVAL, "zsph_sort_index: key outside [0, grid_num)");
+  return ZSPH_OK;
+}
+
+int zsph_neighbor_counts(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int* nb_boundary,
+                         int* nb_governing, void* stream) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, ptc)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  h->last_stream = as_stream(stream);
+  ZCHECK(h, "zsph_neighbor_counts pack", launch_pack(h->kp, h->s, *ptc, h->last_stream));
+  ZCHECK(h, "zsph_neighbor_counts list", launch_nblist(h->kp, h->s, *tmp, h->last_stream));
+  ZCHECK(h, "zsph_neighbor_counts", launch_nb_counts(h->kp, h->s, nb_boundary, nb_governing, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_memcpy(void* dst, const void* src, size_t bytes, int kind, void* stream) {
+  if (kind < 1 || kind > 3) return set_err(nullptr, ZSPH_EINVAL, "zsph_memcpy: kind must be 1, 2 or 3");
+  if (bytes == 0) return ZSPH_OK;
+  cudaStream_t st = as_stream(stream);
+  ZCHECK(nullptr, "zsph_memcpy", cudaMemcpyAsync(dst, src, bytes, (cudaMemcpyKind)kind, st));
+  ZCHECK(nullptr, "zsph_memcpy sync", cudaStreamSynchronize(st));
+  return ZSPH_OK;
+}
+
+int zsph_device_malloc(void** p, size_t bytes) {
+  if (!p) return set_err(nullptr, ZSPH_EINVAL, "zsph_device_malloc: null argument");
+  ZCHECK(nullptr, "zsph_device_malloc", cudaMalloc(p, bytes ? bytes : 1));
+  return ZSPH_OK;
+}
+
+int zsph_device_free(void* p) {
+  if (p) ZCHECK(nullptr, "zsph_device_free", cudaFree(p));
+  return ZSPH_OK;
+}
+
+int zsph_device_synchronize(void) {
+  ZCHECK(nullptr, "zsph_device_synchronize", cudaDeviceSynchronize());
+  return ZSPH_OK;
+}
+
+int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp,
+                       void* stream, float* ms, int cap, int* count, char* names, int names_len) {
+  ENTRY_CHECKS(h);
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  if (!ms || cap <= 0) return set_err(h, ZSPH_EINVAL, "zsph_step_profiled: no output slots");
+  cudaStream_t st = as_stream(stream);
+  h->last_stream = st;
+  const int slots = cap + 1;
+  std::vector<cudaEvent_t> ev(slots);
+  std::vector<const char*> nm(slots, "");
+  for (auto& e : ev) ZCHECK(h, "zsph_step_profiled event", cudaEventCreate(&e));
+  Prof pf;
+  pf.ev = ev.data() + 1;
+  pf.cap = cap;
+  pf.names = nm.data() + 1;
+  cudaEventRecord(ev[0], st);
+  cudaError_t le = step_launches(h, *o, *w, *tmp, st, &pf);
+  cudaError_t se = cudaStreamSynchronize(st);
+  const int n = pf.n;
+  std::string all;
+  for (int k = 0; k < n; ++k) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+    ms[k] = t;
+    all += nm[k + 1];
+    all += k + 1 < n ? "," : "";
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  if (le) return cuda_fail(h, "zsph_step_profiled launch", le);
+  if (se) return cuda_fail(h, "zsph_step_profiled sync", se);
+  if (names && names_len > 0) std::snprintf(names, (size_t)names_len, "%s", all.c_str());
+  if (count) *count = n;
+  return ZSPH_OK;
+}
+
+int zsph_launches_per_step(zsph_handle_t* h) {
+  (void)h;
+  // per sub-step: hash_count, scan_reduce, scan_cells, scatter, sort_big_cells,
+  // rank_gather, nblist, boundary, governing
+  return 2 * 9;
+}
+
+}  // extern "C"

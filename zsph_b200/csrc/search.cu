@@ -1,0 +1,447 @@
+// Neighbour search for sm_100a: cell hash, stable counting sort by cell,
+// cell bounds and reorder.
+//
+// Reference path replaced (single_gpu_sph_src/):
+//   lib/hash.cu:3-26     cuda_ptc_hash      -> k_hash (drop-in) / k_hash_count (fused)
+//   lib/sort.cu:3-6      thrust::sort_by_key-> counting sort: count -> scan -> scatter -> rank
+//   lib/sort.cu:8-84     cuda_sort_data     -> k_scan_cells (bounds) + k_rank_gather (reorder)
+//
+// The reference sorts all 32 key bits with a generic radix sort.  Here the
+// keys are cell ids in [0, G), so a counting sort needs one histogram, one
+// scan over G cells and one scatter.  The scatter uses warp-aggregated
+// atomic tickets, which are not ordered across warps; stability (ties in
+// prior position order, the reference's sort_by_key contract) is restored
+// by ranking each particle among the members of its cell by original
+// position.  Cells with more than kBigSegment members are first sorted in
+// place by one CTA each.  The cell bounds are written from the scanned
+// offsets in closed form, including the reference's end-of-array rules
+// (sort.cu:30-60): with lb(c) the number of particles whose key is below c,
+//   grid_start[c] = min(lb(c),   N-1)
+//   grid_end[c]   = min(lb(c+1), N-1)
+// except that, when the last sorted particle is alone in its cell (key k),
+// grid_end[c] for c >= k and grid_start[c] for c > k are left untouched.
+#include <climits>
+
+#include "zsph_internal.cuh"
+
+namespace zsph {
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Cell hash of one position, exactly as hash.cu:12-15 computes it (IEEE
+// subtract and divide, floorf, float->int conversion, int multiply-add).
+__device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, float y, float z) {
+  const int hx = (int)floorf(__fdiv_rn(__fsub_rn(x, p.grid_xmin), p.grid_size));
+  const int hy = (int)floorf(__fdiv_rn(__fsub_rn(y, p.grid_ymin), p.grid_size));
+  const int hz = (int)floorf(__fdiv_rn(__fsub_rn(z, p.grid_zmin), p.grid_size));
+  return hz * p.grid_xdim * p.grid_ydim + hy * p.grid_xdim + hx;
+}
+
+// hash.cu:16-23: a particle outside the grid becomes type 100 at the grid
+// origin with zero velocity and (rho0, 0); its key becomes 0.
+__device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t& s, int i, int* flags) {
+  const zsph_gpu_param_t& p = kp.p;
+  const float x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
+  int h = cell_hash(p, x, y, z);
+  if (h < p.grid_hash_min || h > p.grid_hash_max) {
+    s.type[i] = 100;
+    s.pos[3 * i] = p.grid_xmin;
+    s.pos[3 * i + 1] = p.grid_ymin;
+    s.pos[3 * i + 2] = p.grid_zmin;
+    s.vel[3 * i] = 0.0f;
+    s.vel[3 * i + 1] = 0.0f;
+    s.vel[3 * i + 2] = 0.0f;
+    s.rhop[2 * i] = p.rho0;
+    s.rhop[2 * i + 1] = 0.0f;
+    h = 0;
+    atomicOr(flags, ZSPH_FLAG_KILLED);
+  }
+  return h;
+}
+
+// One atomic per distinct key per warp; returns this lane's ticket (its
+// arrival rank inside the key's cell).  Lanes of one warp that share a key
+// get consecutive tickets in lane order.
+__device__ __forceinline__ int warp_ticket(int* cnt, int key, unsigned active) {
+  const unsigned peers = __match_any_sync(active, key);
+  const int leader = __ffs(peers) - 1;
+  const int rank = __popc(peers & lanemask_lt());
+  int base = 0;
+  if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&cnt[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + rank;
+}
+
+// Drop-in cuda_ptc_hash: hash + identity index (hash.cu:3-26).
+__global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp, zsph_ptc_t s, zsph_tmp_t t, int* flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kp.n) return;
+  t.hash[i] = hash_and_kill(kp, s, i, flags);
+  t.index[i] = i;
+}
+
+// Fused search, step 1: hash + kill + per-cell ticket.
+__global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp, zsph_ptc_t s, Scratch sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned active = __ballot_sync(0xffffffffu, i < kp.n);
+  if (i >= kp.n) return;
+  const int h = hash_and_kill(kp, s, i, sc.flags);
+  sc.key[i] = h;
+  sc.ticket[i] = warp_ticket(sc.cnt, h, active);
+}
+
+// Drop-in sort_index, step 1: copy keys and carried values, count.
+__global__ void __launch_bounds__(kSearchBlock) k_count_keys(KParams kp, zsph_tmp_t t, Scratch sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned active = __ballot_sync(0xffffffffu, i < kp.n);
+  if (i >= kp.n) return;
+  int h = t.hash[i];
+  if (h < 0 || h >= kp.G) {
+    atomicOr(sc.flags, ZSPH_FLAG_BAD_KEY);
+    h = h < 0 ? 0 : kp.G - 1;
+  }
+  sc.key[i] = h;
+  sc.val[i] = t.index[i];
+  sc.ticket[i] = warp_ticket(sc.cnt, h, active);
+}
+
+// Drop-in sort_data, step 1: histogram of already-sorted keys.
+__global__ void __launch_bounds__(kSearchBlock) k_count_sorted(KParams kp, zsph_tmp_t t, Scratch sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned active = __ballot_sync(0xffffffffu, i < kp.n);
+  if (i >= kp.n) return;
+  int h = t.hash[i];
+  if (h < 0 || h >= kp.G) {
+    atomicOr(sc.flags, ZSPH_FLAG_BAD_KEY);
+    h = h < 0 ? 0 : kp.G - 1;
+  }
+  warp_ticket(sc.cnt, h, active);
+}
+
+// Block-wide exclusive scan of one int per thread (kSearchBlock threads).
+__device__ __forceinline__ int block_exclusive_scan(int v, int* smem_warp, int& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < kSearchBlock / 32 ? smem_warp[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kSearchBlock / 32) smem_warp[lane] = w;
+  }
+  __syncthreads();
+  total = smem_warp[kSearchBlock / 32 - 1];
+  const int before = warp > 0 ? smem_warp[warp - 1] : 0;
+  __syncthreads();
+  return before + x - v;
+}
+
+// Scan step 1: per-tile count sums and last occupied cell; the last CTA to
+// finish scans the tile sums into tile offsets and finds the last key.
+__global__ void __launch_bounds__(kSearchBlock) k_scan_reduce(KParams kp, Scratch sc, int tiles) {
+  __shared__ int sw[kSearchBlock / 32];
+  __shared__ int s_last;
+  __shared__ bool s_am_last;
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int sum = 0, last = -1;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int c = base + k;
+    if (c < kp.G) {
+      const int v = sc.cnt[c];
+      sum += v;
+      if (v > 0) last = c;
+    }
+  }
+  if (threadIdx.x == 0) s_last = -1;
+  int total;
+  block_exclusive_scan(sum, sw, total);
+  if (last >= 0) atomicMax(&s_last, last);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sc.tile_sum[blockIdx.x] = total;
+    sc.tile_last[blockIdx.x] = s_last;
+    __threadfence();
+    const int done = atomicAdd(&sc.misc[0], 1);
+    s_am_last = (done == tiles - 1);
+  }
+  __syncthreads();
+  if (!s_am_last) return;
+  __threadfence();
+  // Last CTA: exclusive scan over the tile sums, in chunks of kSearchBlock.
+  int carry = 0, klast = -1;
+  for (int b0 = 0; b0 < tiles; b0 += kSearchBlock) {
+    const int b = b0 + threadIdx.x;
+    const int v = b < tiles ? ((volatile int*)sc.tile_sum)[b] : 0;
+    const int tl = b < tiles ? ((volatile int*)sc.tile_last)[b] : -1;
+    int chunk;
+    const int ex = block_exclusive_scan(v, sw, chunk);
+    if (b < tiles) sc.tile_off[b] = carry + ex;
+    carry += chunk;
+    if (tl > klast) klast = tl;
+  }
+  if (threadIdx.x == 0) s_last = -1;
+  __syncthreads();
+  atomicMax(&s_last, klast);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sc.misc[1] = s_last;
+    sc.misc[2] = s_last >= 0 ? sc.cnt[s_last] : 0;
+    sc.misc[3] = 0;  // big-cell list length
+    sc.misc[0] = 0;  // ready for the next use
+  }
+}
+
+// Scan step 2: cell offsets, grid_start/grid_end in closed form, count reset.
+__global__ void __launch_bounds__(kSearchBlock) k_scan_cells(KParams kp, Scratch sc, zsph_tmp_t t, int bounds) {
+  __shared__ int sw[kSearchBlock / 32];
+  const int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int c = base + k;
+    v[k] = c < kp.G ? sc.cnt[c] : 0;
+    sum += v[k];
+  }
+  int total;
+  int lb = block_exclusive_scan(sum, sw, total) + sc.tile_off[blockIdx.x];
+  const int n = kp.n, klast = sc.misc[1];
+  const bool last_single = sc.misc[2] == 1;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    const int c = base + k;
+    if (c < kp.G) {
+      const int lb1 = lb + v[k];
+      sc.cell_lb[c] = lb;
+      if (bounds && !(last_single && c > klast)) t.grid_start[c] = min(lb, n - 1);
+      if (bounds && !(last_single && c >= klast)) t.grid_end[c] = min(lb1, n - 1);
+      if (v[k] != 0) sc.cnt[c] = 0;
+      if (v[k] > kBigSegment) {
+        const int slot = atomicAdd(&sc.misc[3], 1);
+        if (slot < kBigListCap) sc.big_list[slot] = c;
+      }
+      if (c == kp.G - 1) sc.cell_lb[kp.G] = lb1;
+      lb = lb1;
+    }
+  }
+}
+
+// Scatter by ticket (unstable inside a cell until ranked).
+__global__ void __launch_bounds__(kSearchBlock) k_scatter(KParams kp, Scratch sc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kp.n) return;
+  sc.perm[sc.cell_lb[sc.key[i]] + sc.ticket[i]] = i;
+}
+
+// Sorts perm[a, a+n) ascending in place with one CTA: a bitonic network in
+// which every comparator puts the minimum at the lower index, so virtual
+// +inf padding beyond n never has to be stored.
+__device__ void cta_sort_segment(int* v, int n) {
+  int P = 1;
+  while (P < n) P <<= 1;
+  for (int k = 2; k <= P; k <<= 1) {
+    for (int idx = threadIdx.x; idx < P / 2; idx += blockDim.x) {
+      const int half = k >> 1;
+      const int blk = idx / half, off = idx % half;
+      const int lo = blk * k + off, hi = blk * k + k - 1 - off;
+      if (hi < n) {
+        const int a = v[lo], b = v[hi];
+        if (a > b) { v[lo] = b; v[hi] = a; }
+      }
+    }
+    __syncthreads();
+    for (int j = k >> 2; j >= 1; j >>= 1) {
+      for (int idx = threadIdx.x; idx < P / 2; idx += blockDim.x) {
+        const int blk = idx / j, off = idx % j;
+        const int lo = blk * 2 * j + off, hi = lo + j;
+        if (hi < n) {
+          const int a = v[lo], b = v[hi];
+          if (a > b) { v[lo] = b; v[hi] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Pre-sorts the members of crowded cells (more than kBigSegment particles).
+// Uses the list built by k_scan_cells, or every cell if the list overflowed.
+__global__ void __launch_bounds__(1024) k_sort_big_cells(KParams kp, Scratch sc) {
+  const int listed = sc.misc[3];
+  if (listed == 0) return;
+  if (listed <= kBigListCap) {
+    for (int e = blockIdx.x; e < listed; e += gridDim.x) {
+      const int c = sc.big_list[e];
+      const int a = sc.cell_lb[c], b = sc.cell_lb[c + 1];
+      cta_sort_segment(sc.perm + a, b - a);
+    }
+  } else {
+    for (int c = blockIdx.x; c < kp.G; c += gridDim.x) {
+      const int a = sc.cell_lb[c], b = sc.cell_lb[c + 1];
+      if (b - a > kBigSegment) cta_sort_segment(sc.perm + a, b - a);
+    }
+  }
+}
+
+// Final slot of the particle scattered to slot t: its rank by original
+// position among the members of its cell.
+__device__ __forceinline__ int ranked_slot(const Scratch& sc, int t, int i, int c) {
+  const int a = sc.cell_lb[c], b = sc.cell_lb[c + 1];
+  if (b - a > kBigSegment) return t;  // pre-sorted by k_sort_big_cells
+  int r = 0;
+  for (int k = a; k < b; ++k) r += (__ldg(&sc.perm[k]) < i) ? 1 : 0;
+  return a + r;
+}
+
+__device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t& w, const Shadow& sh, int src,
+                                           int dst) {
+  const float x = o.pos[3 * src], y = o.pos[3 * src + 1], z = o.pos[3 * src + 2];
+  const float vx = o.vel[3 * src], vy = o.vel[3 * src + 1], vz = o.vel[3 * src + 2];
+  const float2 rp = reinterpret_cast<const float2*>(o.rhop)[src];
+  const float tx = o.tmp_pos[3 * src], ty = o.tmp_pos[3 * src + 1], tz = o.tmp_pos[3 * src + 2];
+  const float ux = o.tmp_vel[3 * src], uy = o.tmp_vel[3 * src + 1], uz = o.tmp_vel[3 * src + 2];
+  const float2 trp = reinterpret_cast<const float2*>(o.tmp_rhop)[src];
+  const int ty_ = o.type[src];
+  const int tb = o.table[src];
+  w.pos[3 * dst] = x; w.pos[3 * dst + 1] = y; w.pos[3 * dst + 2] = z;
+  w.vel[3 * dst] = vx; w.vel[3 * dst + 1] = vy; w.vel[3 * dst + 2] = vz;
+  reinterpret_cast<float2*>(w.rhop)[dst] = rp;
+  w.tmp_pos[3 * dst] = tx; w.tmp_pos[3 * dst + 1] = ty; w.tmp_pos[3 * dst + 2] = tz;
+  w.tmp_vel[3 * dst] = ux; w.tmp_vel[3 * dst + 1] = uy; w.tmp_vel[3 * dst + 2] = uz;
+  reinterpret_cast<float2*>(w.tmp_rhop)[dst] = trp;
+  w.type[dst] = ty_;
+  w.table[dst] = tb + src - dst;  // sort.cu:82
+  sh.pr[dst] = make_float4(x, y, z, rp.x);
+  sh.vp[dst] = make_float4(vx, vy, vz, rp.y);
+  sh.type[dst] = ty_;
+}
+
+// Fused search, last step: rank, write sorted hash/index, gather the eight
+// particle arrays (sort.cu:62-82) and the packed shadows.
+__global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
+                                                              zsph_tmp_t t) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= kp.n) return;
+  const int i = sc.perm[slot];
+  const int c = sc.key[i];
+  const int dst = ranked_slot(sc, slot, i, c);
+  t.index[dst] = i;
+  t.hash[dst] = c;
+  gather_one(o, w, sc.sh, i, dst);
+}
+
+// Drop-in sort_index, last step: sorted keys and carried values.
+__global__ void __launch_bounds__(kSearchBlock) k_rank_values(KParams kp, Scratch sc, zsph_tmp_t t) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= kp.n) return;
+  const int i = sc.perm[slot];
+  const int c = sc.key[i];
+  const int dst = ranked_slot(sc, slot, i, c);
+  t.hash[dst] = c;
+  t.index[dst] = sc.val[i];
+}
+
+// Drop-in sort_data reorder: new[t] = old[index[t]] (sort.cu:62-82).
+__global__ void __launch_bounds__(kSearchBlock) k_gather_by_index(KParams kp, Scratch sc, zsph_ptc_t o,
+                                                                  zsph_ptc_t w, zsph_tmp_t t) {
+  const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot >= kp.n) return;
+  gather_one(o, w, sc.sh, t.index[slot], slot);
+}
+
+// Packed shadows of an unsorted-by-us state (drop-in pair entry points).
+__global__ void __launch_bounds__(kSearchBlock) k_pack(KParams kp, Shadow sh, zsph_ptc_t s) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kp.n) return;
+  const float2 rp = reinterpret_cast<const float2*>(s.rhop)[i];
+  sh.pr[i] = make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], rp.x);
+  sh.vp[i] = make_float4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], rp.y);
+  sh.type[i] = s.type[i];
+}
+
+inline int blocks_for(int n, int b) { return (n + b - 1) / b; }
+
+cudaError_t launch_scan(const KParams& kp, const Scratch& s, int tiles, const zsph_tmp_t& t, int bounds,
+                        cudaStream_t st, Prof* pf = nullptr) {
+  k_scan_reduce<<<tiles, kSearchBlock, 0, st>>>(kp, s, tiles);
+  mark(pf, "scan_reduce", st);
+  k_scan_cells<<<tiles, kSearchBlock, 0, st>>>(kp, s, t, bounds);
+  mark(pf, "scan_cells", st);
+  return cudaGetLastError();
+}
+
+constexpr int kBigSortCtas = 148;
+
+}  // namespace
+
+cudaError_t launch_hash(const KParams& kp, int* flags, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                        cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  k_hash<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, ptc, tmp, flags);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort_index(const KParams& kp, const Scratch& s, int tiles, const zsph_tmp_t& tmp,
+                              cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  const int nb = blocks_for(kp.n, kSearchBlock);
+  k_count_keys<<<nb, kSearchBlock, 0, st>>>(kp, tmp, s);
+  // cell offsets only: cuda_sort_index leaves grid_start/grid_end alone
+  cudaError_t e = launch_scan(kp, s, tiles, tmp, 0, st);
+  if (e) return e;
+  k_scatter<<<nb, kSearchBlock, 0, st>>>(kp, s);
+  k_sort_big_cells<<<kBigSortCtas, 1024, 0, st>>>(kp, s);
+  k_rank_values<<<nb, kSearchBlock, 0, st>>>(kp, s, tmp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sort_data(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o,
+                             const zsph_ptc_t& w, const zsph_tmp_t& tmp, cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  const int nb = blocks_for(kp.n, kSearchBlock);
+  k_count_sorted<<<nb, kSearchBlock, 0, st>>>(kp, tmp, s);
+  cudaError_t e = launch_scan(kp, s, tiles, tmp, 1, st);
+  if (e) return e;
+  k_gather_by_index<<<nb, kSearchBlock, 0, st>>>(kp, s, o, w, tmp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
+                          const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf) {
+  if (kp.n == 0) return cudaSuccess;
+  const int nb = blocks_for(kp.n, kSearchBlock);
+  k_hash_count<<<nb, kSearchBlock, 0, st>>>(kp, o, s);
+  mark(pf, "hash_count", st);
+  cudaError_t e = launch_scan(kp, s, tiles, tmp, 1, st, pf);
+  if (e) return e;
+  k_scatter<<<nb, kSearchBlock, 0, st>>>(kp, s);
+  mark(pf, "scatter", st);
+  k_sort_big_cells<<<kBigSortCtas, 1024, 0, st>>>(kp, s);
+  mark(pf, "sort_big_cells", st);
+  k_rank_gather<<<nb, kSearchBlock, 0, st>>>(kp, s, o, w, tmp);
+  mark(pf, "rank_gather", st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  k_pack<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s.sh, ptc);
+  return cudaGetLastError();
+}
+
+}  // namespace zsph

@@ -1,0 +1,109 @@
+// Internal declarations shared by the sm_100a kernels and the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/zsph.h"
+
+namespace zsph {
+
+constexpr int kSearchBlock = 256;  // threads per CTA for the streaming (HBM-bound) kernels
+constexpr int kScanItems = 8;      // cells per thread in the cell-offset scan
+constexpr int kScanTile = kSearchBlock * kScanItems;
+constexpr int kBigSegment = 256;   // cells holding more particles than this are pre-sorted by a CTA
+constexpr int kBigListCap = 4096;  // at most this many such cells are pre-sorted per sub-step
+constexpr int kPairBlock = 128;    // threads per CTA for the neighbour-list and pair kernels
+constexpr int kMaxNb = 128;        // neighbour-list capacity per particle (overflow -> direct path)
+
+// Constants of one case, passed by value to every kernel.  Mirrors
+// gpu_param_t plus the values the kernels derive from it once on the host.
+struct KParams {
+  zsph_gpu_param_t p;
+  int n;                 // particles
+  int G;                 // cells
+  int XY;                // grid_xdim * grid_ydim
+  float r2lo, r2hi;      // rr2 < r2lo => q <= 2 for sure; rr2 > r2hi => q > 2 for sure
+  float inv_h;
+  float c_fr;            // -5 * adh / h2, the factor of grad W / r
+};
+
+// Packed per-particle shadows of the sorted state, written by the gather
+// (16-byte loads in the pair kernels).  pr = {x, y, z, rho}, vp = {vx, vy, vz, p}.
+struct Shadow {
+  float4* pr;
+  float4* vp;
+  int* type;
+};
+
+// Device scratch owned by a handle; allocated once in zsph_create.
+struct Scratch {
+  int* cnt;          // [G]   per-cell counts (kept zero between uses)
+  int* cell_lb;      // [G+1] exclusive prefix of counts: first sorted slot of each cell
+  int* key;          // [n]   unsorted cell keys
+  int* ticket;       // [n]   arrival rank inside the key's cell
+  int* perm;         // [n]   scattered original positions (stable after ranking)
+  int* val;          // [n]   carried values for zsph_sort_index
+  int* tile_sum;     // [tiles]
+  int* tile_off;     // [tiles]
+  int* tile_last;    // [tiles] last occupied cell of each tile (-1 if none)
+  int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length
+  int* big_list;     // [kBigListCap]
+  uint16_t* nb;      // [kMaxNb * n] neighbour lists, column-major (entry k of particle i at k*n+i)
+  uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
+  int* flags;        // [1]   ZSPH_FLAG_* bits
+  Shadow sh;
+};
+
+// Optional per-launch event markers (profiling): after each kernel launch the
+// launcher records the next event, so event k-1 -> k brackets launch k.
+struct Prof {
+  cudaEvent_t* ev = nullptr;
+  int cap = 0;
+  int n = 0;
+  const char** names = nullptr;
+};
+
+inline void mark(Prof* pf, const char* name, cudaStream_t st) {
+  if (pf && pf->n < pf->cap) {
+    pf->names[pf->n] = name;
+    cudaEventRecord(pf->ev[pf->n++], st);
+  }
+}
+
+struct Handle {
+  KParams kp;
+  Scratch s;
+  int device = 0;
+  int tiles = 0;
+  cudaStream_t last_stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  zsph_ptc_t graph_old{}, graph_new{};
+  zsph_tmp_t graph_tmp{};
+  cudaStream_t graph_stream = nullptr;
+  std::string err;
+};
+
+// search.cu
+cudaError_t launch_hash(const KParams& kp, int* flags, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp, cudaStream_t st);
+cudaError_t launch_sort_index(const KParams& kp, const Scratch& s, int tiles, const zsph_tmp_t& tmp, cudaStream_t st);
+cudaError_t launch_sort_data(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
+                             const zsph_tmp_t& tmp, cudaStream_t st);
+cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
+                          const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf = nullptr);
+cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st);
+
+// equations.cu
+cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                            cudaStream_t st, Prof* pf = nullptr);
+// mode 0: acc_drhodt only; 1: + prediction into out; 2: + correction into out
+cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                             int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr);
+cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& tmp, cudaStream_t st);
+cudaError_t launch_nb_counts(const KParams& kp, const Scratch& s, int* nb_boundary, int* nb_governing,
+                             cudaStream_t st);
+cudaError_t launch_integrate(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                             int correction, cudaStream_t st);
+
+}  // namespace zsph
