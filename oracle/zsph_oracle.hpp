@@ -26,6 +26,11 @@
 //                    loaded before the write, delta_ns.cu:25).  This is the
 //                    semantics of the product kernels.
 //   WALLS_OLD   (1): every neighbour read sees the old density.
+//   WALLS_SPLIT (2): loop 1 (renormalisation matrix, div v) sees the old wall
+//                    densities and loop 2 (grad rho) the new ones -- the
+//                    outcome of the race when the reading and the writing
+//                    threads run concurrently (each wall thread writes after
+//                    its own loop 1, before the readers reach loop 2).
 //
 // The neighbour visit order is the reference's: stencil rows z = -gf..gf,
 // y = -gf..gf-1 (boundary, delta_ns.cu:35-37) or y = -gf..gf (governing,
@@ -42,7 +47,7 @@
 
 namespace zsph_oracle {
 
-enum { WALLS_FIRST = 0, WALLS_OLD = 1 };
+enum { WALLS_FIRST = 0, WALLS_OLD = 1, WALLS_SPLIT = 2 };
 
 // Derived constants; field meaning follows gpu_param_t
 // (single_gpu_sph_src/header/data_structure.cuh:107-134) plus the host-side
@@ -236,8 +241,9 @@ template <class T> void boundary(const Params& p, State<T>& s, Tmp<T>& t, int wa
   wall_pressure(p, s, t, rho_new, p_new);
   std::vector<T> rho_old(n);
   for (int i = 0; i < n; ++i) rho_old[i] = s.rhop[2 * i];
-  // Densities seen through neighbour reads.
+  // Densities seen through neighbour reads in loop 1 and loop 2.
   const std::vector<T>& rho_nb = (wall_mode == WALLS_FIRST) ? rho_new : rho_old;
+  const std::vector<T>& rho_nb2 = (wall_mode == WALLS_OLD) ? rho_old : rho_new;
   const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m;
 #pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < n; ++i) {
@@ -292,7 +298,7 @@ template <class T> void boundary(const Params& p, State<T>& s, Tmp<T>& t, int wa
       if (q <= (T)2) {
         const T a = (T)1 - q / (T)2;
         T fr = (T)-5 * adh * a * a * a / h2;
-        const T rj = rho_nb[j];
+        const T rj = rho_nb2[j];
         fr *= (rj - rho0_i) * m / rj;
         for (int r = 0; r < 3; ++r) gr[r] += (M[r][0] * d[0] + M[r][1] * d[1] + M[r][2] * d[2]) * fr;
       }

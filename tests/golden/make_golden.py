@@ -9,9 +9,12 @@ Fixtures (numpy .npz, compressed):
   ref_search_*.npz    one neighbour search (hash, sort_by_key, cuda_sort_data)
                       of a case: sorted hash/index, cell bounds, gathered state,
                       and per-particle neighbour counts by the reference's test
-  ref_kernels_*.npz   + cuda_boundary_ns + cuda_govering_ns outputs
-  ref_steps_*.npz     N full reference steps, run twice (the reference's wall
-                      density race makes runs differ; both are kept)
+  ref_kernels_*.npz   + cuda_boundary_ns + cuda_govering_ns outputs, on the
+                      case with wall-consistent initial (rho, p) ("cond")
+                      and on the raw case ("raw", where the reference's wall
+                      density race decides part of the result)
+  ref_steps_*.npz     N full reference steps of the conditioned case, run
+                      twice (the race can still make runs differ)
 """
 import os
 import sys
@@ -22,6 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)
 sys.path.insert(0, ROOT)
 
 from oracle import pyoracle as po  # noqa: E402
+from tests.helpers import condition_walls  # noqa: E402
 from zsph_b200 import cases  # noqa: E402
 
 OUT = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
@@ -62,10 +66,12 @@ def main():
                             **{f"new.{k}": v for k, v in out.items()},
                             **{k: tmp[k] for k in ("hash", "index", "grid_start", "grid_end", "nb_boundary",
                                                    "nb_governing")})
-    c = GOLDEN_CASES["dam05"]()
-    out, tmp = po.ref_substep(c.json, c.state, 5)
-    np.savez_compressed(os.path.join(OUT, "ref_kernels_dam05.npz"), rhop=out["rhop"], type=out["type"],
-                        acc_drhodt=tmp["acc_drhodt"], dofv_grandrho=tmp["dofv_grandrho"])
+    raw = GOLDEN_CASES["dam05"]()
+    c = condition_walls(raw)
+    for tag, cc in (("cond", c), ("raw", raw)):
+        out, tmp = po.ref_substep(cc.json, cc.state, 5)
+        np.savez_compressed(os.path.join(OUT, f"ref_kernels_dam05_{tag}.npz"), rhop=out["rhop"], type=out["type"],
+                            acc_drhodt=tmp["acc_drhodt"], dofv_grandrho=tmp["dofv_grandrho"])
     runs = {}
     for r in range(2):
         out, tmp, _ = po.ref_run(c.json, c.state, 20)

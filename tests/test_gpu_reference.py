@@ -7,6 +7,7 @@ import pytest
 
 import zsph_b200 as z
 from oracle import pyoracle as po
+from tests.helpers import condition_walls
 from zsph_b200 import cases
 
 pytestmark = [pytest.mark.gpu,
@@ -54,30 +55,29 @@ def _by_id(arr, table):
     return out
 
 
-def test_kernels_within_reference_spread():
-    c = cases.small(0.04)
-    runs = [po.ref_substep(c.json, c.state, 5) for _ in range(2)]
+def test_kernels_match_reference_cuda_on_wall_consistent_input():
+    # on wall-consistent input the reference's wall-density race has nothing
+    # to decide, so its boundary/governing outputs are a fixed function of the
+    # input: ours must agree to FP32 rounding
+    c = condition_walls(cases.small(0.04))
+    out, tmp = po.ref_substep(c.json, c.state, 5)
     sol = z.Solver.from_case(c)
     sol.neighbor_search("old", "new")
     sol.boundary("new")
     sol.governing("new")
     t = sol.download_tmp()
     new = sol.download("new")
-    ref_out, ref_tmp = runs[0]
-    fl = new.type == 1
-    acc_scale = np.abs(ref_tmp["acc_drhodt"][fl]).max(axis=0)
-    d = np.abs(t["acc_drhodt"][fl] - ref_tmp["acc_drhodt"][fl])
-    spread = np.abs(runs[0][1]["acc_drhodt"][fl] - runs[1][1]["acc_drhodt"][fl]).max(axis=0)
-    # fluid accelerations agree to within the reference's own run-to-run spread
-    # plus FP32 rounding (1e-3 of the field scale: the wall race moves near-wall
-    # values by far more than rounding does)
-    assert np.all(d.max(axis=0) <= spread + 1e-3 * acc_scale), (d.max(axis=0), spread, acc_scale)
-    # interior fluid (no wall in reach): unaffected by the race, FP32 rounding only
+    assert np.array_equal(new.type, out["type"])
+    for k in ("dofv_grandrho", "acc_drhodt"):
+        scale = np.abs(tmp[k]).max(axis=0) + 1e-30
+        d = np.abs(t[k] - tmp[k]).max(axis=0)
+        assert np.all(d <= 1e-4 * scale), (k, d, scale)
+    assert np.allclose(new.rhop, out["rhop"], rtol=1e-6, atol=1e-3)
     sol.close()
 
 
 def test_steps_within_reference_envelope():
-    c = cases.small(0.04)
+    c = condition_walls(cases.small(0.04))
     n = 20
     r0, _, _ = po.ref_run(c.json, c.state, n)
     r1, _, _ = po.ref_run(c.json, c.state, n)
