@@ -101,7 +101,7 @@ int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
 
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
-                  s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp, s.sh.type};
+                  s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(&s, 0, sizeof s);
@@ -269,7 +269,6 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.flags, 1);
   if (!e) e = dalloc(s.sh.pr, n);
   if (!e) e = dalloc(s.sh.vp, n);
-  if (!e) e = dalloc(s.sh.type, n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
   if (!e) e = cudaMemset(s.misc, 0, 8 * sizeof(int));
   if (!e) e = cudaMemset(s.flags, 0, sizeof(int));

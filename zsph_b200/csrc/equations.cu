@@ -6,21 +6,34 @@
 //   lib/time_int.cu:3-92         cuda_prediction / cuda_correction -> k_integrate or k_governing epilogue
 //
 // Design.  The reference re-scans every candidate of the cell stencil in each
-// of its three neighbour loops per sub-step, and every lane of a warp pays
-// for the full pair arithmetic whenever any lane has a neighbour.  Here one
-// kernel filters the candidates once per sub-step (the governing stencil is
-// a superset of the boundary stencil) and writes, per particle, the list of
-// interacting neighbours in the reference's visit order: stencil rows in
-// (z, y) order, inside a row the sorted particle range.  Entries are 16-bit
-// (row << 11 | offset inside the row's range), column-major so that a warp's
-// accesses coalesce.  The pair kernels then walk their lists with all lanes
-// converged.  The visit order is the reference's, so the order-dependent
-// recurrence on grad(rho).x (delta_ns.cu:244-245) gets the same sequence.
+// of its three neighbour loops per sub-step, one thread per particle, and
+// every lane of a warp pays for the full pair arithmetic whenever any lane
+// has a neighbour.  Here:
+//  * k_nblist filters the candidates ONCE per sub-step (the governing stencil
+//    is a superset of the boundary stencil).  One warp per particle: the
+//    lanes test 32 consecutive candidates of a stencil row at a time
+//    (coalesced 16-byte loads), and a ballot compacts the hits in candidate
+//    order into the particle's list, so the list is in the reference's visit
+//    order: stencil rows in (z, y) order, inside a row the sorted particle
+//    range.  Entries are 16-bit, row << 11 | offset inside the row's range,
+//    row-major (128 entries per particle), read back 8 per 16-byte load.
+//  * k_boundary and k_governing walk their particle's list with one thread
+//    per particle, all lanes converged, loading the next four neighbours'
+//    packed data before doing their arithmetic.  The visit order is the
+//    reference's, so the order-dependent recurrence on grad(rho).x
+//    (delta_ns.cu:244-245) sees the same sequence.
+//  * The pair arithmetic uses hardware reciprocal and square-root
+//    approximations (MUFU, relative error ~1 ulp) in place of IEEE divisions;
+//    results agree with the reference to FP32 rounding, not bitwise.
 //
 // Neighbour test: the reference's q = sqrtf(r2)/h <= 2 (delta_ns.cu:67-68),
 // with r2 formed as fma(dz,dz,fma(dy,dy,dx*dx)).  Far from the threshold the
 // test is decided on r2 alone; within a relative 1e-5 of it the exact
 // IEEE sqrt and division decide, so the neighbour set is the reference's.
+//
+// Particle type: only "fluid (type 1)" vs "not fluid" enters the equations,
+// so the packed shadow stores the density with the sign bit set for
+// non-fluid particles (densities are non-negative).
 //
 // Wall densities: the reference writes them in place while neighbours read
 // them (a race, delta_ns.cu:65,130,151).  Here k_nblist extrapolates every
@@ -33,9 +46,6 @@
 namespace zsph {
 namespace {
 
-// Plain coherent loads: some shadow fields are written while the kernel runs.
-#define LDG(p) (*(p))
-
 template <int GF> struct Stencil {
   static constexpr int W = 2 * GF + 1;  // rows per z-plane
   static constexpr int NR = W * W;      // governing rows (y = -GF..GF)
@@ -45,27 +55,23 @@ template <int GF> struct Stencil {
 constexpr int kRowShift = 11;
 constexpr int kOffMask = (1 << kRowShift) - 1;
 constexpr uint8_t kOverflow = 255;
+constexpr int kListVec = kMaxNb / 8;  // uint4 per particle list
 
-// Row ranges of particle i's stencil (delta_ns.cu:39-46), into shared memory
-// columns rs/re (stride kPairBlock).
-template <int GF>
-__device__ __forceinline__ void load_rows(const KParams& kp, const zsph_tmp_t& t, int c, int* rs, int* re) {
-  const zsph_gpu_param_t& p = kp.p;
-#pragma unroll
-  for (int r = 0; r < Stencil<GF>::NR; ++r) {
-    const int z = r / Stencil<GF>::W - GF, y = r % Stencil<GF>::W - GF;
-    const int cell = c + z * kp.XY + y * p.grid_xdim;
-    const int cs = cell - GF, ce = cell + GF;
-    int s = 0, e = 0;
-    if (cs >= p.grid_hash_min && ce <= p.grid_hash_max) {
-      // bounds a caller left stale are clamped to the particle range, so no
-      // row can index outside the arrays (written bounds are always inside)
-      s = max(LDG(&t.grid_start[cs]), 0);
-      e = min(LDG(&t.grid_end[ce]), kp.n);
-    }
-    rs[r * kPairBlock] = s;
-    re[r * kPairBlock] = e;
-  }
+__device__ __forceinline__ float rcp_fast(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float sqrt_fast(float x) {
+  float r;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ bool fluid_of(float w) { return !signbit(w); }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
 }
 
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
@@ -78,18 +84,65 @@ __device__ __forceinline__ bool interacts(const KParams& kp, float rr2) {
   return __fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f;
 }
 
-// Calls f(j) for every interacting neighbour of i in visit order, from the
-// list or, if the list overflowed, by re-filtering the stencil rows.
-template <int GF, bool BOUNDARY_ONLY, class F>
-__device__ __forceinline__ void visit(const KParams& kp, const Scratch& s, int i, float4 pi, const int* rs,
-                                      const int* re, F&& f) {
+// Range [s, e) of stencil row r of a particle in cell c (delta_ns.cu:39-46),
+// clamped to the particle range so that bounds a caller left stale can never
+// index outside the arrays (bounds the search writes are always inside).
+template <int GF>
+__device__ __forceinline__ void row_range(const KParams& kp, const zsph_tmp_t& t, int c, int r, int& s, int& e) {
+  const zsph_gpu_param_t& p = kp.p;
+  const int z = r / Stencil<GF>::W - GF, y = r % Stencil<GF>::W - GF;
+  const int cell = c + z * kp.XY + y * p.grid_xdim;
+  const int cs = cell - GF, ce = cell + GF;
+  s = 0;
+  e = 0;
+  if (cs >= p.grid_hash_min && ce <= p.grid_hash_max) {
+    s = max(t.grid_start[cs], 0);
+    e = min(t.grid_end[ce], kp.n);
+  }
+}
+
+template <int GF>
+__device__ __forceinline__ void load_rows(const KParams& kp, const zsph_tmp_t& t, int c, int* rs, int* re) {
+#pragma unroll
+  for (int r = 0; r < Stencil<GF>::NR; ++r) {
+    int s, e;
+    row_range<GF>(kp, t, c, r, s, e);
+    rs[r * kPairBlock] = s;
+    re[r * kPairBlock] = e;
+  }
+}
+
+// Walks particle i's neighbours in visit order.  fetch(j) loads what the
+// arithmetic needs into a Nb record, use(nb) does the arithmetic; the list
+// is consumed 8 entries per 16-byte load and neighbours are fetched four at
+// a time ahead of their arithmetic.  Particles whose list overflowed re-filter
+// their stencil rows directly.
+template <int GF, bool BOUNDARY_ONLY, class Nb, class Fetch, class Use>
+__device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i, float4 pi, const int* rs,
+                                     const int* re, Fetch&& fetch, Use&& use) {
   const int cnt = s.nb_cnt[i];
   if (cnt != kOverflow) {
-    for (int k = 0; k < cnt; ++k) {
-      const unsigned e = s.nb[(size_t)k * kp.n + i];
-      const int r = (int)(e >> kRowShift);
-      if (BOUNDARY_ONLY && !Stencil<GF>::boundary_row(r)) continue;
-      f(rs[r * kPairBlock] + (int)(e & kOffMask));
+    const uint4* lst = reinterpret_cast<const uint4*>(s.nb) + (size_t)i * kListVec;
+    for (int k = 0; k < cnt; k += 8) {
+      const uint4 v = lst[k >> 3];
+      const unsigned wv[4] = {v.x, v.y, v.z, v.w};
+      int js[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const unsigned ent = (wv[e >> 1] >> ((e & 1) * 16)) & 0xffffu;
+        const int r = (int)(ent >> kRowShift);
+        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r));
+        js[e] = ok ? rs[r * kPairBlock] + (int)(ent & kOffMask) : -1;
+      }
+#pragma unroll
+      for (int h = 0; h < 8; h += 4) {
+        Nb nb[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) nb[e] = fetch(js[h + e] >= 0 ? js[h + e] : i);
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+          if (js[h + e] >= 0) use(nb[e]);
+      }
     }
     return;
   }
@@ -98,75 +151,92 @@ __device__ __forceinline__ void visit(const KParams& kp, const Scratch& s, int i
     const int a = rs[r * kPairBlock], b = re[r * kPairBlock];
     for (int j = a; j < b; ++j) {
       if (j == i) continue;
-      const float4 pj = LDG(&s.sh.pr[j]);
-      if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) f(j);
+      const float4 pj = s.sh.pr[j];
+      if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) use(fetch(j));
     }
   }
 }
 
-// Filters the governing stencil of each particle into its neighbour list;
-// with WALL, also extrapolates the (rho, p) of every non-fluid particle from
-// its fluid neighbours in the boundary stencil (delta_ns.cu:61-85, :116-131)
-// and publishes it in the shadows.
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Filters the governing stencil of each particle into its neighbour list,
+// one warp per particle; with WALL, also extrapolates the (rho, p) of every
+// non-fluid particle from its fluid neighbours in the boundary stencil
+// (delta_ns.cu:61-85, :116-131) and publishes it in the shadows.  The wall
+// sums are reduced across the warp (tree order instead of the reference's
+// sequential order: FP32 rounding differences only).
 template <int GF, bool WALL>
 __global__ void __launch_bounds__(kPairBlock) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
-  __shared__ int s_rs[Stencil<GF>::NR * kPairBlock];
-  __shared__ int s_re[Stencil<GF>::NR * kPairBlock];
-  const int i = blockIdx.x * kPairBlock + threadIdx.x;
-  if (i >= kp.n) return;
-  int* rs = s_rs + threadIdx.x;
-  int* re = s_re + threadIdx.x;
-  load_rows<GF>(kp, t, LDG(&t.hash[i]), rs, re);
+  constexpr int NR = Stencil<GF>::NR;
+  static_assert(NR <= 32, "one lane per stencil row");
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (kPairBlock / 32) + (threadIdx.x >> 5);
+  if (i >= kp.n) return;  // uniform per warp
+  int rs = 0, re = 0;
+  if (lane < NR) row_range<GF>(kp, t, t.hash[i], lane, rs, re);
   const float4 pi = s.sh.pr[i];
+  const bool wall = WALL && !fluid_of(pi.w);
+  uint16_t* out = s.nb + (size_t)i * kMaxNb;
+  const zsph_gpu_param_t& p = kp.p;
   int cnt = 0;
   bool ovf = false;
-  int r = 0, j = rs[0], e = re[0], base = j;
-  for (;;) {
-    while (j >= e) {
-      if (++r >= Stencil<GF>::NR) break;
-      j = rs[r * kPairBlock];
-      e = re[r * kPairBlock];
-      base = j;
-    }
-    if (r >= Stencil<GF>::NR) break;
-    if (j != i) {
-      const float4 pj = LDG(&s.sh.pr[j]);
-      if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) {
-        const int off = j - base;
-        if (cnt < kMaxNb && off <= kOffMask)
-          s.nb[(size_t)cnt * kp.n + i] = (uint16_t)((r << kRowShift) | off);
+  float rsum = 0.0f, wsum = 0.0f;
+  for (int r = 0; r < NR; ++r) {
+    const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
+    for (int k0 = a; k0 < b; k0 += 32) {
+      const int j = k0 + lane;
+      bool hit = false;
+      float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+      float dz = 0.f, rr2 = 0.f;
+      if (j < b && j != i) {
+        pj = s.sh.pr[j];
+        dz = pi.z - pj.z;
+        rr2 = dist2(pi.x - pj.x, pi.y - pj.y, dz);
+        hit = interacts(kp, rr2);
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int pos = cnt + __popc(m & lanemask_lt());
+        const int off = j - a;
+        if (pos < kMaxNb && off <= kOffMask)
+          out[pos] = (uint16_t)((r << kRowShift) | off);
         else
           ovf = true;
-        ++cnt;
+        if (WALL && wall && Stencil<GF>::boundary_row(r) && fluid_of(pj.w)) {
+          const float q = __fsqrt_rn(rr2) / p.h;
+          const float aa = 1.0f - q / 2.0f;
+          float w = aa * aa * aa;
+          w = w * aa;
+          w *= (2.0f * q + 1.0f) * p.adh;
+          const float p1 = s.sh.vp[j].w;
+          rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
+          wsum += w;
+        }
       }
+      cnt += __popc(m);
     }
-    ++j;
   }
-  if (ovf) atomicOr(s.flags, ZSPH_FLAG_NB_OVERFLOW);
-  s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
-  if (!WALL) return;
-  const int ti = s.sh.type[i];
-  if (ti == 1) return;
-  const zsph_gpu_param_t& p = kp.p;
-  float rsum = 0.0f, wsum = 0.0f;
-  visit<GF, true>(kp, s, i, pi, rs, re, [&](int jj) {
-    if (LDG(&s.sh.type[jj]) != 1) return;
-    const float4 pj = LDG(&s.sh.pr[jj]);
-    const float dz = pi.z - pj.z;
-    const float q = sqrtf(dist2(pi.x - pj.x, pi.y - pj.y, dz)) / p.h;
-    const float a = 1.0f - q / 2.0f;
-    float w = a * a * a;
-    w = w * a;
-    w *= (2.0f * q + 1.0f) * p.adh;
-    const float p1 = LDG(&s.sh.vp[jj]).w;
-    rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
-    wsum += w;
-  });
-  if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-  if (rsum < 0.0f) rsum = 0.0f;
-  s.sh.pr[i].w = rsum / p.cs2 + p.rho0;
-  s.sh.vp[i].w = rsum;
+  ovf = __any_sync(0xffffffffu, ovf) || cnt > 254;
+  if (lane == 0) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+  if (WALL && wall) {
+    rsum = warp_sum(rsum);
+    wsum = warp_sum(wsum);
+    if (lane == 0) {
+      if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+      if (rsum < 0.0f) rsum = 0.0f;
+      s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+      s.sh.vp[i].w = rsum;
+    }
+  }
 }
+
+struct NbB1 {  // boundary loop 1
+  float4 pr, vp;
+};
 
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
@@ -178,62 +248,64 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
   if (i >= kp.n) return;
   int* rs = s_rs + threadIdx.x;
   int* re = s_re + threadIdx.x;
-  load_rows<GF>(kp, t, LDG(&t.hash[i]), rs, re);
+  load_rows<GF>(kp, t, t.hash[i], rs, re);
   const zsph_gpu_param_t& p = kp.p;
   const float4 pi = s.sh.pr[i];
   const float4 vi = s.sh.vp[i];
-  const int ti = s.sh.type[i];
+  const bool fi = fluid_of(pi.w);
   const float rho_self = reinterpret_cast<const float2*>(ptc.rhop)[i].x;  // old own density
+  const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
   float Lxx = 0.f, Lxy = 0.f, Lxz = 0.f, Lyy = 0.f, Lyz = 0.f, Lzz = 0.f, divv = 0.f;
-  visit<GF, true>(kp, s, i, pi, rs, re, [&](int j) {
-    const float4 pj = LDG(&s.sh.pr[j]);
-    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    const float q = sqrtf(dist2(dx, dy, dz)) / p.h;
-    const float a = 1.0f - q / 2.0f;
-    float fr = a * a * a;
-    fr *= -5.0f * p.adh / p.h2;
-    const float tl = fr * p.m / pj.w;
-    Lxx -= dx * dx * tl; Lxy -= dx * dy * tl; Lxz -= dx * dz * tl;
-    Lyy -= dy * dy * tl; Lyz -= dy * dz * tl; Lzz -= dz * dz * tl;
-    if (ti == 1 && LDG(&s.sh.type[j]) == 1) {
-      const float4 vj = LDG(&s.sh.vp[j]);
-      const float dvdx = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
-      divv -= fr * dvdx * p.m / pj.w;
-    }
-  });
+  walk<GF, true, NbB1>(
+      kp, s, i, pi, rs, re, [&](int j) { return NbB1{s.sh.pr[j], s.sh.vp[j]}; },
+      [&](const NbB1& nb) {
+        const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+        const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
+        const float a = 1.0f - 0.5f * q;
+        const float fr = c_fr * (a * a * a);
+        const float tl = fr * m * rcp_fast(fabsf(nb.pr.w));
+        Lxx -= dx * dx * tl; Lxy -= dx * dy * tl; Lxz -= dx * dz * tl;
+        Lyy -= dy * dy * tl; Lyz -= dy * dz * tl; Lzz -= dz * dz * tl;
+        if (fi && fluid_of(nb.pr.w)) {
+          const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+          divv -= tl * dvdx;
+        }
+      });
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
                     Lxy * Lxy * Lzz;
   float M00, M01, M02, M10, M11, M12, M20, M21, M22;
   if (fabsf(det) > 1.8e-8f) {
-    M00 = (Lyy * Lzz - Lyz * Lyz) / det;
-    M01 = -1.0f * (Lxy * Lzz - Lyz * Lxz) / det;
-    M02 = (Lxy * Lyz - Lyy * Lxz) / det;
-    M10 = -1.0f * (Lxy * Lzz - Lxz * Lyz) / det;
-    M11 = (Lxx * Lzz - Lxz * Lxz) / det;
-    M12 = -1.0f * (Lxx * Lyz - Lxy * Lxz) / det;
-    M20 = (Lxy * Lyz - Lxz * Lyy) / det;
-    M21 = -1.0f * (Lxx * Lyz - Lxz * Lxy) / det;
-    M22 = (Lxx * Lyy - Lxy * Lxy) / det;
+    const float id = 1.0f / det;
+    M00 = (Lyy * Lzz - Lyz * Lyz) * id;
+    M01 = -(Lxy * Lzz - Lyz * Lxz) * id;
+    M02 = (Lxy * Lyz - Lyy * Lxz) * id;
+    M10 = -(Lxy * Lzz - Lxz * Lyz) * id;
+    M11 = (Lxx * Lzz - Lxz * Lxz) * id;
+    M12 = -(Lxx * Lyz - Lxy * Lxz) * id;
+    M20 = (Lxy * Lyz - Lxz * Lyy) * id;
+    M21 = -(Lxx * Lyz - Lxz * Lxy) * id;
+    M22 = (Lxx * Lyy - Lxy * Lxy) * id;
   } else {
     M00 = 1.f; M01 = 0.f; M02 = 0.f;
     M10 = 0.f; M11 = 1.f; M12 = 0.f;
     M20 = 0.f; M21 = 0.f; M22 = 1.f;
   }
   float gx = 0.f, gy = 0.f, gz = 0.f;
-  visit<GF, true>(kp, s, i, pi, rs, re, [&](int j) {
-    const float4 pj = LDG(&s.sh.pr[j]);
-    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    const float q = sqrtf(dist2(dx, dy, dz)) / p.h;
-    const float a = 1.0f - q / 2.0f;
-    float fr = -5.0f * p.adh * a * a * a / p.h2;
-    fr *= (pj.w - rho_self) * p.m / pj.w;
-    gx += (M00 * dx + M01 * dy + M02 * dz) * fr;
-    gy += (M10 * dx + M11 * dy + M12 * dz) * fr;
-    gz += (M20 * dx + M21 * dy + M22 * dz) * fr;
-  });
+  walk<GF, true, float4>(
+      kp, s, i, pi, rs, re, [&](int j) { return s.sh.pr[j]; },
+      [&](const float4& pj) {
+        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
+        const float a = 1.0f - 0.5f * q;
+        const float r1 = fabsf(pj.w);
+        const float fr = c_fr * (a * a * a) * ((r1 - rho_self) * m * rcp_fast(r1));
+        gx += (M00 * dx + M01 * dy + M02 * dz) * fr;
+        gy += (M10 * dx + M11 * dy + M12 * dz) * fr;
+        gz += (M20 * dx + M21 * dy + M22 * dz) * fr;
+      });
   reinterpret_cast<float4*>(t.dofv_grandrho)[i] = make_float4(gx, gy, gz, divv);
-  if (ti != 1) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(pi.w, vi.w);
+  if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
 }
 
 // time_int.cu:3-48 / :50-92 for one fluid particle, writing into `out`
@@ -286,6 +358,10 @@ __device__ __forceinline__ void integrate_one(const KParams& kp, const zsph_ptc_
   }
 }
 
+struct NbG {  // governing
+  float4 pr, vp, dg;
+};
+
 // cuda_govering_ns (delta_ns.cu:179-267); MODE 1/2 fuses the prediction /
 // correction of the same particle, written into `out` (a different buffer,
 // so neighbours still read the unintegrated state).
@@ -298,37 +374,40 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   if (i >= kp.n) return;
   int* rs = s_rs + threadIdx.x;
   int* re = s_re + threadIdx.x;
-  load_rows<GF>(kp, t, LDG(&t.hash[i]), rs, re);
+  load_rows<GF>(kp, t, t.hash[i], rs, re);
   const zsph_gpu_param_t& p = kp.p;
   const float4 pi = s.sh.pr[i];
   const float4 vi = s.sh.vp[i];
-  const int ti = s.sh.type[i];
-  const float r0 = pi.w, p0 = vi.w;
-  float4 g0 = reinterpret_cast<const float4*>(t.dofv_grandrho)[i];
+  const bool fi = fluid_of(pi.w);
+  const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
+  const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
+  const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
+  float4 g0 = dg[i];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  visit<GF, false>(kp, s, i, pi, rs, re, [&](int j) {
-    const float4 pj = LDG(&s.sh.pr[j]);
-    const float4 vj = LDG(&s.sh.vp[j]);
-    const float4 g1 = LDG(reinterpret_cast<const float4*>(t.dofv_grandrho) + j);
-    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    const float rr2 = dist2(dx, dy, dz);
-    const float dvdx = (vi.x - vj.x) * dx + (vi.y - vj.y) * dy + (vi.z - vj.z) * dz;
-    const float q = sqrtf(rr2) / p.h;
-    const float a = 1.0f - q / 2.0f;
-    const float fr = -5.0f * p.adh * a * a * a / p.h2;
-    const float r1 = pj.w, p1 = vj.w;
-    g0.x *= dx;  // order-dependent recurrence, delta_ns.cu:244-245
-    g0.x += g1.x * dx + (g0.y + g1.y) * dy + (g0.z + g1.z) * dz;
-    acc.w += r0 * dvdx * fr * p.m / r1;
-    float vt = -(p0 + p1) * p.m * fr / (r0 * r1);
-    if (ti == 1 && LDG(&s.sh.type[j]) == 1) {
-      acc.w += p.delta_h_cs * fr * ((r0 - r1) * 2.0f * rr2 / (rr2 + p.eta2) - g0.x) * p.m / r1;
-      vt += p.h_cs_rho_m * fr * (g0.w + g1.w + p.alpha * dvdx / (rr2 + p.eta2)) / (r0 * r1);
-    }
-    acc.x += vt * dx;
-    acc.y += vt * dy;
-    acc.z += vt * dz;
-  });
+  walk<GF, false, NbG>(
+      kp, s, i, pi, rs, re, [&](int j) { return NbG{s.sh.pr[j], s.sh.vp[j], dg[j]}; },
+      [&](const NbG& nb) {
+        const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+        const float rr2 = dist2(dx, dy, dz);
+        const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+        const float q = sqrt_fast(rr2) * inv_h;
+        const float a = 1.0f - 0.5f * q;
+        const float fr = c_fr * (a * a * a);
+        const float r1 = fabsf(nb.pr.w), p1 = nb.vp.w, ir1 = rcp_fast(r1);
+        g0.x *= dx;  // order-dependent recurrence, delta_ns.cu:244-245
+        g0.x += nb.dg.x * dx + (g0.y + nb.dg.y) * dy + (g0.z + nb.dg.z) * dz;
+        const float frm = fr * m * ir1;
+        acc.w += r0 * dvdx * frm;
+        float vt = -(p0 + p1) * frm * ir0;
+        if (fi && fluid_of(nb.pr.w)) {
+          const float ire = rcp_fast(rr2 + p.eta2);
+          acc.w += p.delta_h_cs * frm * ((r0 - r1) * 2.0f * rr2 * ire - g0.x);
+          vt += p.h_cs_rho_m * fr * (g0.w + nb.dg.w + p.alpha * dvdx * ire) * ir0 * ir1;
+        }
+        acc.x += vt * dx;
+        acc.y += vt * dy;
+        acc.z += vt * dz;
+      });
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
   if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(s.flags, ZSPH_FLAG_NAN);
@@ -344,13 +423,15 @@ __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc
   integrate_one<MODE>(kp, ptc, ptc, i, reinterpret_cast<const float4*>(t.acc_drhodt)[i]);
 }
 
+inline int warp_blocks(int n) { return (n + kPairBlock / 32 - 1) / (kPairBlock / 32); }
+inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
+
 template <int GF>
 cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                         cudaStream_t st, Prof* pf) {
-  const int nb = (kp.n + kPairBlock - 1) / kPairBlock;
-  k_nblist<GF, true><<<nb, kPairBlock, 0, st>>>(kp, s, t);
+  k_nblist<GF, true><<<warp_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
-  k_boundary<GF><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t);
+  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, ptc, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();
 }
@@ -358,7 +439,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
 template <int GF>
 cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t, int mode,
                          const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
-  const int nb = (kp.n + kPairBlock - 1) / kPairBlock;
+  const int nb = thread_blocks(kp.n);
   if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
   if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
   if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
@@ -368,8 +449,7 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
 
 template <int GF>
 cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
-  const int nb = (kp.n + kPairBlock - 1) / kPairBlock;
-  k_nblist<GF, false><<<nb, kPairBlock, 0, st>>>(kp, s, t);
+  k_nblist<GF, false><<<warp_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, t);
   return cudaGetLastError();
 }
 
@@ -387,7 +467,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_nb_counts(KParams kp, Scratch 
     return;
   }
   int b = 0;
-  for (int k = 0; k < cnt; ++k) b += Stencil<GF>::boundary_row((int)(s.nb[(size_t)k * kp.n + i] >> kRowShift));
+  for (int k = 0; k < cnt; ++k) b += Stencil<GF>::boundary_row((int)(s.nb[(size_t)i * kMaxNb + k] >> kRowShift));
   if (nb_boundary) nb_boundary[i] = b;
   if (nb_governing) nb_governing[i] = cnt;
 }

@@ -308,6 +308,11 @@ __device__ __forceinline__ int ranked_slot(const Scratch& sc, int t, int i, int 
   return a + r;
 }
 
+// Density with the sign bit marking a non-fluid particle (type != 1).
+__device__ __forceinline__ float packed_rho(float rho, int type) {
+  return type == 1 ? fabsf(rho) : -fabsf(rho);
+}
+
 __device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t& w, const Shadow& sh, int src,
                                            int dst) {
   const float x = o.pos[3 * src], y = o.pos[3 * src + 1], z = o.pos[3 * src + 2];
@@ -326,9 +331,8 @@ __device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t
   reinterpret_cast<float2*>(w.tmp_rhop)[dst] = trp;
   w.type[dst] = ty_;
   w.table[dst] = tb + src - dst;  // sort.cu:82
-  sh.pr[dst] = make_float4(x, y, z, rp.x);
+  sh.pr[dst] = make_float4(x, y, z, packed_rho(rp.x, ty_));
   sh.vp[dst] = make_float4(vx, vy, vz, rp.y);
-  sh.type[dst] = ty_;
 }
 
 // Fused search, last step: rank, write sorted hash/index, gather the eight
@@ -369,9 +373,8 @@ __global__ void __launch_bounds__(kSearchBlock) k_pack(KParams kp, Shadow sh, zs
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kp.n) return;
   const float2 rp = reinterpret_cast<const float2*>(s.rhop)[i];
-  sh.pr[i] = make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], rp.x);
+  sh.pr[i] = make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], packed_rho(rp.x, s.type[i]));
   sh.vp[i] = make_float4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], rp.y);
-  sh.type[i] = s.type[i];
 }
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }

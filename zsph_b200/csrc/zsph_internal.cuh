@@ -30,11 +30,11 @@ struct KParams {
 };
 
 // Packed per-particle shadows of the sorted state, written by the gather
-// (16-byte loads in the pair kernels).  pr = {x, y, z, rho}, vp = {vx, vy, vz, p}.
+// (16-byte loads in the pair kernels).  pr = {x, y, z, +-rho} with the sign
+// bit set for non-fluid particles (type != 1), vp = {vx, vy, vz, p}.
 struct Shadow {
   float4* pr;
   float4* vp;
-  int* type;
 };
 
 // Device scratch owned by a handle; allocated once in zsph_create.
@@ -50,7 +50,7 @@ struct Scratch {
   int* tile_last;    // [tiles] last occupied cell of each tile (-1 if none)
   int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length
   int* big_list;     // [kBigListCap]
-  uint16_t* nb;      // [kMaxNb * n] neighbour lists, column-major (entry k of particle i at k*n+i)
+  uint16_t* nb;      // [n * kMaxNb] neighbour lists, row-major (entry k of particle i at i*kMaxNb+k)
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
   int* flags;        // [1]   ZSPH_FLAG_* bits
   Shadow sh;
