@@ -45,7 +45,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["config1", "config0"], default="config1")
+    ap.add_argument("--workload", choices=["config1", "config0", "medium"], default="config1",
+                    help="config1: the measured case; config0: dx=0.02 (105,048 particles); medium: dx=0.0075 "
+                         "(about 1.3 M particles, for profiling captures that must stay small)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample duration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -53,6 +55,8 @@ def parse():
 
 def make_case(name):
     from zsph_b200 import cases
+    if name == "medium":
+        return cases.dam_break(0.0075, end_step=500)
     return cases.config1() if name == "config1" else cases.config0()
 
 

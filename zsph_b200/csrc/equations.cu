@@ -164,11 +164,34 @@ __device__ __forceinline__ float warp_sum(float v) {
 }
 
 // Filters the governing stencil of each particle into its neighbour list,
-// one warp per particle; with WALL, also extrapolates the (rho, p) of every
-// non-fluid particle from its fluid neighbours in the boundary stencil
-// (delta_ns.cu:61-85, :116-131) and publishes it in the shadows.  The wall
-// sums are reduced across the warp (tree order instead of the reference's
-// sequential order: FP32 rounding differences only).
+// one warp per particle, 64 candidates (two per lane) per iteration; with
+// WALL, also extrapolates the (rho, p) of every non-fluid particle from its
+// fluid neighbours in the boundary stencil (delta_ns.cu:61-85, :116-131) and
+// publishes it in the shadows.  The wall sums are reduced across the warp
+// (tree order instead of the reference's sequential order: FP32 rounding
+// differences only).
+//
+// A stencil row whose y-z slab lies farther than 2h from the particle cannot
+// hold a neighbour and is skipped (with a 0.1% margin on r^2, far above the
+// rounding of cell assignment); rows that wrap around in x (the reference's
+// linear hash aliases x overflow into the next row) are never skipped.
+template <int GF>
+__device__ __forceinline__ bool row_can_hit(const KParams& kp, int c, float4 pi, int r) {
+  const zsph_gpu_param_t& p = kp.p;
+  const int X = p.grid_xdim;
+  const int cz = c / kp.XY, cy = (c - cz * kp.XY) / X, cx = c - cz * kp.XY - cy * X;
+  if (cx - GF < 0 || cx + GF > X - 1) return true;
+  const int z = r / Stencil<GF>::W - GF, y = r % Stencil<GF>::W - GF;
+  // distance (in cell units) from the particle's actual position to the
+  // row's slab [cy+y, cy+y+1) x [cz+z, cz+z+1); zero if inside
+  const float inv_gs = 1.0f / p.grid_size;
+  const float uy = (pi.y - p.grid_ymin) * inv_gs, uz = (pi.z - p.grid_zmin) * inv_gs;
+  const float dy = fmaxf(fmaxf((float)(cy + y) - uy, uy - (float)(cy + y + 1)), 0.0f);
+  const float dz = fmaxf(fmaxf((float)(cz + z) - uz, uz - (float)(cz + z + 1)), 0.0f);
+  const float d2 = (dy * dy + dz * dz) * p.grid_size * p.grid_size;
+  return d2 <= kp.r2hi * 1.001f;
+}
+
 template <int GF, bool WALL>
 __global__ void __launch_bounds__(kPairBlock) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
@@ -176,48 +199,65 @@ __global__ void __launch_bounds__(kPairBlock) k_nblist(KParams kp, Scratch s, zs
   const int lane = threadIdx.x & 31;
   const int i = blockIdx.x * (kPairBlock / 32) + (threadIdx.x >> 5);
   if (i >= kp.n) return;  // uniform per warp
-  int rs = 0, re = 0;
-  if (lane < NR) row_range<GF>(kp, t, t.hash[i], lane, rs, re);
   const float4 pi = s.sh.pr[i];
+  const int c = t.hash[i];
+  int rs = 0, re = 0;
+  if (lane < NR) {
+    row_range<GF>(kp, t, c, lane, rs, re);
+    if (!row_can_hit<GF>(kp, c, pi, lane)) re = rs;
+  }
   const bool wall = WALL && !fluid_of(pi.w);
   uint16_t* out = s.nb + (size_t)i * kMaxNb;
   const zsph_gpu_param_t& p = kp.p;
+  const unsigned lt = lanemask_lt();
   int cnt = 0;
   bool ovf = false;
   float rsum = 0.0f, wsum = 0.0f;
   for (int r = 0; r < NR; ++r) {
     const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
-    for (int k0 = a; k0 < b; k0 += 32) {
-      const int j = k0 + lane;
-      bool hit = false;
-      float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-      float dz = 0.f, rr2 = 0.f;
-      if (j < b && j != i) {
-        pj = s.sh.pr[j];
-        dz = pi.z - pj.z;
-        rr2 = dist2(pi.x - pj.x, pi.y - pj.y, dz);
-        hit = interacts(kp, rr2);
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (hit) {
-        const int pos = cnt + __popc(m & lanemask_lt());
-        const int off = j - a;
-        if (pos < kMaxNb && off <= kOffMask)
-          out[pos] = (uint16_t)((r << kRowShift) | off);
-        else
-          ovf = true;
-        if (WALL && wall && Stencil<GF>::boundary_row(r) && fluid_of(pj.w)) {
-          const float q = __fsqrt_rn(rr2) / p.h;
-          const float aa = 1.0f - q / 2.0f;
-          float w = aa * aa * aa;
-          w = w * aa;
-          w *= (2.0f * q + 1.0f) * p.adh;
-          const float p1 = s.sh.vp[j].w;
-          rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
-          wsum += w;
+    for (int k0 = a; k0 < b; k0 += 64) {
+      bool hit[2];
+      float4 pj[2];
+      float dz[2], rr2[2];
+      int j[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        j[h] = k0 + 32 * h + lane;
+        hit[h] = false;
+        dz[h] = 0.f;
+        rr2[h] = 0.f;
+        pj[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j[h] < b && j[h] != i) {
+          pj[h] = s.sh.pr[j[h]];
+          dz[h] = pi.z - pj[h].z;
+          rr2[h] = dist2(pi.x - pj[h].x, pi.y - pj[h].y, dz[h]);
+          hit[h] = interacts(kp, rr2[h]);
         }
       }
-      cnt += __popc(m);
+      const unsigned m0 = __ballot_sync(0xffffffffu, hit[0]);
+      const unsigned m1 = __ballot_sync(0xffffffffu, hit[1]);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (hit[h]) {
+          const int pos = cnt + (h ? __popc(m0) + __popc(m1 & lt) : __popc(m0 & lt));
+          const int off = j[h] - a;
+          if (pos < kMaxNb && off <= kOffMask)
+            out[pos] = (uint16_t)((r << kRowShift) | off);
+          else
+            ovf = true;
+          if (WALL && wall && Stencil<GF>::boundary_row(r) && fluid_of(pj[h].w)) {
+            const float q = __fsqrt_rn(rr2[h]) / p.h;
+            const float aa = 1.0f - q / 2.0f;
+            float w = aa * aa * aa;
+            w = w * aa;
+            w *= (2.0f * q + 1.0f) * p.adh;
+            const float p1 = s.sh.vp[j[h]].w;
+            rsum += (p1 - pj[h].w * ((0.0f - p.g) * dz[h])) * w;
+            wsum += w;
+          }
+        }
+      }
+      cnt += __popc(m0) + __popc(m1);
     }
   }
   ovf = __any_sync(0xffffffffu, ovf) || cnt > 254;
@@ -366,7 +406,7 @@ struct NbG {  // governing
 // correction of the same particle, written into `out` (a different buffer,
 // so neighbours still read the unintegrated state).
 template <int GF, int MODE>
-__global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
+__global__ void __launch_bounds__(kPairBlock, 6) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
                                                           zsph_ptc_t out) {
   __shared__ int s_rs[Stencil<GF>::NR * kPairBlock];
   __shared__ int s_re[Stencil<GF>::NR * kPairBlock];
