@@ -16,7 +16,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libzsph_ref.so")
 
-WALLS_FIRST, WALLS_OLD = 0, 1
+WALLS_FIRST, WALLS_OLD, WALLS_SPLIT = 0, 1, 2
 _F, _I, _VP = ctypes.c_float, ctypes.c_int, ctypes.c_void_p
 
 

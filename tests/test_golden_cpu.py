@@ -65,27 +65,42 @@ def test_kernels_match_reference_on_wall_consistent_input():
     assert np.allclose(o.new["rhop"], g["rhop"], rtol=1e-6, atol=1e-3)
 
 
-def test_raw_input_reference_lies_near_the_wall_orderings():
-    """On the raw case (hydrostatic walls everywhere) the reference's result
-    depends on its schedule; fluid accelerations do not, and grad(rho) lies in
-    the range spanned by the oracle's deterministic wall orderings."""
+def test_raw_input_matches_reference_away_from_the_wall_race():
+    """On the raw case (hydrostatic walls everywhere) part of the reference's
+    result depends on its thread schedule: a neighbour read of a wall density
+    sees the old or the new value (delta_ns.cu:53,65,151 vs :130).  What does
+    not depend on it must match: the fluid accelerations (which read wall
+    densities only after the boundary kernel), and grad(rho) and drho/dt of
+    every particle with no wall within 2h (two hops for drho/dt, which reads
+    the neighbours' grad(rho)) whose density the wall pass changes."""
+    from scipy.spatial import cKDTree
     g = load("ref_kernels_dam05_raw.npz")
     c = GOLDEN_CASES["dam05"]()
-    res = {}
-    for mode in (po.WALLS_FIRST, po.WALLS_OLD, po.WALLS_SPLIT):
-        o = po.Oracle(c.json, c.state, np.float32)
-        o.search()
-        o.boundary("new", mode)
-        o.governing("new")
-        res[mode] = (o.tmp["dofv_grandrho"].copy(), o.tmp["acc_drhodt"].copy(), o.new["type"].copy())
-    fl = res[0][2] == 1
+    o = po.Oracle(c.json, c.state, np.float32)
+    o.search()
+    rho_old = o.new["rhop"][:, 0].copy()
+    o.boundary("new", po.WALLS_FIRST)
+    o.governing("new")
+    fl = o.new["type"] == 1
     acc_scale = np.abs(g["acc_drhodt"][fl, :3]).max(axis=0)
-    assert np.all(np.abs(res[0][1][fl, :3] - g["acc_drhodt"][fl, :3]).max(axis=0) <= 1e-4 * acc_scale)
-    lo = np.minimum.reduce([r[0] for r in res.values()])
-    hi = np.maximum.reduce([r[0] for r in res.values()])
-    span = (hi - lo).max(axis=0)
-    outside = np.maximum(lo - g["dofv_grandrho"], g["dofv_grandrho"] - hi)
-    assert np.all(outside.max(axis=0) <= 0.1 * span + 1e-3), (outside.max(axis=0), span)
+    assert np.all(np.abs(o.tmp["acc_drhodt"][fl, :3] - g["acc_drhodt"][fl, :3]).max(axis=0) <= 1e-4 * acc_scale)
+    racy = np.where(o.new["rhop"][:, 0] != rho_old)[0]
+    assert len(racy) > 0
+    pos = o.new["pos"].astype(np.float64)
+    reach = 2.0 * o.p.h * 1.001
+    tree = cKDTree(pos)
+    hop1 = np.zeros(len(pos), bool)
+    for lst in tree.query_ball_point(pos[racy], reach):
+        hop1[lst] = True
+    hop2 = hop1.copy()
+    for lst in tree.query_ball_point(pos[hop1], reach):
+        hop2[lst] = True
+    clean1, clean2 = ~hop1, ~hop2
+    assert clean2.sum() >= 500  # the coarse golden case is mostly within reach of a wall
+    for k, mask in (("dofv_grandrho", clean1), ("acc_drhodt", clean2)):
+        scale = np.abs(g[k]).max(axis=0) + 1e-30
+        d = np.abs(o.tmp[k][mask] - g[k][mask]).max(axis=0)
+        assert np.all(d <= 1e-4 * scale), (k, d, scale)
 
 
 def test_steps_match_reference_runs():
