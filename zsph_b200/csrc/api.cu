@@ -71,6 +71,7 @@ void fill_kparams(KParams& kp, const zsph_gpu_param_t& p, int grid_num) {
   kp.r2lo = (float)(R2 * (1.0 - 1e-5));
   kp.r2hi = (float)(R2 * (1.0 + 1e-5));
   kp.inv_h = 1.0f / p.h;
+  kp.inv_gs = 1.0f / p.grid_size;
   kp.c_fr = -5.0f * p.adh / p.h2;
 }
 

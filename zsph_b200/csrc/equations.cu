@@ -163,14 +163,6 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
-// Filters the governing stencil of each particle into its neighbour list,
-// one warp per particle, 64 candidates (two per lane) per iteration; with
-// WALL, also extrapolates the (rho, p) of every non-fluid particle from its
-// fluid neighbours in the boundary stencil (delta_ns.cu:61-85, :116-131) and
-// publishes it in the shadows.  The wall sums are reduced across the warp
-// (tree order instead of the reference's sequential order: FP32 rounding
-// differences only).
-//
 // A stencil row whose y-z slab lies farther than 2h from the particle cannot
 // hold a neighbour and is skipped (with a 0.1% margin on r^2, far above the
 // rounding of cell assignment); rows that wrap around in x (the reference's
@@ -184,93 +176,114 @@ __device__ __forceinline__ bool row_can_hit(const KParams& kp, int c, float4 pi,
   const int z = r / Stencil<GF>::W - GF, y = r % Stencil<GF>::W - GF;
   // distance (in cell units) from the particle's actual position to the
   // row's slab [cy+y, cy+y+1) x [cz+z, cz+z+1); zero if inside
-  const float inv_gs = 1.0f / p.grid_size;
-  const float uy = (pi.y - p.grid_ymin) * inv_gs, uz = (pi.z - p.grid_zmin) * inv_gs;
+  const float uy = (pi.y - p.grid_ymin) * kp.inv_gs, uz = (pi.z - p.grid_zmin) * kp.inv_gs;
   const float dy = fmaxf(fmaxf((float)(cy + y) - uy, uy - (float)(cy + y + 1)), 0.0f);
   const float dz = fmaxf(fmaxf((float)(cz + z) - uz, uz - (float)(cz + z + 1)), 0.0f);
   const float d2 = (dy * dy + dz * dz) * p.grid_size * p.grid_size;
   return d2 <= kp.r2hi * 1.001f;
 }
 
+// Wall pressure contribution of fluid neighbour j of wall particle i
+// (delta_ns.cu:67-85), with the reference's IEEE sqrt and division.
+__device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, float4 pi, int j, float& rsum,
+                                          float& wsum) {
+  const float4 pj = s.sh.pr[j];
+  if (!fluid_of(pj.w)) return;
+  const zsph_gpu_param_t& p = kp.p;
+  const float dz = pi.z - pj.z;
+  const float q = __fsqrt_rn(dist2(pi.x - pj.x, pi.y - pj.y, dz)) / p.h;
+  const float aa = 1.0f - q / 2.0f;
+  float w = aa * aa * aa;
+  w = w * aa;
+  w *= (2.0f * q + 1.0f) * p.adh;
+  const float p1 = s.sh.vp[j].w;
+  rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
+  wsum += w;
+}
+
+// Filters the governing stencil of each particle into its neighbour list,
+// one warp per particle, 32 consecutive candidates of a row per iteration;
+// the exact threshold test runs only under a warp vote, when some lane's r^2
+// lies within 1e-5 of (2h)^2.  With WALL, every non-fluid particle then
+// extrapolates its (rho, p) from the fluid neighbours of its boundary rows
+// (delta_ns.cu:61-85, :116-131), the warp reading back its finished list,
+// and publishes it in the shadows.  The wall sums are reduced across the
+// warp (tree order instead of the reference's sequential order: FP32 rounding
+// differences only).
 template <int GF, bool WALL>
 __global__ void __launch_bounds__(kPairBlock) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   static_assert(NR <= 32, "one lane per stencil row");
-  const int lane = threadIdx.x & 31;
-  const int i = blockIdx.x * (kPairBlock / 32) + (threadIdx.x >> 5);
+  __shared__ int s_rows[kPairBlock / 32][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int i = blockIdx.x * (kPairBlock / 32) + wid;
   if (i >= kp.n) return;  // uniform per warp
   const float4 pi = s.sh.pr[i];
   const int c = t.hash[i];
-  int rs = 0, re = 0;
+  int rs = 0, re = 0, rend = 0;
   if (lane < NR) {
     row_range<GF>(kp, t, c, lane, rs, re);
-    if (!row_can_hit<GF>(kp, c, pi, lane)) re = rs;
+    rend = row_can_hit<GF>(kp, c, pi, lane) ? re : rs;
   }
-  const bool wall = WALL && !fluid_of(pi.w);
   uint16_t* out = s.nb + (size_t)i * kMaxNb;
-  const zsph_gpu_param_t& p = kp.p;
   const unsigned lt = lanemask_lt();
   int cnt = 0;
   bool ovf = false;
-  float rsum = 0.0f, wsum = 0.0f;
   for (int r = 0; r < NR; ++r) {
-    const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
-    for (int k0 = a; k0 < b; k0 += 64) {
-      bool hit[2];
-      float4 pj[2];
-      float dz[2], rr2[2];
-      int j[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        j[h] = k0 + 32 * h + lane;
-        hit[h] = false;
-        dz[h] = 0.f;
-        rr2[h] = 0.f;
-        pj[h] = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (j[h] < b && j[h] != i) {
-          pj[h] = s.sh.pr[j[h]];
-          dz[h] = pi.z - pj[h].z;
-          rr2[h] = dist2(pi.x - pj[h].x, pi.y - pj[h].y, dz[h]);
-          hit[h] = interacts(kp, rr2[h]);
-        }
+    const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, rend, r);
+    for (int k0 = a; k0 < b; k0 += 32) {
+      const int j = k0 + lane;
+      const bool in = j < b && j != i;
+      const float4 pj = s.sh.pr[in ? j : i];
+      const float rr2 = dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z);
+      bool hit = in && rr2 < kp.r2lo;
+      const bool band = in && rr2 >= kp.r2lo && rr2 <= kp.r2hi;
+      if (__any_sync(0xffffffffu, band)) {
+        if (band) hit = __fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f;
       }
-      const unsigned m0 = __ballot_sync(0xffffffffu, hit[0]);
-      const unsigned m1 = __ballot_sync(0xffffffffu, hit[1]);
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        if (hit[h]) {
-          const int pos = cnt + (h ? __popc(m0) + __popc(m1 & lt) : __popc(m0 & lt));
-          const int off = j[h] - a;
-          if (pos < kMaxNb && off <= kOffMask)
-            out[pos] = (uint16_t)((r << kRowShift) | off);
-          else
-            ovf = true;
-          if (WALL && wall && Stencil<GF>::boundary_row(r) && fluid_of(pj[h].w)) {
-            const float q = __fsqrt_rn(rr2[h]) / p.h;
-            const float aa = 1.0f - q / 2.0f;
-            float w = aa * aa * aa;
-            w = w * aa;
-            w *= (2.0f * q + 1.0f) * p.adh;
-            const float p1 = s.sh.vp[j[h]].w;
-            rsum += (p1 - pj[h].w * ((0.0f - p.g) * dz[h])) * w;
-            wsum += w;
-          }
-        }
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const int pos = cnt + __popc(m & lt);
+        const int off = j - a;
+        if (pos < kMaxNb && off <= kOffMask)
+          out[pos] = (uint16_t)((r << kRowShift) | off);
+        else
+          ovf = true;
       }
-      cnt += __popc(m0) + __popc(m1);
+      cnt += __popc(m);
     }
   }
   ovf = __any_sync(0xffffffffu, ovf) || cnt > 254;
   if (lane == 0) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
-  if (WALL && wall) {
-    rsum = warp_sum(rsum);
-    wsum = warp_sum(wsum);
-    if (lane == 0) {
-      if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-      if (rsum < 0.0f) rsum = 0.0f;
-      s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-      s.sh.vp[i].w = rsum;
+  if (!WALL || fluid_of(pi.w)) return;
+  float rsum = 0.0f, wsum = 0.0f;
+  if (!ovf) {
+    s_rows[wid][lane] = rs;
+    __syncwarp();
+    for (int k = lane; k < cnt; k += 32) {
+      const unsigned e = out[k];
+      const int r = (int)(e >> kRowShift);
+      if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum);
     }
+  } else {
+    for (int r = 0; r < NR; ++r) {
+      const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
+      if (!Stencil<GF>::boundary_row(r)) continue;
+      for (int j = a + lane; j < b; j += 32) {
+        if (j == i) continue;
+        const float4 pj = s.sh.pr[j];
+        if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+      }
+    }
+  }
+  rsum = warp_sum(rsum);
+  wsum = warp_sum(wsum);
+  if (lane == 0) {
+    const zsph_gpu_param_t& p = kp.p;
+    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+    if (rsum < 0.0f) rsum = 0.0f;
+    s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+    s.sh.vp[i].w = rsum;
   }
 }
 
@@ -406,7 +419,7 @@ struct NbG {  // governing
 // correction of the same particle, written into `out` (a different buffer,
 // so neighbours still read the unintegrated state).
 template <int GF, int MODE>
-__global__ void __launch_bounds__(kPairBlock, 6) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
+__global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
                                                           zsph_ptc_t out) {
   __shared__ int s_rs[Stencil<GF>::NR * kPairBlock];
   __shared__ int s_re[Stencil<GF>::NR * kPairBlock];

@@ -26,6 +26,7 @@ struct KParams {
   int XY;                // grid_xdim * grid_ydim
   float r2lo, r2hi;      // rr2 < r2lo => q <= 2 for sure; rr2 > r2hi => q > 2 for sure
   float inv_h;
+  float inv_gs;          // 1 / grid_size
   float c_fr;            // -5 * adh / h2, the factor of grad W / r
 };
 
