@@ -131,8 +131,9 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
       for (int e = 0; e < 8; ++e) {
         const unsigned ent = (wv[e >> 1] >> ((e & 1) * 16)) & 0xffffu;
         const int r = (int)(ent >> kRowShift);
-        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r));
-        js[e] = ok ? rs[r * kPairBlock] + (int)(ent & kOffMask) : -1;
+        const int j = rs[r * kPairBlock] + (int)(ent & kOffMask);
+        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r)) && j < re[r * kPairBlock];
+        js[e] = ok ? j : -1;
       }
 #pragma unroll
       for (int h = 0; h < 8; h += 4) {
@@ -201,89 +202,174 @@ __device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, f
   wsum += w;
 }
 
-// Filters the governing stencil of each particle into its neighbour list,
-// one warp per particle, 32 consecutive candidates of a row per iteration;
-// the exact threshold test runs only under a warp vote, when some lane's r^2
-// lies within 1e-5 of (2h)^2.  With WALL, every non-fluid particle then
-// extrapolates its (rho, p) from the fluid neighbours of its boundary rows
-// (delta_ns.cu:61-85, :116-131), the warp reading back its finished list,
-// and publishes it in the shadows.  The wall sums are reduced across the
-// warp (tree order instead of the reference's sequential order: FP32 rounding
-// differences only).
+using u64 = unsigned long long;
+// Packed FP32 pairs (sm_100 f32x2 instructions): each half is rounded
+// exactly as the scalar operation, so r^2 keeps the reference's rounding.
+__device__ __forceinline__ u64 pk2(float a, float b) {
+  u64 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void upk2(u64 v, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ u64 sub2(u64 a, u64 b) {
+  u64 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ u64 mul2(u64 a, u64 b) {
+  u64 r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
+  u64 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+constexpr int kCellWarps = 4;            // cells (warps) per CTA in the list build
+constexpr int kLstStride = kMaxNb + 8;   // uint16 entries per lane row of the shared list buffer (272 bytes)
+
+// Builds the neighbour lists, one warp per grid cell and one lane per
+// particle of the cell (chunks of 32 for crowded cells).  All particles of
+// a cell share the cell's stencil rows (delta_ns.cu:39-46), so the warp
+// walks each row's candidates once: 64 candidates at a time are staged in
+// shared memory as separate x/y/z arrays and every lane tests two of them per
+// step with packed f32x2 arithmetic, collecting hit bits.  The hits are then
+// emitted in candidate order (= the reference's visit order) into a padded
+// per-lane list buffer in shared memory and written out with coalesced
+// 16-byte stores.  The exact threshold test runs only for candidates whose
+// r^2 lies within 1e-5 of (2h)^2.
+//
+// With WALL, every non-fluid particle then extrapolates its (rho, p) from
+// the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
+// summed in the reference's visit order, and publishes it in the shadows.
 template <int GF, bool WALL>
-__global__ void __launch_bounds__(kPairBlock) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
+__global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   static_assert(NR <= 32, "one lane per stencil row");
-  __shared__ int s_rows[kPairBlock / 32][32];
+  __shared__ __align__(16) float s_x[kCellWarps][64];
+  __shared__ __align__(16) float s_y[kCellWarps][64];
+  __shared__ __align__(16) float s_z[kCellWarps][64];
+  __shared__ __align__(16) uint16_t s_lst[kCellWarps][32][kLstStride];
+  __shared__ int s_rows[kCellWarps][32];
+  __shared__ int s_cnt[kCellWarps][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int i = blockIdx.x * (kPairBlock / 32) + wid;
-  if (i >= kp.n) return;  // uniform per warp
-  const float4 pi = s.sh.pr[i];
-  const int c = t.hash[i];
-  int rs = 0, re = 0, rend = 0;
-  if (lane < NR) {
-    row_range<GF>(kp, t, c, lane, rs, re);
-    rend = row_can_hit<GF>(kp, c, pi, lane) ? re : rs;
-  }
-  uint16_t* out = s.nb + (size_t)i * kMaxNb;
-  const unsigned lt = lanemask_lt();
-  int cnt = 0;
-  bool ovf = false;
-  for (int r = 0; r < NR; ++r) {
-    const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, rend, r);
-    for (int k0 = a; k0 < b; k0 += 32) {
-      const int j = k0 + lane;
-      const bool in = j < b && j != i;
-      const float4 pj = s.sh.pr[in ? j : i];
-      const float rr2 = dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z);
-      bool hit = in && rr2 < kp.r2lo;
-      const bool band = in && rr2 >= kp.r2lo && rr2 <= kp.r2hi;
-      if (__any_sync(0xffffffffu, band)) {
-        if (band) hit = __fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f;
-      }
-      const unsigned m = __ballot_sync(0xffffffffu, hit);
-      if (hit) {
-        const int pos = cnt + __popc(m & lt);
-        const int off = j - a;
-        if (pos < kMaxNb && off <= kOffMask)
-          out[pos] = (uint16_t)((r << kRowShift) | off);
-        else
-          ovf = true;
-      }
-      cnt += __popc(m);
-    }
-  }
-  ovf = __any_sync(0xffffffffu, ovf) || cnt > 254;
-  if (lane == 0) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
-  if (!WALL || fluid_of(pi.w)) return;
-  float rsum = 0.0f, wsum = 0.0f;
-  if (!ovf) {
-    s_rows[wid][lane] = rs;
-    __syncwarp();
-    for (int k = lane; k < cnt; k += 32) {
-      const unsigned e = out[k];
-      const int r = (int)(e >> kRowShift);
-      if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum);
-    }
-  } else {
+  const int c = blockIdx.x * kCellWarps + wid;
+  if (c >= kp.G) return;  // uniform per warp
+  const int ca = s.cell_lb[c], cb = s.cell_lb[c + 1];
+  if (ca >= cb) return;
+  int rs = 0, re = 0;
+  if (lane < NR) row_range<GF>(kp, t, c, lane, rs, re);
+  s_rows[wid][lane] = rs;
+  float* sx = s_x[wid];
+  float* sy = s_y[wid];
+  float* sz = s_z[wid];
+  uint16_t* lst = s_lst[wid][lane];
+  for (int p0 = ca; p0 < cb; p0 += 32) {
+    const int i = p0 + lane;
+    const bool act = i < cb;
+    const float4 pi = s.sh.pr[act ? i : p0];
+    const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
+    int cnt = 0;
+    bool ovf = false;
     for (int r = 0; r < NR; ++r) {
       const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
-      if (!Stencil<GF>::boundary_row(r)) continue;
-      for (int j = a + lane; j < b; j += 32) {
-        if (j == i) continue;
-        const float4 pj = s.sh.pr[j];
-        if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+      for (int k0 = a; k0 < b; k0 += 64) {
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = k0 + 32 * h + lane;
+          float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
+          if (j < b) q = s.sh.pr[j];
+          sx[32 * h + lane] = q.x;
+          sy[32 * h + lane] = q.y;
+          sz[32 * h + lane] = q.z;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          unsigned mh = 0u, mhb = 0u;
+#pragma unroll
+          for (int tt = 0; tt < 32; tt += 2) {
+            const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
+            const u64 y2 = *reinterpret_cast<const u64*>(&sy[32 * h + tt]);
+            const u64 z2 = *reinterpret_cast<const u64*>(&sz[32 * h + tt]);
+            const u64 dx = sub2(px, x2), dy = sub2(py, y2), dz = sub2(pz, z2);
+            const u64 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+            float r0, r1;
+            upk2(d2, r0, r1);
+            if (r0 <= kp.r2hi) mhb |= 1u << tt;
+            if (r0 < kp.r2lo) mh |= 1u << tt;
+            if (r1 <= kp.r2hi) mhb |= 2u << tt;
+            if (r1 < kp.r2lo) mh |= 2u << tt;
+          }
+          const int base = k0 + 32 * h;
+          if (i >= base && i < base + 32) {  // the particle itself
+            mh &= ~(1u << (i - base));
+            mhb &= ~(1u << (i - base));
+          }
+          if (!act) mh = mhb = 0u;
+          unsigned band = mhb & ~mh;
+          if (__any_sync(0xffffffffu, band != 0u)) {
+            while (band) {  // exact IEEE test near the threshold
+              const int bb = __ffs(band) - 1;
+              band &= band - 1;
+              const float rr2 = dist2(pi.x - sx[32 * h + bb], pi.y - sy[32 * h + bb], pi.z - sz[32 * h + bb]);
+              if (__fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f) mh |= 1u << bb;
+            }
+          }
+          while (mh) {
+            const int bb = __ffs(mh) - 1;
+            mh &= mh - 1;
+            const int off = base + bb - a;
+            if (cnt < kMaxNb && off <= kOffMask)
+              lst[cnt] = (uint16_t)((r << kRowShift) | off);
+            else
+              ovf = true;
+            ++cnt;
+          }
+        }
       }
     }
-  }
-  rsum = warp_sum(rsum);
-  wsum = warp_sum(wsum);
-  if (lane == 0) {
-    const zsph_gpu_param_t& p = kp.p;
-    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-    if (rsum < 0.0f) rsum = 0.0f;
-    s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-    s.sh.vp[i].w = rsum;
+    if (cnt > 254) ovf = true;
+    s_cnt[wid][lane] = (act && !ovf) ? cnt : 0;
+    if (WALL && act && !fluid_of(pi.w)) {
+      float rsum = 0.0f, wsum = 0.0f;
+      if (!ovf) {
+        for (int k = 0; k < cnt; ++k) {
+          const unsigned e = lst[k];
+          const int r = (int)(e >> kRowShift);
+          if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum);
+        }
+      } else {
+        for (int r = 0; r < NR; ++r) {
+          if (!Stencil<GF>::boundary_row(r)) continue;
+          int a, b;
+          row_range<GF>(kp, t, c, r, a, b);
+          for (int j = a; j < b; ++j) {
+            if (j == i) continue;
+            const float4 pj = s.sh.pr[j];
+            if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+          }
+        }
+      }
+      const zsph_gpu_param_t& p = kp.p;
+      if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+      if (rsum < 0.0f) rsum = 0.0f;
+      s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+      s.sh.vp[i].w = rsum;
+    }
+    __syncwarp();
+    // coalesced copy of the valid list prefixes: two 256-byte rows per store
+    for (int q = lane; q < 32 * (kMaxNb / 8); q += 32) {
+      const int row = q / (kMaxNb / 8), col = q % (kMaxNb / 8);
+      if (col * 8 < s_cnt[wid][row])
+        reinterpret_cast<uint4*>(s.nb + (size_t)(p0 + row) * kMaxNb)[col] =
+            *reinterpret_cast<const uint4*>(&s_lst[wid][row][col * 8]);
+    }
+    if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+    __syncwarp();
   }
 }
 
@@ -476,13 +562,13 @@ __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc
   integrate_one<MODE>(kp, ptc, ptc, i, reinterpret_cast<const float4*>(t.acc_drhodt)[i]);
 }
 
-inline int warp_blocks(int n) { return (n + kPairBlock / 32 - 1) / (kPairBlock / 32); }
+inline int cell_blocks(int G) { return (G + kCellWarps - 1) / kCellWarps; }
 inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 
 template <int GF>
 cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                         cudaStream_t st, Prof* pf) {
-  k_nblist<GF, true><<<warp_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, t);
+  k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
   k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, ptc, t);
   mark(pf, "boundary", st);
@@ -502,7 +588,7 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
 
 template <int GF>
 cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
-  k_nblist<GF, false><<<warp_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, t);
+  k_nblist<GF, false><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   return cudaGetLastError();
 }
 

@@ -368,6 +368,20 @@ __global__ void __launch_bounds__(kSearchBlock) k_gather_by_index(KParams kp, Sc
   gather_one(o, w, sc.sh, t.index[slot], slot);
 }
 
+// Exact per-cell particle ranges [cell_lb[c], cell_lb[c+1]) of an already
+// sorted key array (drop-in pair entry points, whose caller sorted the
+// particles; the fused search produces them in k_scan_cells).  Each particle
+// that starts a new key fills the offsets of the cells since the previous key.
+__global__ void __launch_bounds__(kSearchBlock) k_cell_lb(KParams kp, Scratch sc, zsph_tmp_t t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kp.n) return;
+  const int k = min(max(t.hash[i], 0), kp.G - 1);
+  const int kprev = i > 0 ? min(max(t.hash[i - 1], 0), kp.G - 1) : -1;
+  for (int c = kprev + 1; c <= k; ++c) sc.cell_lb[c] = i;
+  if (i == kp.n - 1)
+    for (int c = max(k, kprev) + 1; c <= kp.G; ++c) sc.cell_lb[c] = kp.n;
+}
+
 // Packed shadows of an unsorted-by-us state (drop-in pair entry points).
 __global__ void __launch_bounds__(kSearchBlock) k_pack(KParams kp, Shadow sh, zsph_ptc_t s) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -441,9 +455,11 @@ cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const 
   return cudaGetLastError();
 }
 
-cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st) {
+cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                        cudaStream_t st) {
   if (kp.n == 0) return cudaSuccess;
   k_pack<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s.sh, ptc);
+  k_cell_lb<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s, tmp);
   return cudaGetLastError();
 }
 

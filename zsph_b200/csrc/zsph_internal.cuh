@@ -93,7 +93,9 @@ cudaError_t launch_sort_data(const KParams& kp, const Scratch& s, int tiles, con
                              const zsph_tmp_t& tmp, cudaStream_t st);
 cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
                           const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf = nullptr);
-cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st);
+// packed shadows + exact cell ranges of a caller-sorted state (drop-in pair entry points)
+cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                        cudaStream_t st);
 
 // equations.cu
 cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
