@@ -39,7 +39,8 @@ enum {
   ZSPH_FLAG_NAN = 1,         /* non-finite acc_drhodt or density */
   ZSPH_FLAG_KILLED = 2,      /* a particle left the grid and became type 100 */
   ZSPH_FLAG_NB_OVERFLOW = 4, /* a neighbour list overflowed (handled, slower path) */
-  ZSPH_FLAG_BAD_KEY = 8      /* zsph_sort_index got a hash outside [0, grid_num) */
+  ZSPH_FLAG_BAD_KEY = 8,     /* zsph_sort_index got a hash outside [0, grid_num) */
+  ZSPH_FLAG_TIMEOUT = 16     /* a bounded wait for a shared-memory staging copy gave up (slower path taken) */
 };
 
 /* cpu_json_t (single_gpu_sph_src/header/data_structure.cuh:6-51); the three

@@ -70,6 +70,15 @@ void fill_kparams(KParams& kp, const zsph_gpu_param_t& p, int grid_num) {
   const double R2 = 4.0 * (double)p.h * (double)p.h;
   kp.r2lo = (float)(R2 * (1.0 - 1e-5));
   kp.r2hi = (float)(R2 * (1.0 + 1e-5));
+  // The reference's test q = sqrtf(r2)/h <= 2 (IEEE sqrt and division, both
+  // monotone under round-to-nearest) holds exactly for r2 <= r2max, the
+  // largest float that passes it; found here with the same float operations.
+  volatile float hh = p.h;
+  auto pass = [&](float r2) { volatile float q = std::sqrt(r2); q = q / hh; return q <= 2.0f; };
+  float t = (float)R2;
+  while (pass(t)) t = std::nextafter(t, INFINITY);
+  while (!pass(t)) t = std::nextafter(t, -INFINITY);
+  kp.r2max = t;
   kp.inv_h = 1.0f / p.h;
   kp.inv_gs = 1.0f / p.grid_size;
   kp.c_fr = -5.0f * p.adh / p.h2;
@@ -251,6 +260,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   std::memset(&h->s, 0, sizeof h->s);
   fill_kparams(h->kp, *gp, grid_num);
   cudaError_t e = cudaGetDevice(&h->device);
+  if (!e) e = init_pair_kernels();
   const size_t n = (size_t)gp->ptc_num, G = (size_t)grid_num;
   h->tiles = (grid_num + kScanTile - 1) / kScanTile;
   Scratch& s = h->s;

@@ -78,11 +78,9 @@ __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
   return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
 }
 
-__device__ __forceinline__ bool interacts(const KParams& kp, float rr2) {
-  if (rr2 > kp.r2hi) return false;
-  if (rr2 < kp.r2lo) return true;
-  return __fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f;
-}
+// The reference's neighbour test q = sqrtf(rr2)/h <= 2 (delta_ns.cu:67-68):
+// IEEE sqrt and division are monotone, so it holds exactly for rr2 <= r2max.
+__device__ __forceinline__ bool interacts(const KParams& kp, float rr2) { return rr2 <= kp.r2max; }
 
 // Range [s, e) of stencil row r of a particle in cell c (delta_ns.cu:39-46),
 // clamped to the particle range so that bounds a caller left stale can never
@@ -112,14 +110,15 @@ __device__ __forceinline__ void load_rows(const KParams& kp, const zsph_tmp_t& t
   }
 }
 
-// Walks particle i's neighbours in visit order.  fetch(j) loads what the
-// arithmetic needs into a Nb record, use(nb) does the arithmetic; the list
-// is consumed 8 entries per 16-byte load and neighbours are fetched four at
-// a time ahead of their arithmetic.  Particles whose list overflowed re-filter
-// their stencil rows directly.
+// Walks particle i's neighbours in visit order.  List entries (row r,
+// offset o) name the global particle rs[r] + o, checked against the row end
+// re[r]; what the arithmetic needs is fetched from index fb[r] + o (fb = rs
+// for the global arrays, or the row's base in a shared-memory window), four
+// neighbours ahead of their arithmetic; invalid slots fetch index fdummy.
+// Particles whose list overflowed re-filter their stencil rows directly.
 template <int GF, bool BOUNDARY_ONLY, class Nb, class Fetch, class Use>
 __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i, float4 pi, const int* rs,
-                                     const int* re, Fetch&& fetch, Use&& use) {
+                                     const int* re, const int* fb, int fdummy, Fetch&& fetch, Use&& use) {
   const int cnt = s.nb_cnt[i];
   if (cnt != kOverflow) {
     const uint4* lst = reinterpret_cast<const uint4*>(s.nb) + (size_t)i * kListVec;
@@ -130,16 +129,16 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
         const unsigned ent = (wv[e >> 1] >> ((e & 1) * 16)) & 0xffffu;
-        const int r = (int)(ent >> kRowShift);
-        const int j = rs[r * kPairBlock] + (int)(ent & kOffMask);
-        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r)) && j < re[r * kPairBlock];
-        js[e] = ok ? j : -1;
+        const int r = (int)(ent >> kRowShift), off = (int)(ent & kOffMask);
+        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r)) &&
+                        rs[r * kPairBlock] + off < re[r * kPairBlock];
+        js[e] = ok ? fb[r * kPairBlock] + off : -1;
       }
 #pragma unroll
       for (int h = 0; h < 8; h += 4) {
         Nb nb[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) nb[e] = fetch(js[h + e] >= 0 ? js[h + e] : i);
+        for (int e = 0; e < 4; ++e) nb[e] = fetch(js[h + e] >= 0 ? js[h + e] : fdummy);
 #pragma unroll
         for (int e = 0; e < 4; ++e)
           if (js[h + e] >= 0) use(nb[e]);
@@ -153,9 +152,112 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
     for (int j = a; j < b; ++j) {
       if (j == i) continue;
       const float4 pj = s.sh.pr[j];
-      if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) use(fetch(j));
+      if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) use(fetch(fb[r * kPairBlock] + (j - a)));
     }
   }
+}
+
+// ---- shared-memory neighbour windows staged with TMA bulk copies ---------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// A CTA's window: for each staged stencil row r, the union [w0, w0+len) of
+// its particles' candidate ranges, packed at offset woff in shared memory.
+// Thread 0 issues one cp.async.bulk per row and array, completing on one
+// mbarrier; every thread then waits with a bounded number of polls.
+struct WinHdr {
+  int w0[32], w1[32], woff[32], len[32];
+  unsigned long long bar;
+  int total, staged;
+};
+
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr int kWaitPolls = 1 << 22;  // bounded wait on the window barrier (each poll suspends briefly)
+
+// Computes the window of the CTA's particles over the rows selected by ROWS
+// (ROWS(r) true), copies NARR packed float4 arrays into `win` (array a at
+// win + a*cap) and rewrites fb (per-thread row bases) to shared indices.
+// Returns false (and leaves fb = rs) when the window does not fit `cap`
+// candidates or the copies did not complete in time.
+template <int NR, int NARR, class RowSel>
+__device__ bool stage_window(WinHdr& wh, float4* win, int cap, const float4* const (&src)[NARR], bool act,
+                             const int* rs, const int* re, int* fb, int* flags, RowSel rows) {
+  const int tid = threadIdx.x;
+  if (tid < NR) {
+    wh.w0[tid] = 0x7fffffff;
+    wh.w1[tid] = -1;
+  }
+  __syncthreads();
+  if (act) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      const int a = rs[r * kPairBlock], b = re[r * kPairBlock];
+      if (rows(r) && a < b) {
+        atomicMin(&wh.w0[r], a);
+        atomicMax(&wh.w1[r], b);
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int tot = 0;
+    for (int r = 0; r < NR; ++r) {
+      const int l = wh.w1[r] > wh.w0[r] ? wh.w1[r] - wh.w0[r] : 0;
+      wh.len[r] = l;
+      wh.woff[r] = tot;
+      tot += l;
+    }
+    wh.total = tot;
+    wh.staged = (tot > 0 && tot <= cap) ? 1 : 0;
+    if (wh.staged) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&wh.bar)), "r"(1) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
+  __syncthreads();
+  if (!wh.staged) return false;
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&wh.bar)),
+                 "r"((uint32_t)(wh.total * NARR * 16))
+                 : "memory");
+    for (int r = 0; r < NR; ++r)
+      if (wh.len[r] > 0)
+#pragma unroll
+        for (int a = 0; a < NARR; ++a)
+          bulk_copy(win + (size_t)a * cap + wh.woff[r], src[a] + wh.w0[r], (uint32_t)(wh.len[r] * 16), &wh.bar);
+  }
+  if (act) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r)
+      if (rows(r)) fb[r * kPairBlock] = wh.woff[r] + (rs[r * kPairBlock] - wh.w0[r]);
+  }
+  int polls = 0;
+  bool done = false;
+  while (!(done = bar_try_wait(&wh.bar, 0)) && ++polls < kWaitPolls) {
+  }
+  if (!done) {  // never expected: report, let the copies land, use the global arrays
+    atomicOr(flags, ZSPH_FLAG_TIMEOUT);
+    polls = 0;
+    while (!bar_try_wait(&wh.bar, 0) && ++polls < kWaitPolls) {
+    }
+  }
+  return __syncthreads_and(done ? 1 : 0) != 0;
 }
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -289,7 +391,7 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
         __syncwarp();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          unsigned mh = 0u, mhb = 0u;
+          unsigned mh = 0u;
 #pragma unroll
           for (int tt = 0; tt < 32; tt += 2) {
             const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
@@ -299,35 +401,31 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
             const u64 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
             float r0, r1;
             upk2(d2, r0, r1);
-            if (r0 <= kp.r2hi) mhb |= 1u << tt;
-            if (r0 < kp.r2lo) mh |= 1u << tt;
-            if (r1 <= kp.r2hi) mhb |= 2u << tt;
-            if (r1 < kp.r2lo) mh |= 2u << tt;
+            if (r0 <= kp.r2max) mh |= 1u << tt;
+            if (r1 <= kp.r2max) mh |= 2u << tt;
           }
           const int base = k0 + 32 * h;
-          if (i >= base && i < base + 32) {  // the particle itself
-            mh &= ~(1u << (i - base));
-            mhb &= ~(1u << (i - base));
-          }
-          if (!act) mh = mhb = 0u;
-          unsigned band = mhb & ~mh;
-          if (__any_sync(0xffffffffu, band != 0u)) {
-            while (band) {  // exact IEEE test near the threshold
-              const int bb = __ffs(band) - 1;
-              band &= band - 1;
-              const float rr2 = dist2(pi.x - sx[32 * h + bb], pi.y - sy[32 * h + bb], pi.z - sz[32 * h + bb]);
-              if (__fdiv_rn(__fsqrt_rn(rr2), kp.p.h) <= 2.0f) mh |= 1u << bb;
+          if (i >= base && i < base + 32) mh &= ~(1u << (i - base));  // the particle itself
+          if (!act) mh = 0u;
+          const int off0 = base - a;
+          if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
+            const unsigned ent0 = ((unsigned)r << kRowShift) | (unsigned)off0;
+            while (mh) {
+              const int bb = __ffs(mh) - 1;
+              mh &= mh - 1;
+              lst[cnt++] = (uint16_t)(ent0 + bb);
             }
-          }
-          while (mh) {
-            const int bb = __ffs(mh) - 1;
-            mh &= mh - 1;
-            const int off = base + bb - a;
-            if (cnt < kMaxNb && off <= kOffMask)
-              lst[cnt] = (uint16_t)((r << kRowShift) | off);
-            else
-              ovf = true;
-            ++cnt;
+          } else {
+            while (mh) {
+              const int bb = __ffs(mh) - 1;
+              mh &= mh - 1;
+              const int off = off0 + bb;
+              if (cnt < kMaxNb && off <= kOffMask)
+                lst[cnt] = (uint16_t)((r << kRowShift) | off);
+              else
+                ovf = true;
+              ++cnt;
+            }
           }
         }
       }
@@ -377,17 +475,47 @@ struct NbB1 {  // boundary loop 1
   float4 pr, vp;
 };
 
+constexpr int kWinCapB = 1536;  // boundary window capacity (candidates), 3x3 stencil
+constexpr int kWinCapG = 2048;  // governing window capacity (candidates), 3x3 stencil
+constexpr int kHdrBytes = (int)((sizeof(WinHdr) + 15) / 16 * 16);
+
+// Dynamic shared memory of a pair kernel: per-thread row starts, row ends
+// and fetch bases (NR columns of kPairBlock), the window header and, for the
+// 3x3 stencil, the window of NARR packed arrays.
+template <int GF> constexpr int pair_smem(int narr, int cap) {
+  return 3 * Stencil<GF>::NR * kPairBlock * 4 + kHdrBytes + (GF == 1 ? narr * cap * 16 : 0);
+}
+
+template <int GF> struct PairSmem {
+  int *rs, *re, *fb;
+  WinHdr* wh;
+  float4* win;
+  __device__ explicit PairSmem(unsigned char* dsm) {
+    constexpr int NR = Stencil<GF>::NR;
+    rs = reinterpret_cast<int*>(dsm) + threadIdx.x;
+    re = rs + NR * kPairBlock;
+    fb = re + NR * kPairBlock;
+    wh = reinterpret_cast<WinHdr*>(dsm + 3 * NR * kPairBlock * 4);
+    win = reinterpret_cast<float4*>(dsm + 3 * NR * kPairBlock * 4 + kHdrBytes);
+  }
+};
+
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
 template <int GF>
 __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
-  __shared__ int s_rs[Stencil<GF>::NR * kPairBlock];
-  __shared__ int s_re[Stencil<GF>::NR * kPairBlock];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
-  if (i >= kp.n) return;
-  int* rs = s_rs + threadIdx.x;
-  int* re = s_re + threadIdx.x;
-  load_rows<GF>(kp, t, t.hash[i], rs, re);
+  const bool act = i < kp.n;
+  if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  bool staged = false;
+  if (GF == 1) {
+    const float4* const src[2] = {s.sh.pr, s.sh.vp};
+    staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapB, src, act, sm.rs, sm.re, sm.fb, s.flags,
+                                             [](int r) { return Stencil<GF>::boundary_row(r); });
+  }
+  if (!act) return;
   const zsph_gpu_param_t& p = kp.p;
   const float4 pi = s.sh.pr[i];
   const float4 vi = s.sh.vp[i];
@@ -395,21 +523,26 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
   const float rho_self = reinterpret_cast<const float2*>(ptc.rhop)[i].x;  // old own density
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
   float Lxx = 0.f, Lxy = 0.f, Lxz = 0.f, Lyy = 0.f, Lyz = 0.f, Lzz = 0.f, divv = 0.f;
-  walk<GF, true, NbB1>(
-      kp, s, i, pi, rs, re, [&](int j) { return NbB1{s.sh.pr[j], s.sh.vp[j]}; },
-      [&](const NbB1& nb) {
-        const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
-        const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
-        const float a = 1.0f - 0.5f * q;
-        const float fr = c_fr * (a * a * a);
-        const float tl = fr * m * rcp_fast(fabsf(nb.pr.w));
-        Lxx -= dx * dx * tl; Lxy -= dx * dy * tl; Lxz -= dx * dz * tl;
-        Lyy -= dy * dy * tl; Lyz -= dy * dz * tl; Lzz -= dz * dz * tl;
-        if (fi && fluid_of(nb.pr.w)) {
-          const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
-          divv -= tl * dvdx;
-        }
-      });
+  auto use1 = [&](const NbB1& nb) {
+    const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+    const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
+    const float a = 1.0f - 0.5f * q;
+    const float fr = c_fr * (a * a * a);
+    const float tl = fr * m * rcp_fast(fabsf(nb.pr.w));
+    Lxx -= dx * dx * tl; Lxy -= dx * dy * tl; Lxz -= dx * dz * tl;
+    Lyy -= dy * dy * tl; Lyz -= dy * dz * tl; Lzz -= dz * dz * tl;
+    if (fi && fluid_of(nb.pr.w)) {
+      const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+      divv -= tl * dvdx;
+    }
+  };
+  const float4* win = sm.win;
+  if (staged)
+    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
+                         [&](int q) { return NbB1{win[q], win[kWinCapB + q]}; }, use1);
+  else
+    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
+                         [&](int q) { return NbB1{s.sh.pr[q], s.sh.vp[q]}; }, use1);
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
                     Lxy * Lxy * Lzz;
@@ -431,18 +564,20 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
     M20 = 0.f; M21 = 0.f; M22 = 1.f;
   }
   float gx = 0.f, gy = 0.f, gz = 0.f;
-  walk<GF, true, float4>(
-      kp, s, i, pi, rs, re, [&](int j) { return s.sh.pr[j]; },
-      [&](const float4& pj) {
-        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
-        const float a = 1.0f - 0.5f * q;
-        const float r1 = fabsf(pj.w);
-        const float fr = c_fr * (a * a * a) * ((r1 - rho_self) * m * rcp_fast(r1));
-        gx += (M00 * dx + M01 * dy + M02 * dz) * fr;
-        gy += (M10 * dx + M11 * dy + M12 * dz) * fr;
-        gz += (M20 * dx + M21 * dy + M22 * dz) * fr;
-      });
+  auto use2 = [&](const float4& pj) {
+    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
+    const float a = 1.0f - 0.5f * q;
+    const float r1 = fabsf(pj.w);
+    const float fr = c_fr * (a * a * a) * ((r1 - rho_self) * m * rcp_fast(r1));
+    gx += (M00 * dx + M01 * dy + M02 * dz) * fr;
+    gy += (M10 * dx + M11 * dy + M12 * dz) * fr;
+    gz += (M20 * dx + M21 * dy + M22 * dz) * fr;
+  };
+  if (staged)
+    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, [&](int q) { return win[q]; }, use2);
+  else
+    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return s.sh.pr[q]; }, use2);
   reinterpret_cast<float4*>(t.dofv_grandrho)[i] = make_float4(gx, gy, gz, divv);
   if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
 }
@@ -507,46 +642,56 @@ struct NbG {  // governing
 template <int GF, int MODE>
 __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
                                                           zsph_ptc_t out) {
-  __shared__ int s_rs[Stencil<GF>::NR * kPairBlock];
-  __shared__ int s_re[Stencil<GF>::NR * kPairBlock];
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
-  if (i >= kp.n) return;
-  int* rs = s_rs + threadIdx.x;
-  int* re = s_re + threadIdx.x;
-  load_rows<GF>(kp, t, t.hash[i], rs, re);
+  const bool act = i < kp.n;
+  if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
+  bool staged = false;
+  if (GF == 1) {
+    const float4* const src[3] = {s.sh.pr, s.sh.vp, dg};
+    staged = stage_window<Stencil<GF>::NR, 3>(*sm.wh, sm.win, kWinCapG, src, act, sm.rs, sm.re, sm.fb, s.flags,
+                                             [](int) { return true; });
+  }
+  if (!act) return;
   const zsph_gpu_param_t& p = kp.p;
   const float4 pi = s.sh.pr[i];
   const float4 vi = s.sh.vp[i];
   const bool fi = fluid_of(pi.w);
   const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
-  const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
   float4 g0 = dg[i];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-  walk<GF, false, NbG>(
-      kp, s, i, pi, rs, re, [&](int j) { return NbG{s.sh.pr[j], s.sh.vp[j], dg[j]}; },
-      [&](const NbG& nb) {
-        const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
-        const float rr2 = dist2(dx, dy, dz);
-        const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
-        const float q = sqrt_fast(rr2) * inv_h;
-        const float a = 1.0f - 0.5f * q;
-        const float fr = c_fr * (a * a * a);
-        const float r1 = fabsf(nb.pr.w), p1 = nb.vp.w, ir1 = rcp_fast(r1);
-        g0.x *= dx;  // order-dependent recurrence, delta_ns.cu:244-245
-        g0.x += nb.dg.x * dx + (g0.y + nb.dg.y) * dy + (g0.z + nb.dg.z) * dz;
-        const float frm = fr * m * ir1;
-        acc.w += r0 * dvdx * frm;
-        float vt = -(p0 + p1) * frm * ir0;
-        if (fi && fluid_of(nb.pr.w)) {
-          const float ire = rcp_fast(rr2 + p.eta2);
-          acc.w += p.delta_h_cs * frm * ((r0 - r1) * 2.0f * rr2 * ire - g0.x);
-          vt += p.h_cs_rho_m * fr * (g0.w + nb.dg.w + p.alpha * dvdx * ire) * ir0 * ir1;
-        }
-        acc.x += vt * dx;
-        acc.y += vt * dy;
-        acc.z += vt * dz;
-      });
+  auto use = [&](const NbG& nb) {
+    const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+    const float rr2 = dist2(dx, dy, dz);
+    const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+    const float q = sqrt_fast(rr2) * inv_h;
+    const float a = 1.0f - 0.5f * q;
+    const float fr = c_fr * (a * a * a);
+    const float r1 = fabsf(nb.pr.w), p1 = nb.vp.w, ir1 = rcp_fast(r1);
+    g0.x *= dx;  // order-dependent recurrence, delta_ns.cu:244-245
+    g0.x += nb.dg.x * dx + (g0.y + nb.dg.y) * dy + (g0.z + nb.dg.z) * dz;
+    const float frm = fr * m * ir1;
+    acc.w += r0 * dvdx * frm;
+    float vt = -(p0 + p1) * frm * ir0;
+    if (fi && fluid_of(nb.pr.w)) {
+      const float ire = rcp_fast(rr2 + p.eta2);
+      acc.w += p.delta_h_cs * frm * ((r0 - r1) * 2.0f * rr2 * ire - g0.x);
+      vt += p.h_cs_rho_m * fr * (g0.w + nb.dg.w + p.alpha * dvdx * ire) * ir0 * ir1;
+    }
+    acc.x += vt * dx;
+    acc.y += vt * dy;
+    acc.z += vt * dz;
+  };
+  const float4* win = sm.win;
+  if (staged)
+    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
+                         [&](int q) { return NbG{win[q], win[kWinCapG + q], win[2 * kWinCapG + q]}; }, use);
+  else
+    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
+                         [&](int q) { return NbG{s.sh.pr[q], s.sh.vp[q], dg[q]}; }, use);
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
   if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(s.flags, ZSPH_FLAG_NAN);
@@ -570,7 +715,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
                         cudaStream_t st, Prof* pf) {
   k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
-  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, 0, st>>>(kp, s, ptc, t);
+  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(2, kWinCapB), st>>>(kp, s, ptc, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();
 }
@@ -579,9 +724,10 @@ template <int GF>
 cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t, int mode,
                          const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
   const int nb = thread_blocks(kp.n);
-  if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
-  if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
-  if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, out);
+  const int sm = pair_smem<GF>(3, kWinCapG);
+  if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
+  if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
+  if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
   mark(pf, "governing", st);
   return cudaGetLastError();
 }
@@ -612,6 +758,22 @@ __global__ void __launch_bounds__(kSearchBlock) k_nb_counts(KParams kp, Scratch 
 }
 
 }  // namespace
+
+cudaError_t init_pair_kernels() {
+  cudaError_t e = cudaSuccess;
+  auto setb = [&](auto fn, int bytes) {
+    if (!e) e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  };
+  setb(k_boundary<1>, pair_smem<1>(2, kWinCapB));
+  setb(k_boundary<2>, pair_smem<2>(2, kWinCapB));
+  setb(k_governing<1, 0>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<1, 1>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<1, 2>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<2, 0>, pair_smem<2>(3, kWinCapG));
+  setb(k_governing<2, 1>, pair_smem<2>(3, kWinCapG));
+  setb(k_governing<2, 2>, pair_smem<2>(3, kWinCapG));
+  return e;
+}
 
 cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                             cudaStream_t st, Prof* pf) {

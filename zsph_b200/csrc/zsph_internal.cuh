@@ -25,6 +25,7 @@ struct KParams {
   int G;                 // cells
   int XY;                // grid_xdim * grid_ydim
   float r2lo, r2hi;      // rr2 < r2lo => q <= 2 for sure; rr2 > r2hi => q > 2 for sure
+  float r2max;           // q = sqrtf(rr2)/h <= 2 exactly when rr2 <= r2max (IEEE, monotone)
   float inv_h;
   float inv_gs;          // 1 / grid_size
   float c_fr;            // -5 * adh / h2, the factor of grad W / r
@@ -100,6 +101,8 @@ cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
 // equations.cu
 cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                             cudaStream_t st, Prof* pf = nullptr);
+// one-time kernel attributes (shared-memory windows above 48 KB); call before launches
+cudaError_t init_pair_kernels();
 // mode 0: acc_drhodt only; 1: + prediction into out; 2: + correction into out
 cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                              int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr);
