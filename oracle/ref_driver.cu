@@ -14,6 +14,8 @@
 #include "equation.cuh"
 #include "lib.cuh"
 
+#include <sstream>
+
 __constant__ gpu_param_t par;
 __constant__ gpu_tmp_t tmp_data;
 
@@ -89,7 +91,11 @@ static void to_param(const rcase_t* c, cpu_param_t* cp) {
   j.dt = c->dt; j.start_step = 0; j.current_step = 0; j.end_step = 0; j.output_step = 1;
   j.ptc_num = c->ptc_num; j.water_ptc_num = 0; j.air_ptc_num = 0; j.wall_ptc_num = 0; j.rigid_ptc_num = 0;
   j.thread_num = 1; j.gpu_id = 0;
+  // the reference's host code prints banners to stdout; keep stdout for the caller
+  std::ostringstream sink;
+  std::streambuf* prev = std::cout.rdbuf(sink.rdbuf());
   set_cpu_param(cp, &j);  // reference host derivation (exits on dt > dt_max; callers pre-check)
+  std::cout.rdbuf(prev);
 }
 
 // Derived constants as the reference computes them.

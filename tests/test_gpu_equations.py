@@ -37,8 +37,11 @@ def _close(gpu, ref32, ref64, what):
     assert d <= KERNEL_RTOL * scale, f"{what}: max|gpu-oracle32| = {d:.3e}, scale {scale:.3e}"
 
 
+@pytest.mark.parametrize("stage", ["0", "1"], ids=["global", "smem_windows"])
 @pytest.mark.parametrize("mk", [lambda: cases.small(0.04), cases.config0, lambda: cases.random_cloud(6000, 2)])
-def test_boundary_and_governing_match_oracle(mk):
+def test_boundary_and_governing_match_oracle(mk, stage, monkeypatch):
+    # stage=1: neighbour windows staged in shared memory by TMA bulk copies
+    monkeypatch.setenv("ZSPH_STAGE_WINDOWS", stage)
     c = mk()
     sol, o32, o64 = _sorted_pair(c)
     sol.boundary("new")

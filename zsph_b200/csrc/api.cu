@@ -14,6 +14,7 @@
 // index, cell bounds, acc_drhodt and dofv_grandrho; new_ is scratch.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -82,6 +83,11 @@ void fill_kparams(KParams& kp, const zsph_gpu_param_t& p, int grid_num) {
   kp.inv_h = 1.0f / p.h;
   kp.inv_gs = 1.0f / p.grid_size;
   kp.c_fr = -5.0f * p.adh / p.h2;
+  // Shared-memory neighbour windows (TMA) are off by default: at 112 KB per
+  // 128-particle CTA they limit the pair kernels to 8 warps per SM, which
+  // measured slower than L1-cached global loads at 20 warps per SM.
+  const char* sw = std::getenv("ZSPH_STAGE_WINDOWS");
+  kp.stage_windows = (sw && sw[0] == '1') ? 1 : 0;
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
   const bool act = i < kp.n;
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   bool staged = false;
-  if (GF == 1) {
+  if (GF == 1 && kp.stage_windows) {
     const float4* const src[2] = {s.sh.pr, s.sh.vp};
     staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapB, src, act, sm.rs, sm.re, sm.fb, s.flags,
                                              [](int r) { return Stencil<GF>::boundary_row(r); });
@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
   bool staged = false;
-  if (GF == 1) {
+  if (GF == 1 && kp.stage_windows) {
     const float4* const src[3] = {s.sh.pr, s.sh.vp, dg};
     staged = stage_window<Stencil<GF>::NR, 3>(*sm.wh, sm.win, kWinCapG, src, act, sm.rs, sm.re, sm.fb, s.flags,
                                              [](int) { return true; });
@@ -715,7 +715,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
                         cudaStream_t st, Prof* pf) {
   k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
-  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(2, kWinCapB), st>>>(kp, s, ptc, t);
+  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(kp.stage_windows ? 2 : 0, kWinCapB), st>>>(kp, s, ptc, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();
 }
@@ -724,7 +724,7 @@ template <int GF>
 cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t, int mode,
                          const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
   const int nb = thread_blocks(kp.n);
-  const int sm = pair_smem<GF>(3, kWinCapG);
+  const int sm = pair_smem<GF>(kp.stage_windows ? 3 : 0, kWinCapG);
   if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
   if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
   if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);

@@ -29,6 +29,7 @@ struct KParams {
   float inv_h;
   float inv_gs;          // 1 / grid_size
   float c_fr;            // -5 * adh / h2, the factor of grad W / r
+  int stage_windows;     // 1: pair kernels stage neighbour windows in shared memory (TMA bulk copies)
 };
 
 // Packed per-particle shadows of the sorted state, written by the gather
