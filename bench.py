@@ -73,7 +73,8 @@ class Dist:
             backend = "nccl" if torch.cuda.is_available() else "gloo"
             if torch.cuda.is_available():
                 torch.cuda.set_device(self.local)
-            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+            tmo = float(os.environ.get("ZSPH_PG_TIMEOUT", "300"))
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=tmo))
             self.pg = True
 
     def barrier(self):
