@@ -149,6 +149,17 @@ int zsph_hash(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, vo
 /* cuda_sort_index (single_gpu_sph_src/lib/sort.cu:3-6): stable ascending
  * sort of tmp->hash carrying tmp->index.  Keys must lie in [0, grid_num). */
 int zsph_sort_index(zsph_handle_t* h, const zsph_tmp_t* tmp, void* stream);
+/* No counterpart in the reference.  The same stable sort as zsph_sort_index
+ * for callers that cannot allocate device memory: it needs no handle (whose
+ * creation calls cudaMalloc) and calls no allocator.  Its scratch is a fixed
+ * static device array of about 3.2 MB, held by every GPU that loads the
+ * library until the process exits, so it accepts at most 131072 particles
+ * (gparam->ptc_num) and 131072 cells (grid_num) and returns ZSPH_EINVAL
+ * beyond that.  The first call on a device looks up the array's address
+ * (cudaGetSymbolAddress); make that call before any stream capture.  All
+ * calls share the array: calls whose work overlaps on the GPU race.  Errors
+ * are reported through zsph_last_error(NULL, ...). */
+int zsph_sort_index_noalloc(const zsph_gpu_param_t* gparam, int grid_num, const zsph_tmp_t* tmp, void* stream);
 /* cuda_sort_data (single_gpu_sph_src/lib/sort.cu:8-84): grid_start/grid_end
  * from the sorted keys (with the reference's end-of-array rules) and the
  * gather of all eight particle arrays from old_ into new_. */

@@ -114,6 +114,7 @@ _sig = {
     "zsph_set_params": (_I, [_HP, ctypes.POINTER(GpuParam)]),
     "zsph_hash": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
     "zsph_sort_index": (_I, [_HP, ctypes.POINTER(Tmp), _VP]),
+    "zsph_sort_index_noalloc": (_I, [ctypes.POINTER(GpuParam), _I, ctypes.POINTER(Tmp), _VP]),
     "zsph_sort_data": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
     "zsph_neighbor_search": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
     "zsph_boundary": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),

@@ -146,6 +146,10 @@ cudaError_t step_launches(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t&
 
 }  // namespace
 
+namespace zsph {
+void record_library_error(const std::string& msg) { set_err(nullptr, ZSPH_OK, msg); }
+}  // namespace zsph
+
 extern "C" {
 
 const char* zsph_version(void) { return "zsph-b200 0.1 (sm_100a)"; }

@@ -88,6 +88,9 @@ struct Handle {
   std::string err;
 };
 
+// api.cu: message returned by zsph_last_error(NULL, ...)
+void record_library_error(const std::string& msg);
+
 // search.cu
 cudaError_t launch_hash(const KParams& kp, int* flags, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp, cudaStream_t st);
 cudaError_t launch_sort_index(const KParams& kp, const Scratch& s, int tiles, const zsph_tmp_t& tmp, cudaStream_t st);
