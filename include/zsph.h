@@ -34,6 +34,11 @@ enum {
   ZSPH_ENOMEM = 6    /* device allocation failed */
 };
 
+/* Equation sets (zsph_set_equations): the reference builds deltasph with
+ * -DZSPH_DELTA (equation/delta_ns.cu) and simplesph with -DZSPH_SIMPLE
+ * (equation/simple_ns.cu) from the same sources. */
+enum { ZSPH_EQ_DELTA = 0, ZSPH_EQ_SIMPLE = 1 };
+
 /* Bits of the device status word (zsph_status). */
 enum {
   ZSPH_FLAG_NAN = 1,         /* non-finite acc_drhodt or density */
@@ -141,6 +146,11 @@ void zsph_destroy(zsph_handle_t* h);
 /* Replaces the constants (dt and physics) of an existing handle; the grid
  * and particle count must not change. */
 int zsph_set_params(zsph_handle_t* h, const zsph_gpu_param_t* gparam);
+
+/* Selects the equations of zsph_boundary, zsph_governing, zsph_step and
+ * zsph_run: ZSPH_EQ_DELTA (default; equation/delta_ns.cu) or ZSPH_EQ_SIMPLE
+ * (equation/simple_ns.cu, whose div(v) is the scalar tmp->dofv). */
+int zsph_set_equations(zsph_handle_t* h, int equations);
 
 /* cuda_ptc_hash (single_gpu_sph_src/lib/hash.cu:3-26): cell hash of every
  * particle into tmp->hash, identity into tmp->index, out-of-grid particles

@@ -15,13 +15,20 @@ if [ ! -d "$SG" ]; then
   echo "reference sources not found at $SG; oracle/_ref not built" >&2
   exit 0
 fi
-mkdir -p "$OUT/obj"
 NVCC=${NVCC:-nvcc}
 ARCH="-gencode arch=compute_100a,code=sm_100a"
-FLAGS="-std=c++17 -rdc=true $ARCH -lineinfo -maxrregcount 64 -Xcompiler -fPIC -D__STD_HEADER_CUH__ -DZSPH_DELTA -include $HERE/ref_shim.cuh -I $SG/header"
-for f in lib/hash.cu lib/sort.cu equation/delta_ns.cu lib/time_int.cu lib/init.cu lib/check.cu; do
-  "$NVCC" $FLAGS -c "$SG/$f" -o "$OUT/obj/$(basename "$f" .cu).o"
-done
-"$NVCC" $FLAGS -c "$HERE/ref_driver.cu" -o "$OUT/obj/ref_driver.o"
-"$NVCC" -shared -rdc=true $ARCH -Xcompiler -fPIC "$OUT"/obj/*.o -o "$OUT/libzsph_ref.so"
-echo "built $OUT/libzsph_ref.so"
+# deltasph (-DZSPH_DELTA, delta_ns.cu) and simplesph (-DZSPH_SIMPLE, simple_ns.cu),
+# as the reference's two CMake targets select them
+build() {
+  local macro=$1 eqfile=$2 lib=$3 obj="$OUT/obj_$3"
+  mkdir -p "$obj"
+  local FLAGS="-std=c++17 -rdc=true $ARCH -lineinfo -maxrregcount 64 -Xcompiler -fPIC -D__STD_HEADER_CUH__ -D$macro -include $HERE/ref_shim.cuh -I $SG/header"
+  for f in lib/hash.cu lib/sort.cu "$eqfile" lib/time_int.cu lib/init.cu lib/check.cu; do
+    "$NVCC" $FLAGS -c "$SG/$f" -o "$obj/$(basename "$f" .cu).o"
+  done
+  "$NVCC" $FLAGS -c "$HERE/ref_driver.cu" -o "$obj/ref_driver.o"
+  "$NVCC" -shared -rdc=true $ARCH -Xcompiler -fPIC "$obj"/*.o -o "$OUT/$lib.so"
+  echo "built $OUT/$lib.so"
+}
+build ZSPH_DELTA equation/delta_ns.cu libzsph_ref
+build ZSPH_SIMPLE equation/simple_ns.cu libzsph_ref_simple

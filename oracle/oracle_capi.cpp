@@ -85,6 +85,15 @@ int oracle_max_threads(void) { return omp_get_max_threads(); }
   }                                                                                                 \
   void oracle_neighbor_count_##SUF(const Params* p, const State<T>* s, const Tmp<T>* t, int ylast, int* out) { \
     neighbor_count<T>(*p, *s, *t, ylast, out);                                                      \
+  }                                                                                                 \
+  void oracle_boundary_simple_##SUF(const Params* p, State<T>* s, Tmp<T>* t, T* dofv) {             \
+    boundary_simple<T>(*p, *s, dofv, *t);                                                           \
+  }                                                                                                 \
+  void oracle_governing_simple_##SUF(const Params* p, const State<T>* s, Tmp<T>* t, const T* dofv) { \
+    governing_simple<T>(*p, *s, dofv, *t);                                                          \
+  }                                                                                                 \
+  void oracle_step_simple_##SUF(const Params* p, State<T>* o, State<T>* w, Tmp<T>* t, T* dofv, int nsteps) { \
+    for (int k = 0; k < nsteps; ++k) step_simple<T>(*p, *o, *w, *t, dofv);                          \
   }
 
 ORACLE_INSTANCE(f32, float)

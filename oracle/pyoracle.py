@@ -15,6 +15,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libzsph_ref.so")
+REF_SIMPLE_SO = os.path.join(HERE, "_ref", "libzsph_ref_simple.so")
 
 WALLS_FIRST, WALLS_OLD, WALLS_SPLIT = 0, 1, 2
 _F, _I, _VP = ctypes.c_float, ctypes.c_int, ctypes.c_void_p
@@ -150,6 +151,25 @@ class Oracle:
         self._fn("step")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
                          ctypes.byref(self._t), _I(nsteps), _I(wall_mode))
 
+    # simple-SPH equations (the reference's simplesph target); div(v) is the
+    # scalar array self.dofv
+    def _dofv(self):
+        if not hasattr(self, "dofv"):
+            self.dofv = np.zeros(self.p.ptc_num, self.dtype)
+        return self.dofv
+
+    def boundary_simple(self, which="new"):
+        self._fn("boundary_simple")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
+                                    _p(self._dofv()))
+
+    def governing_simple(self, which="new"):
+        self._fn("governing_simple")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
+                                     _p(self._dofv()))
+
+    def step_simple(self, nsteps=1):
+        self._fn("step_simple")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
+                                ctypes.byref(self._t), _p(self._dofv()), _I(nsteps))
+
     def neighbor_count(self, which="new", stencil="governing") -> np.ndarray:
         out = np.zeros(self.p.ptc_num, np.int32)
         ylast = self.p.grid_factor if stencil == "governing" else self.p.grid_factor - 1
@@ -174,32 +194,33 @@ class RState(ctypes.Structure):
 
 class RTmp(ctypes.Structure):
     _fields_ = [(n, _VP) for n in ("acc_drhodt", "dofv_grandrho", "index", "hash", "grid_start", "grid_end",
-                                   "nb_boundary", "nb_governing")]
+                                   "nb_boundary", "nb_governing", "dofv")]
 
 
-_ref = None
+_ref = {}
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_SO)
+def ref_available(simple: bool = False) -> bool:
+    return os.path.exists(REF_SIMPLE_SO if simple else REF_SO)
 
 
-def ref_lib() -> ctypes.CDLL:
-    global _ref
-    if _ref is None:
-        _ref = ctypes.CDLL(REF_SO)
-        _ref.ref_substep.restype = _I
-        _ref.ref_run.restype = _I
-        _ref.ref_params.restype = _I
-        _ref.ref_last_error.restype = ctypes.c_char_p
-    return _ref
+def ref_lib(simple: bool = False) -> ctypes.CDLL:
+    """The reference build: deltasph (default) or simplesph (simple=True)."""
+    if simple not in _ref:
+        lib_ = ctypes.CDLL(REF_SIMPLE_SO if simple else REF_SO)
+        lib_.ref_substep.restype = _I
+        lib_.ref_run.restype = _I
+        lib_.ref_params.restype = _I
+        lib_.ref_last_error.restype = ctypes.c_char_p
+        _ref[simple] = lib_
+    return _ref[simple]
 
 
-def ref_params(json):
+def ref_params(json, simple: bool = False):
     from zsph_b200 import GpuParam  # same field layout as the reference's gpu_param_t
     gp = GpuParam()
     G = _I(0)
-    ref_lib().ref_params(ctypes.byref(case_of(json)), ctypes.byref(gp), ctypes.byref(G))
+    ref_lib(simple).ref_params(ctypes.byref(case_of(json)), ctypes.byref(gp), ctypes.byref(G))
     return gp, G.value
 
 
@@ -218,33 +239,35 @@ def _rout(n, G):
     tmp = dict(acc_drhodt=np.zeros((n, 4), np.float32), dofv_grandrho=np.zeros((n, 4), np.float32),
                index=np.zeros(n, np.int32), hash=np.zeros(n, np.int32), grid_start=np.zeros(G, np.int32),
                grid_end=np.zeros(G, np.int32), nb_boundary=np.zeros(n, np.int32),
-               nb_governing=np.zeros(n, np.int32))
+               nb_governing=np.zeros(n, np.int32), dofv=np.zeros(n, np.float32))
     return out, tmp, RState(*[_p(out[k]) for k, _ in RState._fields_]), RTmp(*[_p(tmp[k]) for k, _ in RTmp._fields_])
 
 
-def ref_substep(json, state, stage: int):
+def ref_substep(json, state, stage: int, simple: bool = False):
     """Runs the reference's kernels of one predictor sub-step up to `stage`
     (1 hash, 2 sort_index, 3 sort_data, 4 boundary, 5 governing, 6 prediction)."""
-    _, G = ref_params(json)
+    _, G = ref_params(json, simple)
     n = int(json.ptc_num)
     arrs, rin = _rstate(state, n)
     out, tmp, rout, rtmp = _rout(n, G)
     c = case_of(json)
-    rc = ref_lib().ref_substep(ctypes.byref(c), ctypes.byref(rin), _I(stage), ctypes.byref(rout), ctypes.byref(rtmp))
+    lib_ = ref_lib(simple)
+    rc = lib_.ref_substep(ctypes.byref(c), ctypes.byref(rin), _I(stage), ctypes.byref(rout), ctypes.byref(rtmp))
     if rc:
-        raise RuntimeError(ref_lib().ref_last_error().decode())
+        raise RuntimeError(lib_.ref_last_error().decode())
     return out, tmp
 
 
-def ref_run(json, state, nsteps: int, warmup: int = 0):
+def ref_run(json, state, nsteps: int, warmup: int = 0, simple: bool = False):
     """Runs `warmup + nsteps` full reference steps; returns (OLD state, tmp, ms/step of the last nsteps)."""
-    _, G = ref_params(json)
+    _, G = ref_params(json, simple)
     n = int(json.ptc_num)
     arrs, rin = _rstate(state, n)
     out, tmp, rout, rtmp = _rout(n, G)
     ms = ctypes.c_float(0.0)
-    rc = ref_lib().ref_run(ctypes.byref(case_of(json)), ctypes.byref(rin), _I(warmup), _I(nsteps), ctypes.byref(rout),
-                           ctypes.byref(rtmp), ctypes.byref(ms))
+    lib_ = ref_lib(simple)
+    rc = lib_.ref_run(ctypes.byref(case_of(json)), ctypes.byref(rin), _I(warmup), _I(nsteps), ctypes.byref(rout),
+                      ctypes.byref(rtmp), ctypes.byref(ms))
     if rc:
-        raise RuntimeError(ref_lib().ref_last_error().decode())
+        raise RuntimeError(lib_.ref_last_error().decode())
     return out, tmp, float(ms.value)

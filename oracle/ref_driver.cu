@@ -14,6 +14,7 @@
 #include "equation.cuh"
 #include "lib.cuh"
 
+#include <cstring>
 #include <sstream>
 
 __constant__ gpu_param_t par;
@@ -69,6 +70,7 @@ typedef struct {
   float *acc_drhodt, *dofv_grandrho;  // 4 per particle
   int *index, *hash, *grid_start, *grid_end;
   int *nb_boundary, *nb_governing;  // neighbour counts (may be null)
+  float* dofv;                      // scalar div(v) of the simple equations (may be null)
 } rtmp_t;
 
 static int g_err = 0;
@@ -120,6 +122,7 @@ struct Session {
 };
 
 static int open_session(const rcase_t* c, const rstate_t* in, Session& s) {
+  memset(&s.tmp, 0, sizeof s.tmp);  // alloc_gpu_tmp_data sets dofv_grandrho or dofv, by build
   to_param(c, &s.cp);
   set_gpu_param(&s.gp, &s.cp);
   const int n = s.cp.ptc_num;
@@ -155,7 +158,8 @@ static void close_session(Session& s) {
   delete_gpu_ptc_data(&s.old_);
   delete_gpu_ptc_data(&s.new_);
   cudaFree(s.tmp.acc_drhodt);
-  cudaFree(s.tmp.dofv_grandrho);
+  if (s.tmp.dofv_grandrho) cudaFree(s.tmp.dofv_grandrho);
+  if (s.tmp.dofv) cudaFree(s.tmp.dofv);
   cudaFree(s.tmp.hash);
   cudaFree(s.tmp.index);
   cudaFree(s.tmp.grid_start);
@@ -177,7 +181,9 @@ static int copy_out(Session& s, const gpu_ptc_t& src, rstate_t* out, rtmp_t* t) 
   }
   if (t) {
     if (!e && t->acc_drhodt) e = cudaMemcpy(t->acc_drhodt, s.tmp.acc_drhodt, n * sizeof(float4), cudaMemcpyDeviceToHost);
-    if (!e && t->dofv_grandrho) e = cudaMemcpy(t->dofv_grandrho, s.tmp.dofv_grandrho, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (!e && t->dofv_grandrho && s.tmp.dofv_grandrho)
+      e = cudaMemcpy(t->dofv_grandrho, s.tmp.dofv_grandrho, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    if (!e && t->dofv && s.tmp.dofv) e = cudaMemcpy(t->dofv, s.tmp.dofv, n * sizeof(float), cudaMemcpyDeviceToHost);
     if (!e && t->index) e = cudaMemcpy(t->index, s.tmp.index, n * sizeof(int), cudaMemcpyDeviceToHost);
     if (!e && t->hash) e = cudaMemcpy(t->hash, s.tmp.hash, n * sizeof(int), cudaMemcpyDeviceToHost);
     if (!e && t->grid_start) e = cudaMemcpy(t->grid_start, s.tmp.grid_start, G * sizeof(int), cudaMemcpyDeviceToHost);

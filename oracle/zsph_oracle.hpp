@@ -428,4 +428,92 @@ template <class T> void neighbor_count(const Params& p, const State<T>& s, const
   }
 }
 
+
+// ---- simple-SPH equations (the reference's simplesph target) ---------------
+
+// single_gpu_sph_src/equation/simple_ns.cu:3-97 (cuda_boundary_ns of the
+// simple equations): wall pressure from fluid neighbours and the scalar
+// div(v) = -sum F (v_ij . x_ij) m / rho_j over fluid pairs, one loop over the
+// boundary stencil rows.  Walls read only fluid densities, so the in-place
+// wall write (:94) has no reader in this kernel.
+template <class T> void boundary_simple(const Params& p, State<T>& s, T* dofv, const Tmp<T>& t) {
+  const int n = p.ptc_num;
+  std::vector<T> rho_new(n), p_new(n);
+  wall_pressure(p, s, t, rho_new, p_new);
+  const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    T dv_sum = 0;
+    const T px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
+    const T vx = s.vel[3 * i], vy = s.vel[3 * i + 1], vz = s.vel[3 * i + 2];
+    const int ti = s.type[i];
+    for_each_candidate(p, t, i, p.grid_factor - 1, [&](int j) {
+      const T dx = px - s.pos[3 * j], dy = py - s.pos[3 * j + 1], dz = pz - s.pos[3 * j + 2];
+      const T dvdx = (vx - s.vel[3 * j]) * dx + (vy - s.vel[3 * j + 1]) * dy + (vz - s.vel[3 * j + 2]) * dz;
+      const T q = std::sqrt(rr2_of(dx, dy, dz)) / h;
+      if (q <= (T)2) {
+        const T a = (T)1 - q / (T)2;
+        T fr = a * a * a;
+        fr *= (T)-5 * adh / h2;
+        if (ti == 1 && s.type[j] == 1) dv_sum -= fr * dvdx * m / s.rhop[2 * j];  // simple_ns.cu:69-72
+      }
+    });
+    dofv[i] = dv_sum;
+  }
+  for (int i = 0; i < n; ++i)  // simple_ns.cu:81-95
+    if (s.type[i] != 1) { s.rhop[2 * i] = rho_new[i]; s.rhop[2 * i + 1] = p_new[i]; }
+}
+
+// single_gpu_sph_src/equation/simple_ns.cu:99-180 (cuda_govering_ns of the
+// simple equations).
+template <class T> void governing_simple(const Params& p, const State<T>& s, const T* dofv, Tmp<T>& t) {
+  const int n = p.ptc_num;
+  const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m, eta2 = (T)p.eta2;
+  const T dhc = (T)p.delta_h_cs, hcrm = (T)p.h_cs_rho_m, alpha = (T)p.alpha, g = (T)p.g;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    T acc[4] = {0, 0, 0, 0};
+    const T px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
+    const T vx = s.vel[3 * i], vy = s.vel[3 * i + 1], vz = s.vel[3 * i + 2];
+    const T r0 = s.rhop[2 * i], p0 = s.rhop[2 * i + 1];
+    const int ti = s.type[i];
+    const T d0 = dofv[i];
+    for_each_candidate(p, t, i, p.grid_factor, [&](int j) {
+      const T dx = px - s.pos[3 * j], dy = py - s.pos[3 * j + 1], dz = pz - s.pos[3 * j + 2];
+      const T dvdx = (vx - s.vel[3 * j]) * dx + (vy - s.vel[3 * j + 1]) * dy + (vz - s.vel[3 * j + 2]) * dz;
+      const T rr2 = rr2_of(dx, dy, dz);
+      const T q = std::sqrt(rr2) / h;
+      if (q <= (T)2) {
+        const T a = (T)1 - q / (T)2;
+        const T fr = (T)-5 * adh * a * a * a / h2;
+        const T r1 = s.rhop[2 * j], p1 = s.rhop[2 * j + 1];
+        acc[3] += (r0 * dvdx * fr + (r0 - r1) * rr2 * fr * dhc / (rr2 + eta2)) * m / r1;  // simple_ns.cu:162
+        T vt = -(p0 + p1) * m * fr / (r0 * r1);
+        if (ti == 1 && s.type[j] == 1) vt += hcrm * fr * (d0 + dofv[j] + alpha * dvdx / (rr2 + eta2)) / (r0 * r1);
+        acc[0] += vt * dx;
+        acc[1] += vt * dy;
+        acc[2] += vt * dz;
+      }
+    });
+    acc[2] += g;
+    for (int k = 0; k < 4; ++k) t.acc_drhodt[4 * i + k] = acc[k];
+  }
+}
+
+// One step of the simplesph driver (same call order as main.cu:63-88).
+template <class T> void step_simple(const Params& p, State<T>& o, State<T>& w, Tmp<T>& t, T* dofv) {
+  hash(p, o, t);
+  sort_index(p, t);
+  sort_data(p, o, w, t);
+  boundary_simple(p, w, dofv, t);
+  governing_simple(p, w, dofv, t);
+  prediction(p, w, t);
+  hash(p, w, t);
+  sort_index(p, t);
+  sort_data(p, w, o, t);
+  boundary_simple(p, o, dofv, t);
+  governing_simple(p, o, dofv, t);
+  correction(p, o, t);
+}
+
 }  // namespace zsph_oracle

@@ -78,6 +78,14 @@ def main():
         for k in ("pos", "vel", "rhop", "table", "type"):
             runs[f"run{r}.{k}"] = out[k]
     np.savez_compressed(os.path.join(OUT, "ref_steps_dam05.npz"), nsteps=np.array(20), **runs)
+    # simplesph build (equation/simple_ns.cu): one sub-step's kernels and 20 steps of the raw case
+    if po.ref_available(simple=True):
+        out, tmp = po.ref_substep(raw.json, raw.state, 5, simple=True)
+        np.savez_compressed(os.path.join(OUT, "ref_simple_kernels_dam05.npz"), rhop=out["rhop"],
+                            acc_drhodt=tmp["acc_drhodt"], dofv=tmp["dofv"])
+        out, _, _ = po.ref_run(raw.json, raw.state, 20, simple=True)
+        np.savez_compressed(os.path.join(OUT, "ref_simple_steps_dam05.npz"), nsteps=np.array(20),
+                            **{k: out[k] for k in ("pos", "vel", "rhop", "table")})
     print("golden fixtures written to", OUT)
 
 

@@ -103,6 +103,27 @@ def test_raw_input_matches_reference_away_from_the_wall_race():
         assert np.all(d <= 1e-4 * scale), (k, d, scale)
 
 
+def test_simple_kernels_and_steps_match_reference_simplesph():
+    g = load("ref_simple_kernels_dam05.npz")
+    c = GOLDEN_CASES["dam05"]()
+    o = po.Oracle(c.json, c.state, np.float32)
+    o.search()
+    o.boundary_simple("new")
+    o.governing_simple("new")
+    for k, mine in (("dofv", o.dofv), ("acc_drhodt", o.tmp["acc_drhodt"])):
+        scale = np.abs(g[k]).max(axis=0) + 1e-30
+        assert np.all(np.abs(mine - g[k]).max(axis=0) <= 1e-4 * scale), k
+    assert np.allclose(o.new["rhop"], g["rhop"], rtol=1e-6, atol=1e-3)
+    s = load("ref_simple_steps_dam05.npz")
+    o = po.Oracle(c.json, c.state, np.float32)
+    o.step_simple(int(s["nsteps"]))
+    ida = o.old["table"] + np.arange(c.n)
+    idr = s["table"] + np.arange(c.n)
+    a = np.empty_like(o.old["pos"]); a[ida] = o.old["pos"]
+    b = np.empty_like(s["pos"]); b[idr] = s["pos"]
+    assert np.abs(a - b).max() < 1e-5
+
+
 def test_steps_match_reference_runs():
     g = load("ref_steps_dam05.npz")
     n = int(g["nsteps"])

@@ -131,3 +131,23 @@ def test_fp32_oracle_tracks_fp64_oracle():
     pa = np.empty_like(a.old["pos"]); pa[ida] = a.old["pos"]
     pb = np.empty_like(b.old["pos"]); pb[idb] = b.old["pos"]
     assert np.abs(pa - pb).max() < 1e-5
+
+
+def test_simple_equations_fp32_tracks_fp64_and_rest():
+    # simplesph equations: a column at rest in a closed box stays near rest,
+    # and the FP32 instance tracks the FP64 one
+    c = cases.dam_break(0.04, water=(0.6, 0.6, 0.6), tank=(0.6, 0.6, 0.6))
+    o = po.Oracle(c.json, c.state, np.float64)
+    o.search()
+    o.boundary_simple("new")
+    o.governing_simple("new")
+    pos = o.new["pos"]
+    f = (o.new["type"] == 1) & np.all((pos > 0.15) & (pos < 0.45), axis=1)
+    assert np.abs(o.tmp["acc_drhodt"][f, 2]).mean() < 0.05 * 9.81
+    a = po.Oracle(c.json, c.state, np.float32)
+    b = po.Oracle(c.json, c.state, np.float64)
+    a.step_simple(5)
+    b.step_simple(5)
+    pa = np.empty_like(a.old["pos"]); pa[a.old["table"] + np.arange(c.n)] = a.old["pos"]
+    pb = np.empty_like(b.old["pos"]); pb[b.old["table"] + np.arange(c.n)] = b.old["pos"]
+    assert np.abs(pa - pb).max() < 1e-5

@@ -23,6 +23,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libzsph_b200.so")
 
 ZSPH_OK, ZSPH_EINVAL, ZSPH_ECUDA, ZSPH_ENAN, ZSPH_ETIMEOUT, ZSPH_EIO, ZSPH_ENOMEM = range(7)
+EQ_DELTA, EQ_SIMPLE = 0, 1
 FLAG_NAN, FLAG_KILLED, FLAG_NB_OVERFLOW, FLAG_BAD_KEY = 1, 2, 4, 8
 _CODES = {0: "ZSPH_OK", 1: "ZSPH_EINVAL", 2: "ZSPH_ECUDA", 3: "ZSPH_ENAN", 4: "ZSPH_ETIMEOUT", 5: "ZSPH_EIO",
           6: "ZSPH_ENOMEM"}
@@ -112,6 +113,7 @@ _sig = {
     "zsph_create": (_I, [ctypes.POINTER(GpuParam), _I, ctypes.POINTER(_HP)]),
     "zsph_destroy": (None, [_HP]),
     "zsph_set_params": (_I, [_HP, ctypes.POINTER(GpuParam)]),
+    "zsph_set_equations": (_I, [_HP, _I]),
     "zsph_hash": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP]),
     "zsph_sort_index": (_I, [_HP, ctypes.POINTER(Tmp), _VP]),
     "zsph_sort_index_noalloc": (_I, [ctypes.POINTER(GpuParam), _I, ctypes.POINTER(Tmp), _VP]),
@@ -353,6 +355,13 @@ class Solver:
                    stream, ms, cap, ctypes.byref(cnt), names, len(names))
         nm = names.value.decode().split(",")
         return [(nm[k], float(ms[k])) for k in range(cnt.value)]
+
+    def set_equations(self, which: int) -> None:
+        """EQ_DELTA (deltasph, default) or EQ_SIMPLE (simplesph)."""
+        self._call(lib.zsph_set_equations, int(which))
+
+    def download_dofv(self) -> np.ndarray:
+        return self.copy_from_device(self.tmp.dofv, np.empty(self.n, np.float32))
 
     def launches_per_step(self) -> int:
         return int(lib.zsph_launches_per_step(self.h))

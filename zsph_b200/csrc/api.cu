@@ -88,6 +88,7 @@ void fill_kparams(KParams& kp, const zsph_gpu_param_t& p, int grid_num) {
   // measured slower than L1-cached global loads at 20 warps per SM.
   const char* sw = std::getenv("ZSPH_STAGE_WINDOWS");
   kp.stage_windows = (sw && sw[0] == '1') ? 1 : 0;
+  kp.equations = ZSPH_EQ_DELTA;
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -110,8 +111,12 @@ int check_ptc(zsph_handle* h, const zsph_ptc_t* p) {
 
 int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
   if (!t) return set_err(h, ZSPH_EINVAL, "null scratch buffers");
-  if (h->kp.n > 0 && (!t->acc_drhodt || !t->dofv_grandrho || !t->index || !t->hash || !t->grid_start || !t->grid_end))
+  if (h->kp.n > 0 && (!t->acc_drhodt || !t->index || !t->hash || !t->grid_start || !t->grid_end))
     return set_err(h, ZSPH_EINVAL, "a tmp array pointer is null");
+  if (h->kp.n > 0 && h->kp.equations == ZSPH_EQ_DELTA && !t->dofv_grandrho)
+    return set_err(h, ZSPH_EINVAL, "tmp->dofv_grandrho is null (delta equations)");
+  if (h->kp.n > 0 && h->kp.equations == ZSPH_EQ_SIMPLE && !t->dofv)
+    return set_err(h, ZSPH_EINVAL, "tmp->dofv is null (simple equations)");
   return ZSPH_OK;
 }
 
@@ -320,11 +325,25 @@ int zsph_set_params(zsph_handle_t* h, const zsph_gpu_param_t* gp) {
   if (gp->ptc_num != h->kp.n || gp->grid_xdim != h->kp.p.grid_xdim || gp->grid_ydim != h->kp.p.grid_ydim ||
       gp->grid_zdim != h->kp.p.grid_zdim)
     return set_err(h, ZSPH_EINVAL, "zsph_set_params: particle count and grid must not change");
+  const int eq = h->kp.equations;
   fill_kparams(h->kp, *gp, h->kp.G);
+  h->kp.equations = eq;
   if (h->graph) {  // kernel arguments changed: re-capture on the next zsph_run
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
   }
+  return ZSPH_OK;
+}
+
+int zsph_set_equations(zsph_handle_t* h, int equations) {
+  if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle");
+  if (equations != ZSPH_EQ_DELTA && equations != ZSPH_EQ_SIMPLE)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_equations: ZSPH_EQ_DELTA or ZSPH_EQ_SIMPLE");
+  if (h->kp.equations != equations && h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->kp.equations = equations;
   return ZSPH_OK;
 }
 

@@ -698,6 +698,87 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   if (MODE != 0) integrate_one<MODE>(kp, ptc, out, i, acc);
 }
 
+// ---- simple-SPH equations (the reference's simplesph target) --------------
+
+struct NbS {  // simple boundary / governing
+  float4 pr, vp;
+  float dv;
+};
+
+// single_gpu_sph_src/equation/simple_ns.cu:3-97: scalar div(v) over fluid
+// pairs of the boundary stencil into tmp.dofv; new wall (rho, p) (computed
+// by k_nblist) into ptc.rhop.  Walls read only fluid densities here, so the
+// reference has no wall-density race in this kernel.
+template <int GF>
+__global__ void __launch_bounds__(kPairBlock) k_boundary_simple(KParams kp, Scratch s, zsph_ptc_t ptc,
+                                                                zsph_tmp_t t) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PairSmem<GF> sm(dsm);
+  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  if (i >= kp.n) return;
+  load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  const zsph_gpu_param_t& p = kp.p;
+  const float4 pi = s.sh.pr[i];
+  const float4 vi = s.sh.vp[i];
+  const bool fi = fluid_of(pi.w);
+  float divv = 0.f;
+  if (fi)
+    walk<GF, true, NbB1>(
+        kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return NbB1{s.sh.pr[q], s.sh.vp[q]}; },
+        [&](const NbB1& nb) {
+          if (!fluid_of(nb.pr.w)) return;
+          const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+          const float q = sqrt_fast(dist2(dx, dy, dz)) * kp.inv_h;
+          const float a = 1.0f - 0.5f * q;
+          const float fr = kp.c_fr * (a * a * a);
+          const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+          divv -= fr * dvdx * p.m * rcp_fast(nb.pr.w);
+        });
+  t.dofv[i] = divv;
+  if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
+}
+
+// single_gpu_sph_src/equation/simple_ns.cu:99-180, with the same fused
+// prediction / correction epilogue as k_governing.
+template <int GF, int MODE>
+__global__ void __launch_bounds__(kPairBlock) k_governing_simple(KParams kp, Scratch s, zsph_ptc_t ptc,
+                                                                 zsph_tmp_t t, zsph_ptc_t out) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  PairSmem<GF> sm(dsm);
+  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  if (i >= kp.n) return;
+  load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  const zsph_gpu_param_t& p = kp.p;
+  const float4 pi = s.sh.pr[i];
+  const float4 vi = s.sh.vp[i];
+  const bool fi = fluid_of(pi.w);
+  const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
+  const float d0 = t.dofv[i];
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  walk<GF, false, NbS>(
+      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return NbS{s.sh.pr[q], s.sh.vp[q], t.dofv[q]}; },
+      [&](const NbS& nb) {
+        const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+        const float rr2 = dist2(dx, dy, dz);
+        const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
+        const float q = sqrt_fast(rr2) * kp.inv_h;
+        const float a = 1.0f - 0.5f * q;
+        const float fr = kp.c_fr * (a * a * a);
+        const float r1 = fabsf(nb.pr.w), p1 = nb.vp.w, ir1 = rcp_fast(r1);
+        const float ire = rcp_fast(rr2 + p.eta2);
+        acc.w += (r0 * dvdx * fr + (r0 - r1) * rr2 * fr * p.delta_h_cs * ire) * p.m * ir1;  // simple_ns.cu:162
+        float vt = -(p0 + p1) * p.m * fr * ir0 * ir1;
+        if (fi && fluid_of(nb.pr.w)) vt += p.h_cs_rho_m * fr * (d0 + nb.dv + p.alpha * dvdx * ire) * ir0 * ir1;
+        acc.x += vt * dx;
+        acc.y += vt * dy;
+        acc.z += vt * dz;
+      });
+  acc.z += p.g;
+  reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
+  if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(s.flags, ZSPH_FLAG_NAN);
+  if (MODE != 0) integrate_one<MODE>(kp, ptc, out, i, acc);
+}
+
 // Drop-in cuda_prediction / cuda_correction: in place.
 template <int MODE>
 __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc_t ptc, zsph_tmp_t t) {
@@ -715,7 +796,11 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
                         cudaStream_t st, Prof* pf) {
   k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
-  k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(kp.stage_windows ? 2 : 0, kWinCapB), st>>>(kp, s, ptc, t);
+  if (kp.equations == ZSPH_EQ_SIMPLE)
+    k_boundary_simple<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, ptc, t);
+  else
+    k_boundary<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(kp.stage_windows ? 2 : 0, kWinCapB), st>>>(
+        kp, s, ptc, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();
 }
@@ -724,6 +809,14 @@ template <int GF>
 cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t, int mode,
                          const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
   const int nb = thread_blocks(kp.n);
+  if (kp.equations == ZSPH_EQ_SIMPLE) {
+    const int ss = pair_smem<GF>(0, 0);
+    if (mode == 0) k_governing_simple<GF, 0><<<nb, kPairBlock, ss, st>>>(kp, s, ptc, t, out);
+    if (mode == 1) k_governing_simple<GF, 1><<<nb, kPairBlock, ss, st>>>(kp, s, ptc, t, out);
+    if (mode == 2) k_governing_simple<GF, 2><<<nb, kPairBlock, ss, st>>>(kp, s, ptc, t, out);
+    mark(pf, "governing", st);
+    return cudaGetLastError();
+  }
   const int sm = pair_smem<GF>(kp.stage_windows ? 3 : 0, kWinCapG);
   if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
   if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
@@ -772,6 +865,14 @@ cudaError_t init_pair_kernels() {
   setb(k_governing<2, 0>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<2, 1>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<2, 2>, pair_smem<2>(3, kWinCapG));
+  setb(k_boundary_simple<1>, pair_smem<1>(0, 0));
+  setb(k_boundary_simple<2>, pair_smem<2>(0, 0));
+  setb(k_governing_simple<1, 0>, pair_smem<1>(0, 0));
+  setb(k_governing_simple<1, 1>, pair_smem<1>(0, 0));
+  setb(k_governing_simple<1, 2>, pair_smem<1>(0, 0));
+  setb(k_governing_simple<2, 0>, pair_smem<2>(0, 0));
+  setb(k_governing_simple<2, 1>, pair_smem<2>(0, 0));
+  setb(k_governing_simple<2, 2>, pair_smem<2>(0, 0));
   return e;
 }
 

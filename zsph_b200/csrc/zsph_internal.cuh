@@ -30,6 +30,7 @@ struct KParams {
   float inv_gs;          // 1 / grid_size
   float c_fr;            // -5 * adh / h2, the factor of grad W / r
   int stage_windows;     // 1: pair kernels stage neighbour windows in shared memory (TMA bulk copies)
+  int equations;         // ZSPH_EQ_DELTA or ZSPH_EQ_SIMPLE
 };
 
 // Packed per-particle shadows of the sorted state, written by the gather
