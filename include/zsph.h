@@ -220,6 +220,40 @@ int zsph_status(zsph_handle_t* h, int* flags, int clear);
 /* Copies the last error message of the handle (or of the library when h is
  * NULL) into buf; returns its length. */
 int zsph_last_error(zsph_handle_t* h, char* buf, int len);
+/* ---- particle files (legacy VTK, no libVTK) ----------------------------- */
+
+/* Arrays written to a VTK file; the run-time form of the reference's
+ * ZSPH_OUTPUT_* compile-time macros (deltasph/CMakeLists.txt:25-31). */
+enum {
+  ZSPH_OUT_P = 1, ZSPH_OUT_TYPE = 2, ZSPH_OUT_VEL = 4, ZSPH_OUT_ACC = 8,
+  ZSPH_OUT_RHO = 16, ZSPH_OUT_HASH = 32, ZSPH_OUT_TABLE = 64,
+  ZSPH_OUT_REFERENCE = 1 | 2 | 4 | 8 /* what the deltasph build writes */
+};
+
+/* write_vtk (single_gpu_sph_src/io/write_vtk.cu:29-130): legacy VTK, BINARY
+ * big-endian, POINTS plus the POINT_DATA arrays selected by flags.  Host
+ * arrays in the reference layout; unused ones may be NULL. */
+int zsph_write_vtk(const char* path, int ptc_num, const float* pos, const float* vel, const float* rhop,
+                   const int* type, const float* acc_drhodt, const int* hash, const int* table, int flags);
+/* read_vtk (single_gpu_sph_src/io/read_vkt.cu:3-92): points and the point
+ * arrays "p", "rho", "vel", "acc" (double arrays; with accept_float also
+ * float arrays, which the reference ignores), "type" (int, required) and
+ * "table" (int); missing arrays get the reference's defaults (p 0, rho rho0,
+ * vel 0, acc 0, table 0).  ASCII or BINARY; the point count must equal
+ * ptc_num. */
+int zsph_read_vtk(const char* path, int ptc_num, float rho0, int accept_float, float* pos, float* vel, float* rhop,
+                  float* acc_drhodt, int* type, int* table);
+
+/* Output thread pool (io/mul_thread.cu:3-81, deltasph/main.cu:101-142):
+ * zsph_writer_submit copies the selected device arrays into one of nthreads
+ * pinned host buffers on `stream` (waiting while all buffers are in use) and
+ * returns; a worker thread writes output_path/zsph<step>.vtk once the copy has
+ * completed.  zsph_writer_destroy finishes pending files and joins. */
+typedef struct zsph_writer zsph_writer_t;
+int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthreads, zsph_writer_t** out);
+int zsph_writer_submit(zsph_writer_t* w, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int step, void* stream);
+int zsph_writer_destroy(zsph_writer_t* w);
+
 /* Plain device-memory helpers for callers without their own CUDA runtime
  * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,
  * deltasph/main.cu:41-45).  kind: 1 host->device, 2 device->host,

@@ -136,7 +136,34 @@ _sig = {
     "zsph_device_malloc": (_I, [ctypes.POINTER(_VP), ctypes.c_size_t]),
     "zsph_device_free": (_I, [_VP]),
     "zsph_device_synchronize": (_I, []),
+    "zsph_write_vtk": (_I, [ctypes.c_char_p, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _I]),
+    "zsph_read_vtk": (_I, [ctypes.c_char_p, _I, _F, _I, _VP, _VP, _VP, _VP, _VP, _VP]),
+    "zsph_writer_create": (_I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_VP)]),
+    "zsph_writer_submit": (_I, [_VP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _VP]),
+    "zsph_writer_destroy": (_I, [_VP]),
 }
+
+OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
+OUT_REFERENCE = OUT_P | OUT_TYPE | OUT_VEL | OUT_ACC
+
+
+def write_vtk(path: str, st, acc=None, hash=None, flags: int = OUT_REFERENCE) -> None:
+    """zsph_write_vtk of a host State (io/write_vtk.cu:29-130)."""
+    f = lambda a, dt: None if a is None else np.ascontiguousarray(a, dtype=dt)
+    pos, vel, rhop = f(st.pos, np.float32), f(st.vel, np.float32), f(st.rhop, np.float32)
+    typ, tab, a4, hs = f(st.type, np.int32), f(st.table, np.int32), f(acc, np.float32), f(hash, np.int32)
+    check(lib.zsph_write_vtk(path.encode(), len(st.type), _ptr(pos), _ptr(vel), _ptr(rhop), _ptr(typ), _ptr(a4),
+                             _ptr(hs), _ptr(tab), int(flags)))
+
+
+def read_vtk(path: str, n: int, rho0: float = 1000.0, accept_float: bool = False):
+    """zsph_read_vtk (io/read_vkt.cu:3-92): returns (State, acc_drhodt)."""
+    st = State(np.empty((n, 3), np.float32), np.empty((n, 3), np.float32), np.empty((n, 2), np.float32),
+               np.empty(n, np.int32), np.empty(n, np.int32))
+    acc = np.empty((n, 4), np.float32)
+    check(lib.zsph_read_vtk(path.encode(), n, float(rho0), 1 if accept_float else 0, _ptr(st.pos), _ptr(st.vel),
+                            _ptr(st.rhop), _ptr(acc), _ptr(st.type), _ptr(st.table)))
+    return st, acc
 for _name, (_res, _args) in _sig.items():
     _fn = getattr(lib, _name)
     _fn.restype = _res
