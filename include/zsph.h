@@ -254,6 +254,51 @@ int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthr
 int zsph_writer_submit(zsph_writer_t* w, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int step, void* stream);
 int zsph_writer_destroy(zsph_writer_t* w);
 
+/* ---- Learned-corrector network (no reference counterpart) -----------------
+ * A per-particle MLP 32 -> 128 -> 128 -> 4 with SiLU, bf16 weights and fp32
+ * accumulation on the fifth-generation tensor cores.  Its fp32 master
+ * parameters form one vector of ZSPH_MLP_NPARAM floats:
+ *   W1[128][32], b1[128], W2[128][128], b2[128], W3[4][128], b3[4]
+ * (weights row-major [out][in]).  Inputs are feature TILES: 128 rows of 32
+ * standardized bf16 features, 8 KB per tile, in the tensor-core operand
+ * layout (zsph_mlp_pack writes it); rows past the last valid one are zero.
+ * Training partials: one row of ZSPH_MLP_NPARTIAL floats per CTA of
+ * zsph_mlp_grad, the gradient in parameter order followed by the loss sum. */
+enum {
+  ZSPH_MLP_IN = 32,
+  ZSPH_MLP_HID = 128,
+  ZSPH_MLP_OUT = 4,
+  ZSPH_MLP_NPARAM = 21252,
+  ZSPH_MLP_NPARTIAL = 21256,
+  ZSPH_MLP_TILE_ROWS = 128,
+  ZSPH_MLP_TILE_BYTES = 8192
+};
+typedef struct zsph_mlp zsph_mlp_t;
+/* Creates the network on the current device with seeded uniform
+ * (+-1/sqrt(fan_in)) weights, zero biases and zero Adam moments. */
+int zsph_mlp_create(unsigned long long seed, zsph_mlp_t** out);
+int zsph_mlp_destroy(zsph_mlp_t* m);
+/* Host <-> device copies of the fp32 master parameters (set also refreshes
+ * the bf16 weights) and of the Adam moments and step count. */
+int zsph_mlp_set_params(zsph_mlp_t* m, const float* params);
+int zsph_mlp_get_params(zsph_mlp_t* m, float* params);
+int zsph_mlp_set_moments(zsph_mlp_t* m, const float* m1, const float* m2, int step);
+int zsph_mlp_get_moments(zsph_mlp_t* m, float* m1, float* m2, int* step);
+/* Device rows [n][32] fp32 -> feature tiles: (x - mean) * inv_std rounded to
+ * bf16 (mean, inv_std: 32 host floats each); tiles holds ceil(n/128) tiles. */
+int zsph_mlp_pack(const float* rows, int n, const float* mean, const float* inv_std, void* tiles, void* stream);
+/* out[n][4] (device) = network(tiles), standardized outputs. */
+int zsph_mlp_forward(zsph_mlp_t* m, const void* tiles, int n, float* out, void* stream);
+/* Gradient of  sum_r w[r] * |net(x_r) - y_r|^2 * inv_wsum  over the tiles
+ * tile_ids[0..ntiles) (NULL: tiles 0..ntiles-1); y and w are indexed by
+ * tile*128 + row.  Writes *nparts rows of partials (at most the SM count). */
+int zsph_mlp_grad(zsph_mlp_t* m, const void* tiles, const float* y, const float* w, const int* tile_ids,
+                  int ntiles, float inv_wsum, float* partial, int* nparts, void* stream);
+/* One Adam step (fp32, no weight decay) from nparts partial rows, summed in
+ * row order; refreshes the bf16 weights. */
+int zsph_mlp_adam(zsph_mlp_t* m, const float* partial, int nparts, float lr, float beta1, float beta2, float eps,
+                  void* stream);
+
 /* Plain device-memory helpers for callers without their own CUDA runtime
  * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,
  * deltasph/main.cu:41-45).  kind: 1 host->device, 2 device->host,

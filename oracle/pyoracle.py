@@ -94,7 +94,9 @@ class Oracle:
         if rc != 0:
             raise ValueError("dt > dt_max")
         n, G = self.p.ptc_num, self.p.grid_num
-        cv = lambda a, shape: (np.zeros(shape, self.dtype) if a is None else np.ascontiguousarray(a, self.dtype))
+        # always a private copy: the oracle steps in place, and a caller's
+        # float32 arrays would otherwise be shared with (and mutated by) it
+        cv = lambda a, shape: (np.zeros(shape, self.dtype) if a is None else np.array(a, self.dtype, order="C"))
         self.old = dict(pos=cv(state.pos, (n, 3)), vel=cv(state.vel, (n, 3)), rhop=cv(state.rhop, (n, 2)),
                         tmp_pos=cv(state.tmp_pos, (n, 3)), tmp_vel=cv(state.tmp_vel, (n, 3)),
                         tmp_rhop=cv(state.tmp_rhop, (n, 2)),

@@ -141,6 +141,16 @@ _sig = {
     "zsph_writer_create": (_I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_VP)]),
     "zsph_writer_submit": (_I, [_VP, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _VP]),
     "zsph_writer_destroy": (_I, [_VP]),
+    "zsph_mlp_create": (_I, [ctypes.c_ulonglong, ctypes.POINTER(_VP)]),
+    "zsph_mlp_destroy": (_I, [_VP]),
+    "zsph_mlp_set_params": (_I, [_VP, _VP]),
+    "zsph_mlp_get_params": (_I, [_VP, _VP]),
+    "zsph_mlp_set_moments": (_I, [_VP, _VP, _VP, _I]),
+    "zsph_mlp_get_moments": (_I, [_VP, _VP, _VP, _IP]),
+    "zsph_mlp_pack": (_I, [_VP, _I, _VP, _VP, _VP, _VP]),
+    "zsph_mlp_forward": (_I, [_VP, _VP, _I, _VP, _VP]),
+    "zsph_mlp_grad": (_I, [_VP, _VP, _VP, _VP, _VP, _I, _F, _VP, _IP, _VP]),
+    "zsph_mlp_adam": (_I, [_VP, _VP, _I, _F, _F, _F, _F, _VP]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -420,3 +430,117 @@ class _DeviceInts:
             lib.zsph_device_free(self.ptr)
         except Exception:
             pass
+
+
+class DeviceArray:
+    """A device buffer with a fixed numpy shape/dtype (library allocator)."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.shape = tuple(np.atleast_1d(shape)) if not isinstance(shape, tuple) else shape
+        self.dtype = np.dtype(dtype)
+        self.nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        p = _VP()
+        check(lib.zsph_device_malloc(ctypes.byref(p), max(self.nbytes, 16)))
+        self.ptr = p
+
+    @classmethod
+    def from_host(cls, a: np.ndarray) -> "DeviceArray":
+        a = np.ascontiguousarray(a)
+        d = cls(a.shape, a.dtype)
+        d.set(a)
+        return d
+
+    def set(self, a: np.ndarray) -> None:
+        a = np.ascontiguousarray(a, self.dtype)
+        assert a.nbytes == self.nbytes
+        if self.nbytes:
+            _cudart_memcpy(self.ptr, a.ctypes.data, self.nbytes, 1)
+
+    def zero(self) -> None:
+        self.set(np.zeros(self.shape, self.dtype))
+
+    def get(self) -> np.ndarray:
+        out = np.empty(self.shape, self.dtype)
+        if self.nbytes:
+            _cudart_memcpy(out.ctypes.data, self.ptr, self.nbytes, 2)
+        return out
+
+    def __del__(self):
+        try:
+            lib.zsph_device_free(self.ptr)
+        except Exception:
+            pass
+
+
+MLP_IN, MLP_HID, MLP_OUT, MLP_NPARAM, MLP_NPARTIAL, MLP_TILE = 32, 128, 4, 21252, 21256, 128
+
+
+class Mlp:
+    """The learned-corrector network (zsph_mlp_*): tensor-core forward,
+    backward and Adam on the current device."""
+
+    def __init__(self, seed: int = 0):
+        self.h = _VP()
+        check(lib.zsph_mlp_create(int(seed), ctypes.byref(self.h)))
+
+    def close(self) -> None:
+        if self.h:
+            lib.zsph_mlp_destroy(self.h)
+            self.h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(MLP_NPARAM, np.float32)
+        check(lib.zsph_mlp_get_params(self.h, out.ctypes.data))
+        return out
+
+    @params.setter
+    def params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == MLP_NPARAM
+        check(lib.zsph_mlp_set_params(self.h, p.ctypes.data))
+
+    def moments(self):
+        m1, m2, st = np.empty(MLP_NPARAM, np.float32), np.empty(MLP_NPARAM, np.float32), ctypes.c_int(0)
+        check(lib.zsph_mlp_get_moments(self.h, m1.ctypes.data, m2.ctypes.data, ctypes.byref(st)))
+        return m1, m2, st.value
+
+    def set_moments(self, m1, m2, step: int) -> None:
+        m1, m2 = np.ascontiguousarray(m1, np.float32), np.ascontiguousarray(m2, np.float32)
+        check(lib.zsph_mlp_set_moments(self.h, m1.ctypes.data, m2.ctypes.data, int(step)))
+
+    @staticmethod
+    def pack(rows: DeviceArray, n: int, mean=None, inv_std=None) -> DeviceArray:
+        tiles = DeviceArray(((n + MLP_TILE - 1) // MLP_TILE, 4096), np.uint16)
+        mv = None if mean is None else np.ascontiguousarray(mean, np.float32)
+        sv = None if inv_std is None else np.ascontiguousarray(inv_std, np.float32)
+        check(lib.zsph_mlp_pack(rows.ptr, int(n), None if mv is None else mv.ctypes.data,
+                                None if sv is None else sv.ctypes.data, tiles.ptr, None))
+        _cudart_sync()
+        return tiles
+
+    def forward(self, tiles: DeviceArray, n: int) -> np.ndarray:
+        out = DeviceArray((n, 4), np.float32)
+        check(lib.zsph_mlp_forward(self.h, tiles.ptr, int(n), out.ptr, None))
+        return out.get()
+
+    def grad(self, tiles: DeviceArray, y: DeviceArray, w: DeviceArray, ntiles: int, inv_wsum: float,
+             tile_ids: DeviceArray | None = None):
+        """Returns (partial rows as a DeviceArray, number of rows)."""
+        partial = DeviceArray((max(ntiles, 1) if ntiles < 512 else 512, MLP_NPARTIAL), np.float32)
+        nparts = ctypes.c_int(0)
+        check(lib.zsph_mlp_grad(self.h, tiles.ptr, y.ptr, w.ptr, None if tile_ids is None else tile_ids.ptr,
+                                int(ntiles), float(inv_wsum), partial.ptr, ctypes.byref(nparts), None))
+        return partial, nparts.value
+
+    def adam(self, partial: DeviceArray, nparts: int, lr: float = 1e-3, beta1: float = 0.9, beta2: float = 0.999,
+             eps: float = 1e-8) -> None:
+        check(lib.zsph_mlp_adam(self.h, partial.ptr, int(nparts), float(lr), float(beta1), float(beta2), float(eps),
+                                None))
+        _cudart_sync()
