@@ -284,6 +284,12 @@ int zsph_mlp_set_params(zsph_mlp_t* m, const float* params);
 int zsph_mlp_get_params(zsph_mlp_t* m, float* params);
 int zsph_mlp_set_moments(zsph_mlp_t* m, const float* m1, const float* m2, int step);
 int zsph_mlp_get_moments(zsph_mlp_t* m, float* m1, float* m2, int* step);
+/* Standardization the learned corrector applies around the network: input
+ * feature k enters as (x_k - in_mean[k]) * in_inv_std[k] (32 floats each);
+ * output k leaves as y_k * out_std[k] + out_mean[k] (4 floats each). */
+int zsph_mlp_set_norm(zsph_mlp_t* m, const float* in_mean, const float* in_inv_std, const float* out_mean,
+                      const float* out_std);
+int zsph_mlp_get_norm(zsph_mlp_t* m, float* in_mean, float* in_inv_std, float* out_mean, float* out_std);
 /* Device rows [n][32] fp32 -> feature tiles: (x - mean) * inv_std rounded to
  * bf16 (mean, inv_std: 32 host floats each); tiles holds ceil(n/128) tiles. */
 int zsph_mlp_pack(const float* rows, int n, const float* mean, const float* inv_std, void* tiles, void* stream);
@@ -298,6 +304,73 @@ int zsph_mlp_grad(zsph_mlp_t* m, const void* tiles, const float* y, const float*
  * row order; refreshes the bf16 weights. */
 int zsph_mlp_adam(zsph_mlp_t* m, const float* partial, int nparts, float lr, float beta1, float beta2, float eps,
                   void* stream);
+
+/* ---- Learned-corrector form of the step (no reference counterpart) --------
+ * The predictor sub-step stays the plain one; its governing walk also
+ * accumulates 32 non-dimensional neighbour aggregates per fluid particle
+ * (lengths in h, speeds in c0, densities in rho0; zeros for walls), among
+ * them D = a_n - a_c(prev): the predictor-stage (acc, drho/dt) minus the
+ * particle's previous corrector-stage value.  The corrector-stage value is
+ * predicted as a_n + D (linear extrapolation over the two half steps) plus
+ * the network's residual (accelerations in c0^2/h, density rates in
+ * rho0 c0/h), and one tensor-core kernel applies the correction of
+ * time_int.cu:50-92 with it in place of the corrector sub-step.  The first
+ * step of a run is plain (it has no previous corrector value).  Delta-SPH
+ * equations only. */
+
+/* The 32 non-dimensional feature scales of the handle's case. */
+int zsph_learn_feature_scales(zsph_handle_t* h, float* scale);
+/* The predictor sub-step of zsph_step (search old_ into new_, boundary,
+ * governing of new_ with the predicted state written into old_) that also
+ * writes the raw features [ptc_num][32] (new_'s sorted order) to the device
+ * array `features` (16-byte aligned). */
+int zsph_learn_features(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+                        float* features, void* stream);
+/* nsteps plain steps (zsph_step); at every `every`-th one the features and
+ * the targets (plain corrector minus predictor values) of every particle are
+ * kept on the handle as one training snapshot (fluid rows weight 1, others
+ * 0), up to `capacity` snapshots (fixed by the first call).  *count: the
+ * snapshots held. */
+int zsph_learn_collect(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+                       int nsteps, int every, int capacity, int* count, void* stream);
+/* Drops the handle's snapshots. */
+int zsph_learn_clear(zsph_handle_t* h);
+
+typedef struct {
+  int snapshots_train, snapshots_val;
+  long long rows_train;        /* fluid rows trained on */
+  int epochs, iterations;
+  float loss_first, loss_last; /* mean standardized squared error of the first / last epoch */
+  /* held-out snapshots, fluid rows: |prediction - corrector| / |corrector|
+   * with the network, (_base) with the predictor-stage values alone and
+   * (_extrap) with the extrapolation a_n + D alone */
+  float val_acc_rel_l2, val_acc_rel_l2_base, val_acc_rel_l2_extrap;
+  float val_drho_rel_l2, val_drho_rel_l2_base, val_drho_rel_l2_extrap;
+  float seconds;
+} zsph_learn_train_stats_t;
+
+/* Trains `net` on the handle's snapshots: sets its standardization from the
+ * training snapshots (FP64 moments), then `epochs` passes of Adam over
+ * shuffled 128-row tiles (batch_tiles per step, learning rate lr with cosine
+ * decay to lr/20, seeded shuffle).  The last val_frac of the snapshots, in
+ * collection order, are held out and reported in *stats. */
+int zsph_learn_train(zsph_handle_t* h, zsph_mlp_t* net, int epochs, int batch_tiles, float lr,
+                     unsigned long long seed, float val_frac, zsph_learn_train_stats_t* stats, void* stream);
+
+typedef struct {
+  int steps, learned, plain, judged, fallbacks;
+  float err_max, err_mean, err_last; /* judged |a_learned - a_plain| / |a_plain| over fluid particles */
+} zsph_learn_run_stats_t;
+
+/* nsteps steps of the learned form.  Every judge_every-th step (0: never)
+ * also runs the plain corrector, which judges the network's accelerations
+ * (relative L2 over fluid particles) and supplies that step's result; when
+ * the error exceeds tol the plain corrector takes over until a judged step
+ * passes again.  old_ holds the state afterwards (in the last search's
+ * order); the host reads the judge's two sums on judged steps. */
+int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old_, const zsph_ptc_t* new_,
+                     const zsph_tmp_t* tmp, int nsteps, int judge_every, float tol, zsph_learn_run_stats_t* stats,
+                     void* stream);
 
 /* Plain device-memory helpers for callers without their own CUDA runtime
  * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,

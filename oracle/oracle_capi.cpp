@@ -94,6 +94,10 @@ int oracle_max_threads(void) { return omp_get_max_threads(); }
   }                                                                                                 \
   void oracle_step_simple_##SUF(const Params* p, State<T>* o, State<T>* w, Tmp<T>* t, T* dofv, int nsteps) { \
     for (int k = 0; k < nsteps; ++k) step_simple<T>(*p, *o, *w, *t, dofv);                          \
+  }                                                                                                 \
+  void oracle_features_##SUF(const Params* p, const State<T>* s, const Tmp<T>* t, const float* scale,       \
+                             const T* acc_prev, T* out) {                                           \
+    features<T>(*p, *s, *t, scale, acc_prev, out);                                                  \
   }
 
 ORACLE_INSTANCE(f32, float)

@@ -153,6 +153,17 @@ class Oracle:
         self._fn("step")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
                          ctypes.byref(self._t), _I(nsteps), _I(wall_mode))
 
+    def features(self, scale, which="new", acc_prev=None) -> np.ndarray:
+        """Learned-corrector inputs of `which` (after search, boundary and
+        governing); acc_prev: previous corrector-stage (acc, drho/dt) in the
+        order before the search (None: those four features are zero)."""
+        out = np.zeros((self.p.ptc_num, 32), self.dtype)
+        sc = np.ascontiguousarray(scale, np.float32)
+        ap = None if acc_prev is None else np.ascontiguousarray(acc_prev, self.dtype)
+        self._fn("features")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
+                             _p(sc), _p(ap), _p(out))
+        return out
+
     # simple-SPH equations (the reference's simplesph target); div(v) is the
     # scalar array self.dofv
     def _dofv(self):

@@ -356,6 +356,76 @@ template <class T> void governing(const Params& p, const State<T>& s, Tmp<T>& t)
   }
 }
 
+// Learned-corrector inputs (no reference counterpart): the 32 neighbour
+// aggregates that the learned form's predictor-stage governing walk writes
+// for each fluid particle (zeros for walls), restated as plain sums over the
+// governing stencil's neighbours (q <= 2).  Reads dofv_grandrho from the
+// boundary pass and acc_drhodt from governing(); out[32 i + k] = f_k * scale[k].
+//  0 sum_fluid w W      1 sum_wall w W       2-4 sum w F x_ij      5 divv_i
+//  6-8 sum_fluid w F (divv_j - divv_i) x_ij    9-11 divv_i sum_fluid w F x_ij
+//  12 sum_fluid w F (rho_i - rho_j) 2e          13 sum w F (p_i - p_j) 2e
+//  14-17 acc, drho/dt   18-20 v_i   21 rho_i - rho0   22-24 grad rho_i
+//  25-27, 31 D = (acc, drho/dt) - the previous corrector-stage value of the
+//  same particle (acc_prev, in the order before this search: index[i])
+//  28-30 sum_wall -(p_i + p_j) m F x_ij / (rho_i rho_j)
+//  w = m / rho_j, grad W = F x_ij, e = r^2/(r^2+eta^2)
+template <class T>
+void features(const Params& p, const State<T>& s, const Tmp<T>& t, const float* scale, const T* acc_prev, T* out) {
+  const int n = p.ptc_num;
+  const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m, eta2 = (T)p.eta2, rho0 = (T)p.rho0;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    T f[32] = {};
+    if (s.type[i] == 1) {
+      const T px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
+      const T vx = s.vel[3 * i], vy = s.vel[3 * i + 1], vz = s.vel[3 * i + 2];
+      const T r0 = s.rhop[2 * i], p0 = s.rhop[2 * i + 1];
+      const T* G0 = &t.dofv_grandrho[4 * i];
+      T k3[3] = {0, 0, 0};
+      for_each_candidate(p, t, i, p.grid_factor, [&](int j) {
+        const T d[3] = {px - s.pos[3 * j], py - s.pos[3 * j + 1], pz - s.pos[3 * j + 2]};
+        const T rr2 = rr2_of(d[0], d[1], d[2]);
+        const T q = std::sqrt(rr2) / h;
+        if (!(q <= (T)2)) return;
+        const T a = (T)1 - q / (T)2;
+        const T fr = (T)-5 * adh * a * a * a / h2;
+        const T r1 = s.rhop[2 * j], p1 = s.rhop[2 * j + 1];
+        const T frm = fr * m / r1, e = rr2 / (rr2 + eta2);
+        const T wW = adh * a * a * a * a * ((T)2 * q + (T)1) * m / r1;
+        for (int c = 0; c < 3; ++c) f[2 + c] += frm * d[c];
+        f[13] += frm * (p0 - p1) * (T)2 * e;
+        if (s.type[j] == 1) {
+          const T* G1 = &t.dofv_grandrho[4 * j];
+          f[0] += wW;
+          for (int c = 0; c < 3; ++c) {
+            f[6 + c] += frm * (G1[3] - G0[3]) * d[c];
+            k3[c] += frm * d[c];
+          }
+          f[12] += frm * (r0 - r1) * (T)2 * e;
+        } else {
+          f[1] += wW;
+          const T vt = -(p0 + p1) * m * fr / (r0 * r1);
+          for (int c = 0; c < 3; ++c) f[28 + c] += vt * d[c];
+        }
+      });
+      f[5] = G0[3];
+      for (int c = 0; c < 3; ++c) {
+        f[9 + c] = G0[3] * k3[c];
+        f[22 + c] = G0[c];
+      }
+      for (int c = 0; c < 4; ++c) f[14 + c] = t.acc_drhodt[4 * i + c];
+      if (acc_prev) {
+        const T* ap = &acc_prev[4 * (size_t)t.index[i]];
+        for (int c = 0; c < 3; ++c) f[25 + c] = t.acc_drhodt[4 * i + c] - ap[c];
+        f[31] = t.acc_drhodt[4 * i + 3] - ap[3];
+      }
+      f[18] = vx; f[19] = vy; f[20] = vz;
+      f[21] = r0 - rho0;
+    }
+    for (int k = 0; k < 32; ++k) out[32 * (size_t)i + k] = f[k] * (T)scale[k];
+  }
+}
+
 // single_gpu_sph_src/lib/time_int.cu:3-48
 template <class T> void prediction(const Params& p, State<T>& s, const Tmp<T>& t) {
   const T hdt = (T)p.half_dt, rho0 = (T)p.rho0, cs2 = (T)p.cs2;

@@ -1,0 +1,97 @@
+"""Learned-corrector form: the predictor-stage features against the CPU
+oracle, training on snapshots of plain steps (the network must beat the
+predictor-only corrector on held-out snapshots), the learned run with its
+judge, and the fallback to the plain corrector when the network is wrong."""
+import numpy as np
+import pytest
+
+import zsph_b200 as z
+from oracle import pyoracle as po
+from zsph_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+FEAT_TOL = 2e-3  # |gpu - oracle| per feature, relative to the feature's RMS over fluid rows
+
+
+def _moving_state(dx=0.04, steps=60):
+    c = cases.small(dx)
+    sol = z.Solver.from_case(c)
+    sol.run(steps)
+    sol.sync()
+    return c, sol
+
+
+def test_features_match_oracle():
+    c, sol = _moving_state()
+    st = sol.download("old")
+    prev = sol.download_tmp()["acc_drhodt"]  # the last corrector-stage values, old_'s order
+    scale = sol.feature_scales()
+    feats = sol.learn_features()  # predictor sub-step: features of new_'s order
+    o = po.Oracle(c.json, st)
+    o.search("old", "new")
+    o.boundary("new", po.WALLS_FIRST)
+    o.governing("new")
+    want = o.features(scale, "new", acc_prev=prev)
+    fluid = o.new["type"] == 1
+    assert np.array_equal(sol.download("new").type, o.new["type"])
+    assert np.all(feats[~fluid] == 0)
+    for k in range(32):
+        rms = np.sqrt(np.mean(want[fluid, k].astype(np.float64) ** 2)) + 1e-30
+        err = np.max(np.abs(feats[fluid, k] - want[fluid, k])) / rms
+        assert err < FEAT_TOL, (k, err)
+    sol.close()
+
+
+@pytest.fixture(scope="module")
+def trained():
+    c, sol = _moving_state(0.04, 40)
+    count = sol.collect(160, 2, 80)
+    assert count == 80
+    net = z.Mlp(seed=7)
+    stats = sol.train(net, epochs=30, batch_tiles=32, lr=2e-3, seed=1, val_frac=0.2)
+    print("train", stats)
+    yield c, sol, net, stats
+    net.close()
+    sol.close()
+
+
+def test_training_beats_predictor_only(trained):
+    """What the learned corrector gains: on held-out snapshots its
+    corrector-stage values are closer to the plain corrector's than the
+    predictor-stage values alone; the stats also report the extrapolation
+    prior alone, the network's share of the gain."""
+    _, _, _, s = trained
+    assert s["snapshots_train"] == 64 and s["snapshots_val"] == 16
+    assert s["loss_last"] < s["loss_first"]
+    assert s["val_acc_rel_l2"] < s["val_acc_rel_l2_base"]
+    assert s["val_drho_rel_l2"] < s["val_drho_rel_l2_base"]
+    assert s["val_acc_rel_l2_extrap"] < s["val_acc_rel_l2_base"]
+
+
+def test_learned_run_is_judged(trained):
+    _, sol, net, _ = trained
+    r = sol.run_learned(net, 40, judge_every=10, tol=1e-2)
+    print("run", r)
+    assert r["steps"] == 40 and r["judged"] == 4
+    assert r["learned"] + r["plain"] == 36
+    assert np.isfinite(r["err_max"]) and r["err_max"] > 0
+    st = sol.download("old")
+    assert np.all(np.isfinite(st.pos)) and np.all(np.isfinite(st.vel))
+    assert sol.status() == 0
+
+
+def test_untrained_network_falls_back():
+    c, sol = _moving_state(0.04, 20)
+    net = z.Mlp(seed=3)
+    norm = net.norm
+    norm["out_std"] = np.full(4, 50.0, np.float32)  # untrained and loud: far off the plain corrector
+    net.norm = norm
+    r = sol.run_learned(net, 30, judge_every=5, tol=1e-2)
+    print("run", r)
+    assert r["judged"] == 6 and r["fallbacks"] >= 1 and r["plain"] > 0
+    assert r["err_max"] > 1e-2
+    st = sol.download("old")
+    assert np.all(np.isfinite(st.pos))
+    net.close()
+    sol.close()

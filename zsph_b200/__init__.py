@@ -98,6 +98,25 @@ class Tmp(ctypes.Structure):
                                    "grid_end")]
 
 
+class LearnTrainStats(ctypes.Structure):
+    """zsph_learn_train_stats_t."""
+    _fields_ = [("snapshots_train", ctypes.c_int), ("snapshots_val", ctypes.c_int), ("rows_train", ctypes.c_longlong),
+                ("epochs", ctypes.c_int), ("iterations", ctypes.c_int)] + \
+               [(n, ctypes.c_float) for n in ("loss_first", "loss_last", "val_acc_rel_l2", "val_acc_rel_l2_base",
+                                              "val_acc_rel_l2_extrap", "val_drho_rel_l2", "val_drho_rel_l2_base",
+                                              "val_drho_rel_l2_extrap", "seconds")]
+
+
+class LearnRunStats(ctypes.Structure):
+    """zsph_learn_run_stats_t."""
+    _fields_ = [(n, ctypes.c_int) for n in ("steps", "learned", "plain", "judged", "fallbacks")] + \
+               [(n, ctypes.c_float) for n in ("err_max", "err_mean", "err_last")]
+
+
+def _as_dict(s: ctypes.Structure) -> dict:
+    return {k: getattr(s, k) for k, _ in s._fields_}
+
+
 _HP = ctypes.c_void_p
 _sig = {
     "zsph_read_json": (_I, [ctypes.c_char_p, ctypes.POINTER(JsonCase), ctypes.c_char_p, _I]),
@@ -151,6 +170,16 @@ _sig = {
     "zsph_mlp_forward": (_I, [_VP, _VP, _I, _VP, _VP]),
     "zsph_mlp_grad": (_I, [_VP, _VP, _VP, _VP, _VP, _I, _F, _VP, _IP, _VP]),
     "zsph_mlp_adam": (_I, [_VP, _VP, _I, _F, _F, _F, _F, _VP]),
+    "zsph_mlp_set_norm": (_I, [_VP, _VP, _VP, _VP, _VP]),
+    "zsph_mlp_get_norm": (_I, [_VP, _VP, _VP, _VP, _VP]),
+    "zsph_learn_feature_scales": (_I, [_HP, _VP]),
+    "zsph_learn_features": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _VP]),
+    "zsph_learn_collect": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _I, _IP,
+                                _VP]),
+    "zsph_learn_clear": (_I, [_HP]),
+    "zsph_learn_train": (_I, [_HP, _VP, _I, _I, _F, ctypes.c_ulonglong, _F, ctypes.POINTER(LearnTrainStats), _VP]),
+    "zsph_run_learned": (_I, [_HP, _VP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _F,
+                              ctypes.POINTER(LearnRunStats), _VP]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -403,6 +432,43 @@ class Solver:
     def launches_per_step(self) -> int:
         return int(lib.zsph_launches_per_step(self.h))
 
+    # ---- learned-corrector form (zsph_learn_*, zsph_run_learned) ----------
+    def feature_scales(self) -> np.ndarray:
+        s = np.empty(32, np.float32)
+        self._call(lib.zsph_learn_feature_scales, s.ctypes.data)
+        return s
+
+    def learn_features(self, stream=None) -> np.ndarray:
+        """Predictor sub-step that also returns the raw features of the
+        sorted (new_) order."""
+        buf = DeviceArray((self.n, 32), np.float32)
+        self._call(lib.zsph_learn_features, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+                   buf.ptr, stream)
+        _cudart_sync()
+        return buf.get()
+
+    def collect(self, nsteps: int, every: int, capacity: int, stream=None) -> int:
+        c = ctypes.c_int(0)
+        self._call(lib.zsph_learn_collect, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+                   int(nsteps), int(every), int(capacity), ctypes.byref(c), stream)
+        return c.value
+
+    def clear_snapshots(self) -> None:
+        self._call(lib.zsph_learn_clear)
+
+    def train(self, net: "Mlp", epochs: int = 10, batch_tiles: int = 148, lr: float = 2e-3, seed: int = 0,
+              val_frac: float = 0.1, stream=None) -> dict:
+        st = LearnTrainStats()
+        self._call(lib.zsph_learn_train, net.h, int(epochs), int(batch_tiles), float(lr), int(seed), float(val_frac),
+                   ctypes.byref(st), stream)
+        return _as_dict(st)
+
+    def run_learned(self, net: "Mlp", nsteps: int, judge_every: int = 10, tol: float = 1e-2, stream=None) -> dict:
+        st = LearnRunStats()
+        self._call(lib.zsph_run_learned, net.h, ctypes.byref(self.old), ctypes.byref(self.new),
+                   ctypes.byref(self.tmp), int(nsteps), int(judge_every), float(tol), ctypes.byref(st), stream)
+        return _as_dict(st)
+
 
 # ---- device-memory helpers through the library's own C ABI ----------------
 def _cudart_memcpy(dst, src, nbytes, kind):
@@ -510,6 +576,20 @@ class Mlp:
         m1, m2, st = np.empty(MLP_NPARAM, np.float32), np.empty(MLP_NPARAM, np.float32), ctypes.c_int(0)
         check(lib.zsph_mlp_get_moments(self.h, m1.ctypes.data, m2.ctypes.data, ctypes.byref(st)))
         return m1, m2, st.value
+
+    @property
+    def norm(self) -> dict:
+        v = {k: np.zeros(n, np.float32) for k, n in (("in_mean", 32), ("in_inv_std", 32), ("out_mean", 4),
+                                                       ("out_std", 4))}
+        check(lib.zsph_mlp_get_norm(self.h, v["in_mean"].ctypes.data, v["in_inv_std"].ctypes.data,
+                                    v["out_mean"].ctypes.data, v["out_std"].ctypes.data))
+        return v
+
+    @norm.setter
+    def norm(self, v: dict) -> None:
+        a = {k: np.ascontiguousarray(v[k], np.float32) for k in ("in_mean", "in_inv_std", "out_mean", "out_std")}
+        check(lib.zsph_mlp_set_norm(self.h, a["in_mean"].ctypes.data, a["in_inv_std"].ctypes.data,
+                                    a["out_mean"].ctypes.data, a["out_std"].ctypes.data))
 
     def set_moments(self, m1, m2, step: int) -> None:
         m1, m2 = np.ascontiguousarray(m1, np.float32), np.ascontiguousarray(m2, np.float32)

@@ -24,8 +24,6 @@
 
 using namespace zsph;
 
-struct zsph_handle : public zsph::Handle {};
-
 namespace {
 
 std::mutex g_err_mu;
@@ -135,10 +133,10 @@ template <class T> cudaError_t dalloc(T*& p, size_t count) {
 // One sub-step of the fused path: search `from` into `to`, boundary on `to`,
 // governing + integration of `to` written into `from`.
 cudaError_t substep(zsph_handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
-                    cudaStream_t st, Prof* pf) {
+                    cudaStream_t st, Prof* pf, const FeatOut* feat = nullptr) {
   cudaError_t e = launch_search(h->kp, h->s, h->tiles, from, to, t, st, pf);
   if (!e) e = launch_boundary(h->kp, h->s, to, t, st, pf);
-  if (!e) e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf);
+  if (!e) e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf, feat);
   return e;
 }
 
@@ -153,6 +151,10 @@ cudaError_t step_launches(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t&
 
 namespace zsph {
 void record_library_error(const std::string& msg) { set_err(nullptr, ZSPH_OK, msg); }
+cudaError_t run_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
+                        cudaStream_t st, Prof* pf, const FeatOut* feat) {
+  return substep(static_cast<zsph_handle*>(h), from, to, t, mode, st, pf, feat);
+}
 }  // namespace zsph
 
 extern "C" {
@@ -314,6 +316,7 @@ void zsph_destroy(zsph_handle_t* h) {
   if (!h) return;
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
+  learn_destroy(h);
   free_scratch(h->s);
   delete h;
 }

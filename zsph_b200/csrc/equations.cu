@@ -41,6 +41,8 @@
 // reads neighbours' densities from the shadows (new wall values) and a
 // wall's own old density from ptc.rhop, and writes the new wall values to
 // ptc.rhop at the end, when no reader is left.
+#include <cuda_bf16.h>
+
 #include "integrate.cuh"
 #include "zsph_internal.cuh"
 
@@ -587,12 +589,30 @@ struct NbG {  // governing
   float4 pr, vp, dg;
 };
 
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// Learned-corrector aggregates of one fluid particle (FeatOut; the network's
+// input order).  w = m / rho_j, grad W = F x_ij, e = r^2 / (r^2 + eta^2).
+struct FeatAcc {
+  float shep_f = 0.f, shep_w = 0.f;        // 0, 1: sum w W over fluid / wall j
+  float gx = 0.f, gy = 0.f, gz = 0.f;      // 2-4: sum w F x_ij
+  float dx = 0.f, dy = 0.f, dz = 0.f;      // 6-8: sum_fluid w F (divv_j - divv_i) x_ij
+  float kx = 0.f, ky = 0.f, kz = 0.f;      // 9-11 (times divv_i): sum_fluid w F x_ij
+  float lap_rho = 0.f;                     // 12: sum_fluid w F (rho_i - rho_j) 2e
+  float lap_p = 0.f;                       // 13: sum w F (p_i - p_j) 2e
+  float wx = 0.f, wy = 0.f, wz = 0.f;      // 28-30: pressure force of wall neighbours
+};
+
 // cuda_govering_ns (delta_ns.cu:179-267); MODE 1/2 fuses the prediction /
 // correction of the same particle, written into `out` (a different buffer,
-// so neighbours still read the unintegrated state).
-template <int GF, int MODE>
+// so neighbours still read the unintegrated state).  FEAT (predictor stage
+// of the learned form) also accumulates and writes the FeatOut aggregates.
+template <int GF, int MODE, bool FEAT = false>
 __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
-                                                          zsph_ptc_t out) {
+                                                          zsph_ptc_t out, FeatOut fo) {
   extern __shared__ __align__(16) unsigned char dsm[];
   PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
@@ -613,7 +633,9 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
   float4 g0 = dg[i];
+  const float4 g0i = g0;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  FeatAcc fa;
   auto use = [&](const NbG& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
     const float rr2 = dist2(dx, dy, dz);
@@ -627,6 +649,25 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
     const float frm = fr * m * ir1;
     acc.w += r0 * dvdx * frm;
     float vt = -(p0 + p1) * frm * ir0;
+    if constexpr (FEAT) {
+      if (fi) {
+        const bool fj = fluid_of(nb.pr.w);
+        const float e = rr2 * rcp_fast(rr2 + p.eta2);
+        const float wW = -0.2f * p.h2 * frm * a * (2.0f * q + 1.0f);  // (m/rho_j) W, W = adh a^4 (2q+1)
+        fa.gx += frm * dx; fa.gy += frm * dy; fa.gz += frm * dz;
+        fa.lap_p += frm * (p0 - p1) * 2.0f * e;
+        if (fj) {
+          const float dd = frm * (nb.dg.w - g0i.w);
+          fa.shep_f += wW;
+          fa.dx += dd * dx; fa.dy += dd * dy; fa.dz += dd * dz;
+          fa.kx += frm * dx; fa.ky += frm * dy; fa.kz += frm * dz;
+          fa.lap_rho += frm * (r0 - r1) * 2.0f * e;
+        } else {
+          fa.shep_w += wW;
+          fa.wx += vt * dx; fa.wy += vt * dy; fa.wz += vt * dz;
+        }
+      }
+    }
     if (fi && fluid_of(nb.pr.w)) {
       const float ire = rcp_fast(rr2 + p.eta2);
       acc.w += p.delta_h_cs * frm * ((r0 - r1) * 2.0f * rr2 * ire - g0.x);
@@ -646,6 +687,48 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
   if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(s.flags, ZSPH_FLAG_NAN);
+  if constexpr (FEAT) {
+    // D: this predictor-stage value minus the particle's previous corrector-stage value
+    const float4 ap = fo.acc_prev ? fo.acc_prev[t.index[i]] : acc;
+    const float4 dp = fi ? make_float4(acc.x - ap.x, acc.y - ap.y, acc.z - ap.z, acc.w - ap.w)
+                         : make_float4(0.f, 0.f, 0.f, 0.f);
+    if (fo.d_out) fo.d_out[i] = dp;
+    float f[kFeat];
+    if (fi) {
+      const float fv[kFeat] = {fa.shep_f, fa.shep_w, fa.gx, fa.gy, fa.gz, g0i.w, fa.dx, fa.dy,
+                               fa.dz, g0i.w * fa.kx, g0i.w * fa.ky, g0i.w * fa.kz, fa.lap_rho, fa.lap_p, acc.x, acc.y,
+                               acc.z, acc.w, vi.x, vi.y, vi.z, r0 - p.rho0, g0i.x, g0i.y,
+                               g0i.z, dp.x, dp.y, dp.z, fa.wx, fa.wy, fa.wz, dp.w};
+#pragma unroll
+      for (int k = 0; k < kFeat; ++k) f[k] = fv[k] * fo.scale[k];
+    } else {
+#pragma unroll
+      for (int k = 0; k < kFeat; ++k) f[k] = 0.f;
+    }
+    if (fo.raw) {
+      float4* dst = reinterpret_cast<float4*>(fo.raw) + (size_t)i * (kFeat / 4);
+#pragma unroll
+      for (int k = 0; k < kFeat / 4; ++k) dst[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
+    }
+    if (fo.tiles) {
+      unsigned char* tile = fo.tiles + (size_t)(i >> 7) * 8192;
+      const int r = i & 127;
+#pragma unroll
+      for (int cb = 0; cb < kFeat / 8; ++cb) {
+        uint32_t u[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int c = cb * 8 + 2 * e;
+          u[e] = fi ? pack_bf16x2((f[c] - fo.mean[c]) * fo.inv_std[c], (f[c + 1] - fo.mean[c + 1]) * fo.inv_std[c + 1])
+                    : 0u;
+        }
+        // element (r, c) of a 128-row operand tile: ((c/8)*16 + r/8)*128 + (r%8)*16 + (c%8)*2
+        *reinterpret_cast<uint4*>(tile + ((cb * 16 + (r >> 3)) << 7) + ((r & 7) << 4)) =
+            make_uint4(u[0], u[1], u[2], u[3]);
+      }
+    }
+    if (fo.acc_copy) fo.acc_copy[i] = acc;
+  }
   if (MODE != 0) integrate_one<MODE>(kp, ptc, out, i, acc);
 }
 
@@ -758,7 +841,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
 
 template <int GF>
 cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t, int mode,
-                         const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
+                         const zsph_ptc_t& out, cudaStream_t st, Prof* pf, const FeatOut* feat) {
   const int nb = thread_blocks(kp.n);
   if (kp.equations == ZSPH_EQ_SIMPLE) {
     const int ss = pair_smem<GF>(0, 0);
@@ -769,9 +852,16 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
     return cudaGetLastError();
   }
   const int sm = pair_smem<GF>(kp.stage_windows ? 3 : 0, kWinCapG);
-  if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
-  if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
-  if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out);
+  if (feat) {
+    if (mode != 1) return cudaErrorInvalidValue;
+    k_governing<GF, 1, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, *feat);
+    mark(pf, "governing_feat", st);
+    return cudaGetLastError();
+  }
+  const FeatOut none{};
+  if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
+  if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
+  if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
   mark(pf, "governing", st);
   return cudaGetLastError();
 }
@@ -816,6 +906,8 @@ cudaError_t init_pair_kernels() {
   setb(k_governing<2, 0>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<2, 1>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<2, 2>, pair_smem<2>(3, kWinCapG));
+  setb(k_governing<1, 1, true>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<2, 1, true>, pair_smem<2>(3, kWinCapG));
   setb(k_boundary_simple<1>, pair_smem<1>(0, 0));
   setb(k_boundary_simple<2>, pair_smem<2>(0, 0));
   setb(k_governing_simple<1, 0>, pair_smem<1>(0, 0));
@@ -843,10 +935,11 @@ cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t&
 }
 
 cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
-                             int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf) {
+                             int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf, const FeatOut* feat) {
   if (kp.n == 0) return cudaSuccess;
-  if (kp.p.grid_factor == 1) return governing_gf<1>(kp, s, ptc, t, mode, out, st, pf);
-  if (kp.p.grid_factor == 2) return governing_gf<2>(kp, s, ptc, t, mode, out, st, pf);
+  if (feat && kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
+  if (kp.p.grid_factor == 1) return governing_gf<1>(kp, s, ptc, t, mode, out, st, pf, feat);
+  if (kp.p.grid_factor == 2) return governing_gf<2>(kp, s, ptc, t, mode, out, st, pf, feat);
   return cudaErrorInvalidValue;
 }
 

@@ -113,8 +113,9 @@ struct MlpArgs {
   // correct
   KParams kp;
   zsph_ptc_t ptc;  // state after the predictor (n+1/2 plus tmp_* = n), corrected in place
-  float4* acc;     // predictor-stage (acc, drho/dt) in, corrector-stage out
-  float4 oa, ob;   // delta = yhat * oa + ob (de-standardized, dimensional)
+  float4* acc;          // predictor-stage (acc, drho/dt) in, corrector-stage out
+  const float4* dprev;  // D: predictor-stage value minus the previous corrector value
+  float4 oa, ob;        // residual = yhat * oa + ob (de-standardized, dimensional)
 };
 
 __device__ __forceinline__ float tanh_mufu(float x) {
@@ -305,11 +306,13 @@ __global__ void __launch_bounds__(128, 1) k_mlp(MlpArgs a) {
       if (row < a.nrows) a.out[row] = make_float4(yh[0], yh[1], yh[2], yh[3]);
     } else if (MODE == kCorrect) {
       if (row < a.nrows && a.ptc.type[row] == 1) {
+        // corrector stage = linear extrapolation a_n + D + learned residual
         float4 acc = a.acc[row];
-        acc.x += fmaf(yh[0], a.oa.x, a.ob.x);
-        acc.y += fmaf(yh[1], a.oa.y, a.ob.y);
-        acc.z += fmaf(yh[2], a.oa.z, a.ob.z);
-        acc.w += fmaf(yh[3], a.oa.w, a.ob.w);
+        const float4 d = a.dprev[row];
+        acc.x += d.x + fmaf(yh[0], a.oa.x, a.ob.x);
+        acc.y += d.y + fmaf(yh[1], a.oa.y, a.ob.y);
+        acc.z += d.z + fmaf(yh[2], a.oa.z, a.ob.z);
+        acc.w += d.w + fmaf(yh[3], a.oa.w, a.ob.w);
         a.acc[row] = acc;
         if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(a.flags, ZSPH_FLAG_NAN);
         integrate_one<2>(a.kp, a.ptc, a.ptc, row, acc);
@@ -521,28 +524,24 @@ uint64_t mix64(uint64_t& s) {
   return z ^ (z >> 31);
 }
 
+__nv_bfloat16* bf(void* p) { return static_cast<__nv_bfloat16*>(p); }
+
 }  // namespace
 }  // namespace zsph
 
-struct zsph_mlp {
-  float* w = nullptr;   // master parameters
-  float* m1 = nullptr;  // Adam moments
-  float* m2 = nullptr;
-  __nv_bfloat16* w1 = nullptr;
-  __nv_bfloat16* w2 = nullptr;
-  __nv_bfloat16* w3p = nullptr;
-  int step = 0;
-};
-
 namespace zsph {
 
-Net mlp_net(const zsph_mlp& m) {
-  return Net{m.w1, m.w2, m.w3p, m.w + kOffB1, m.w + kOffB2, m.w + kOffB3};
+int mlp_sm_count() {
+  return init_mlp_kernels() ? 0 : g_sms;
 }
 
-// learned-corrector epilogue over the state after the predictor (api.cu)
-cudaError_t launch_mlp_correct(const zsph_mlp& m, const KParams& kp, const void* tiles, const zsph_ptc_t& ptc,
-                               float4* acc, float4 oa, float4 ob, int* flags, cudaStream_t st) {
+Net mlp_net(const Mlp& m) {
+  return Net{bf(m.w1), bf(m.w2), bf(m.w3p), m.w + kOffB1, m.w + kOffB2, m.w + kOffB3};
+}
+
+// learned-corrector epilogue over the state after the predictor (learn.cu)
+cudaError_t launch_mlp_correct(const Mlp& m, const KParams& kp, const void* tiles, const zsph_ptc_t& ptc,
+                               float4* acc, const float4* dprev, float4 oa, float4 ob, int* flags, cudaStream_t st) {
   cudaError_t e = init_mlp_kernels();
   if (e) return e;
   MlpArgs a{};
@@ -554,6 +553,7 @@ cudaError_t launch_mlp_correct(const zsph_mlp& m, const KParams& kp, const void*
   a.kp = kp;
   a.ptc = ptc;
   a.acc = acc;
+  a.dprev = dprev;
   a.oa = oa;
   a.ob = ob;
   const int grid = std::min(a.ntiles, 2 * g_sms);
@@ -561,7 +561,7 @@ cudaError_t launch_mlp_correct(const zsph_mlp& m, const KParams& kp, const void*
   return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_forward(const zsph_mlp& m, const void* tiles, int n, float* out, int* flags,
+cudaError_t launch_mlp_forward(const Mlp& m, const void* tiles, int n, float* out, int* flags,
                                cudaStream_t st) {
   cudaError_t e = init_mlp_kernels();
   if (e) return e;
@@ -577,7 +577,7 @@ cudaError_t launch_mlp_forward(const zsph_mlp& m, const void* tiles, int n, floa
   return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_grad(const zsph_mlp& m, const void* tiles, const float* y, const float* w, const int* ids,
+cudaError_t launch_mlp_grad(const Mlp& m, const void* tiles, const float* y, const float* w, const int* ids,
                             int ntiles, float inv_wsum, float* partial, int* nparts, int* flags, cudaStream_t st) {
   cudaError_t e = init_mlp_kernels();
   if (e) return e;
@@ -597,13 +597,13 @@ cudaError_t launch_mlp_grad(const zsph_mlp& m, const void* tiles, const float* y
   return cudaGetLastError();
 }
 
-cudaError_t launch_mlp_adam(zsph_mlp& m, const float* partial, int nparts, float lr, float b1, float b2, float eps,
+cudaError_t launch_mlp_adam(Mlp& m, const float* partial, int nparts, float lr, float b1, float b2, float eps,
                             cudaStream_t st) {
   m.step += 1;
   const float bc1 = (float)(1.0 - std::pow((double)b1, (double)m.step));
   const float bc2 = (float)(1.0 - std::pow((double)b2, (double)m.step));
-  k_adam<<<(kNParam + 255) / 256, 256, 0, st>>>(m.w, m.m1, m.m2, partial, nparts, lr, b1, b2, eps, bc1, bc2, m.w1,
-                                                m.w2, m.w3p);
+  k_adam<<<(kNParam + 255) / 256, 256, 0, st>>>(m.w, m.m1, m.m2, partial, nparts, lr, b1, b2, eps, bc1, bc2, bf(m.w1),
+                                                bf(m.w2), bf(m.w3p));
   return cudaGetLastError();
 }
 
@@ -640,8 +640,16 @@ int zsph_mlp_create(unsigned long long seed, zsph_mlp_t** out) {
   }
   m->m1 = m->w + kNParam;
   m->m2 = m->w + 2 * kNParam;
-  m->w2 = m->w1 + kHid * kIn;
-  m->w3p = m->w2 + kHid * kHid;
+  m->w2 = bf(m->w1) + kHid * kIn;
+  m->w3p = bf(m->w2) + kHid * kHid;
+  for (int k = 0; k < kFeat; ++k) {
+    m->in_mean[k] = 0.f;
+    m->in_inv_std[k] = 1.f;
+  }
+  for (int k = 0; k < kOut; ++k) {
+    m->out_mean[k] = 0.f;
+    m->out_std[k] = 1.f;
+  }
   std::vector<float> h(kNParam, 0.f);
   uint64_t s = seed;
   auto uni = [&](float bound) { return (float)(((mix64(s) >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0) * bound; };
@@ -652,7 +660,7 @@ int zsph_mlp_create(unsigned long long seed, zsph_mlp_t** out) {
   if (!e) e = cudaMemset(m->w1, 0, sizeof(__nv_bfloat16) * (kHid * kIn + kHid * kHid + kOutPad * kHid));
   if (!e) e = cudaMemcpy(m->w, h.data(), sizeof(float) * kNParam, cudaMemcpyHostToDevice);
   if (!e) {
-    k_refresh<<<(kNParam + 255) / 256, 256>>>(m->w, m->w1, m->w2, m->w3p);
+    k_refresh<<<(kNParam + 255) / 256, 256>>>(m->w, bf(m->w1), bf(m->w2), bf(m->w3p));
     e = cudaDeviceSynchronize();
   }
   if (e) {
@@ -675,7 +683,7 @@ int zsph_mlp_set_params(zsph_mlp_t* m, const float* params) {
   if (!m || !params) return fail(ZSPH_EINVAL, "zsph_mlp_set_params: bad argument");
   cudaError_t e = cudaMemcpy(m->w, params, sizeof(float) * kNParam, cudaMemcpyHostToDevice);
   if (!e) {
-    k_refresh<<<(kNParam + 255) / 256, 256>>>(m->w, m->w1, m->w2, m->w3p);
+    k_refresh<<<(kNParam + 255) / 256, 256>>>(m->w, bf(m->w1), bf(m->w2), bf(m->w3p));
     e = cudaDeviceSynchronize();
   }
   return e ? fail_cuda(e, "zsph_mlp_set_params") : ZSPH_OK;
@@ -702,6 +710,25 @@ int zsph_mlp_get_moments(zsph_mlp_t* m, float* m1, float* m2, int* step) {
   if (!e && m2) e = cudaMemcpy(m2, m->m2, sizeof(float) * kNParam, cudaMemcpyDeviceToHost);
   if (step) *step = m->step;
   return e ? fail_cuda(e, "zsph_mlp_get_moments") : ZSPH_OK;
+}
+
+int zsph_mlp_set_norm(zsph_mlp_t* m, const float* in_mean, const float* in_inv_std, const float* out_mean,
+                      const float* out_std) {
+  if (!m || !in_mean || !in_inv_std || !out_mean || !out_std) return fail(ZSPH_EINVAL, "zsph_mlp_set_norm: bad argument");
+  std::memcpy(m->in_mean, in_mean, sizeof m->in_mean);
+  std::memcpy(m->in_inv_std, in_inv_std, sizeof m->in_inv_std);
+  std::memcpy(m->out_mean, out_mean, sizeof m->out_mean);
+  std::memcpy(m->out_std, out_std, sizeof m->out_std);
+  return ZSPH_OK;
+}
+
+int zsph_mlp_get_norm(zsph_mlp_t* m, float* in_mean, float* in_inv_std, float* out_mean, float* out_std) {
+  if (!m) return fail(ZSPH_EINVAL, "zsph_mlp_get_norm: bad argument");
+  if (in_mean) std::memcpy(in_mean, m->in_mean, sizeof m->in_mean);
+  if (in_inv_std) std::memcpy(in_inv_std, m->in_inv_std, sizeof m->in_inv_std);
+  if (out_mean) std::memcpy(out_mean, m->out_mean, sizeof m->out_mean);
+  if (out_std) std::memcpy(out_std, m->out_std, sizeof m->out_std);
+  return ZSPH_OK;
 }
 
 int zsph_mlp_pack(const float* rows, int n, const float* mean, const float* inv_std, void* tiles, void* stream) {

@@ -60,6 +60,23 @@ struct Scratch {
   Shadow sh;
 };
 
+// Learned-corrector inputs written by the predictor-stage governing walk
+// (k_governing<GF, 1, true>): kFeat non-dimensional neighbour aggregates per
+// fluid particle (zeros for walls).  Feature k of particle i is
+// raw = sum_k * scale[k]; the network reads (raw - mean) * inv_std as bf16
+// in the tensor-core tile layout.
+constexpr int kFeat = 32;
+struct FeatOut {
+  float* raw;              // [n][kFeat] raw features, or null
+  unsigned char* tiles;    // ceil(n/128) tiles of standardized bf16 features, or null
+  float4* acc_copy;        // copy of the predictor-stage (acc, drho/dt), or null
+  const float4* acc_prev;  // previous corrector-stage (acc, drho/dt) in the search's source order
+  float4* d_out;           // [n] D = predictor-stage value - previous corrector value (sorted order)
+  float scale[kFeat];
+  float mean[kFeat];
+  float inv_std[kFeat];
+};
+
 // Optional per-launch event markers (profiling): after each kernel launch the
 // launcher records the next event, so event k-1 -> k brackets launch k.
 struct Prof {
@@ -87,7 +104,40 @@ struct Handle {
   zsph_tmp_t graph_tmp{};
   cudaStream_t graph_stream = nullptr;
   std::string err;
+  struct LearnState* learn = nullptr;  // learned-corrector data and scratch (learn.cu)
 };
+
+// learn.cu: frees the handle's learned-corrector state
+void learn_destroy(Handle* h);
+
+// api.cu: one sub-step of the fused path (search `from` into `to`, boundary
+// on `to`, governing of `to` with the integration written into `from`)
+cudaError_t run_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
+                        cudaStream_t st, Prof* pf, const FeatOut* feat);
+
+// mlp.cu
+struct Mlp {
+  float* w = nullptr;   // fp32 master parameters (ZSPH_MLP_NPARAM)
+  float* m1 = nullptr;  // Adam moments
+  float* m2 = nullptr;
+  void* w1 = nullptr;   // bf16 weights [128][32], [128][128], [16][128]
+  void* w2 = nullptr;
+  void* w3p = nullptr;
+  int step = 0;
+  // input / output standardization of the learned corrector
+  float in_mean[kFeat], in_inv_std[kFeat];
+  float out_mean[4], out_std[4];
+};
+cudaError_t launch_mlp_correct(const Mlp& m, const KParams& kp, const void* tiles, const zsph_ptc_t& ptc,
+                               float4* acc, const float4* dprev, float4 oa, float4 ob, int* flags, cudaStream_t st);
+cudaError_t launch_mlp_forward(const Mlp& m, const void* tiles, int n, float* out, int* flags, cudaStream_t st);
+cudaError_t launch_mlp_grad(const Mlp& m, const void* tiles, const float* y, const float* w, const int* ids,
+                            int ntiles, float inv_wsum, float* partial, int* nparts, int* flags, cudaStream_t st);
+cudaError_t launch_mlp_adam(Mlp& m, const float* partial, int nparts, float lr, float b1, float b2, float eps,
+                            cudaStream_t st);
+cudaError_t launch_mlp_pack(const float* rows, int n, const float* mean, const float* inv_std, void* tiles,
+                            cudaStream_t st);
+int mlp_sm_count();
 
 // api.cu: message returned by zsph_last_error(NULL, ...)
 void record_library_error(const std::string& msg);
@@ -109,8 +159,10 @@ cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_
 // one-time kernel attributes (shared-memory windows above 48 KB); call before launches
 cudaError_t init_pair_kernels();
 // mode 0: acc_drhodt only; 1: + prediction into out; 2: + correction into out
+// feat (mode 1, delta equations only): also write the learned-corrector inputs
 cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
-                             int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr);
+                             int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr,
+                             const FeatOut* feat = nullptr);
 cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& tmp, cudaStream_t st);
 cudaError_t launch_nb_counts(const KParams& kp, const Scratch& s, int* nb_boundary, int* nb_governing,
                              cudaStream_t st);
@@ -118,3 +170,7 @@ cudaError_t launch_integrate(const KParams& kp, const Scratch& s, const zsph_ptc
                              int correction, cudaStream_t st);
 
 }  // namespace zsph
+
+// the opaque C types of include/zsph.h
+struct zsph_handle : public zsph::Handle {};
+struct zsph_mlp : public zsph::Mlp {};
