@@ -50,6 +50,8 @@ def parse():
                          "(about 1.3 M particles, for profiling captures that must stay small)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample duration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-corrector leg")
+    ap.add_argument("--learn-epochs", type=int, default=20)
     return ap.parse_args()
 
 
@@ -198,6 +200,52 @@ def cpu_baseline(case, target_s: float) -> dict:
                       f"{dt:.1f} s)"}
 
 
+# ---------------------------------------------------------------- learned form
+def learned_leg(args, dist, sol, stream, sptr, n, ms_plain):
+    """Learned-corrector form on the bench's case: the network is trained on
+    the GPU (own tensor-core kernels) on 200 snapshots of plain dam-break
+    steps at dx = 0.02 (every 10th of 2000 steps after 100 settling steps),
+    then the learned form runs K steps of the bench's case with the plain
+    corrector judging every 10th step (tolerance 1e-2, fallback above it)
+    and, separately, K steps without judging (the network's speed alone)."""
+    import torch
+    import zsph_b200 as z
+    from zsph_b200 import cases
+    t0 = time.perf_counter()
+    c0 = cases.config0()
+    s0 = z.Solver.from_case(c0)
+    s0.run(100)
+    snaps = s0.collect(2000, 10, 200)
+    net = z.Mlp(seed=1)
+    train = s0.train(net, epochs=args.learn_epochs, batch_tiles=148, lr=2e-3, seed=3, val_frac=0.1)
+    s0.close()
+    prep_s = time.perf_counter() - t0
+    K = args.steps
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return dist.max(a.elapsed_time(b)), r
+
+    ms_j, rj = timed(lambda: sol.run_learned(net, K, judge_every=10, tol=1e-2, stream=sptr))
+    ms_u, ru = timed(lambda: sol.run_learned(net, K, judge_every=0, tol=1e-2, stream=sptr))
+    net.close()
+    v_j, v_u = dist.world * n * K / (ms_j / 1e3), dist.world * n * K / (ms_u / 1e3)
+    return {"value": v_j, "unit": "particle-steps/s", "ms_per_step": ms_j / K,
+            "speedup_vs_plain": ms_plain / ms_j, "judge_every": 10, "tol": 1e-2, "run": rj,
+            "unjudged": {"value": v_u, "ms_per_step": ms_u / K, "speedup_vs_plain": ms_plain / ms_u, "run": ru},
+            "train": dict(train, snapshots=snaps, data="dam break dx=0.02 (105,048 particles), plain steps 100-2100, "
+                                                       "every 10th step", prep_seconds=prep_s),
+            "what": "corrector stage = predictor-stage value + (value - previous corrector value) + network "
+                    "residual; judged steps run the plain corrector, compare accelerations (relative L2, fluid) "
+                    "and keep the plain result; above tol the plain corrector runs until a judged step passes"}
+
+
 # ---------------------------------------------------------------- our arm
 def run_ours(args, dist: Dist):
     import ctypes
@@ -293,6 +341,8 @@ def run_ours(args, dist: Dist):
                    "read of the 4-byte device status word), zsph_gpu_to_cpu of pos/vel/rhop/type/table; "
                    "host wall clock, max over ranks"}
 
+    learned = None if args.no_learned else learned_leg(args, dist, sol, stream, sptr, n, ms / K)
+
     cpu = None
     if dist.rank == 0 and not args.no_cpu_baseline:
         cpu = cpu_baseline(case, args.cpu_seconds)
@@ -307,7 +357,7 @@ def run_ours(args, dist: Dist):
                    "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
         "roofline": roofline, "dominant_kernel": dominant, "kernels": kern, "cpu_baseline": cpu,
-        "status_flags": flags,
+        "learned": learned, "status_flags": flags,
     }
     sol.close()
     return line

@@ -372,6 +372,63 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old_, 
                      const zsph_tmp_t* tmp, int nsteps, int judge_every, float tol, zsph_learn_run_stats_t* stats,
                      void* stream);
 
+/* ---- Precision form (no reference counterpart) ----------------------------
+ * zsph_set_precision(h, 1): a particle's position is held as its integer grid
+ * cell (one int per particle, kept on the handle for old_ and new_ and moved
+ * by the search) plus the FP32 offset from the cell's corner, which the pos
+ * arrays then hold instead of absolute coordinates.  Pair distances are
+ * formed as cell difference * grid_size + offset difference, and zsph_step /
+ * zsph_run integrate offsets and move cells.  Needs grid_size_factor 1, the
+ * delta-SPH equations and grid dimensions up to 1023; the fused step entry
+ * points only (zsph_step, zsph_run). */
+int zsph_set_precision(zsph_handle_t* h, int on);
+/* Loads absolute FP64 positions (host, [ptc_num][3]) into old_ as cell +
+ * offset (the precision form must be on). */
+int zsph_precise_load(zsph_handle_t* h, const zsph_ptc_t* old_, const double* pos, void* stream);
+/* Absolute FP64 positions of old_ (host, [ptc_num][3]); also valid with the
+ * precision form off (then the FP32 positions widened). */
+int zsph_precise_positions(zsph_handle_t* h, const zsph_ptc_t* old_, double* pos, void* stream);
+
+/* FP64 global sums over the fluid particles of old_ (and the attached body):
+ * mass, volume sum(m/rho), momentum, kinetic energy, potential energy
+ * -m g z, internal energy of the linear equation of state
+ * m c0^2 (ln(rho/rho0) + rho0/rho - 1). */
+typedef struct {
+  double mass, volume, momentum[3], kinetic, potential, internal;
+  double body_kinetic, body_potential;
+} zsph_conservation_t;
+int zsph_conservation(zsph_handle_t* h, const zsph_ptc_t* old_, zsph_conservation_t* out, void* stream);
+
+/* ---- 6DOF rigid body coupled to the fluid (no reference counterpart) -------
+ * The particles of type 2 whose original index (table[i] + i) lies in
+ * [first, first + count) form one rigid body of the given mass.  They act
+ * as dummy walls (density and pressure extrapolated from the fluid,
+ * delta_ns.cu:61-131) that move with the body.  After every fused
+ * sub-step's governing kernel the fluid's pressure force on each body
+ * particle is summed in FP64 into the body's force and torque about its
+ * centre of mass, the body is advanced in FP64 by the same predictor-
+ * corrector as the fluid (angular acceleration as
+ * Test_6DOF/equation/acc_alpha.cpp:20-33, quaternion rate as
+ * Test_6DOF/equation/time_int.cpp:14-15), and its particles are placed from
+ * its pose.  Inertia: Test_6DOF/equation/rigid_info.cpp:18-39 (about the
+ * particles' centroid, mass shared equally).  Works with and without the
+ * precision form. */
+typedef struct {
+  int first, count;         /* original particle indices of the body */
+  double mass;              /* kg */
+  double pos[3];            /* centre of mass (output: the particles' centroid) */
+  double vel[3], omega[3];  /* linear and angular (world frame) velocity */
+  double q[4];              /* orientation (w, x, y, z) */
+  double force[3], torque[3]; /* output: the last fluid force and torque */
+  double inertia[9];        /* output: body-frame inertia about the centre of mass */
+} zsph_rigid_t;
+/* Attaches the body to the handle using the particles' current positions in
+ * old_ (the body frame is the given orientation); sets the body particles'
+ * velocities from vel and omega. */
+int zsph_rigid_attach(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_rigid_t* body, void* stream);
+/* Current body state. */
+int zsph_rigid_get(zsph_handle_t* h, zsph_rigid_t* body);
+
 /* Plain device-memory helpers for callers without their own CUDA runtime
  * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,
  * deltasph/main.cu:41-45).  kind: 1 host->device, 2 device->host,

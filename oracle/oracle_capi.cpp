@@ -98,7 +98,12 @@ int oracle_max_threads(void) { return omp_get_max_threads(); }
   void oracle_features_##SUF(const Params* p, const State<T>* s, const Tmp<T>* t, const float* scale,       \
                              const T* acc_prev, T* out) {                                           \
     features<T>(*p, *s, *t, scale, acc_prev, out);                                                  \
-  }
+  }                                                                                                 \
+  void oracle_step_rigid_##SUF(const Params* p, State<T>* o, State<T>* w, Tmp<T>* t, Rigid* b, int nsteps, \
+                               int wall_mode) {                                                     \
+    for (int k = 0; k < nsteps; ++k) step_rigid<T>(*p, *o, *w, *t, *b, wall_mode);                  \
+  }                                                                                                 \
+  void oracle_rigid_place_##SUF(const Params* p, State<T>* s, const Rigid* b) { rigid_place<T>(*p, *s, *b); }
 
 ORACLE_INSTANCE(f32, float)
 ORACLE_INSTANCE(f64, double)

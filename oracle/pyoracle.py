@@ -84,6 +84,15 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(_VP)
 
 
+class ORigid(ctypes.Structure):
+    """zsph_oracle::Rigid."""
+    _fields_ = [(n, ctypes.c_double * k) for n, k in (("x", 3), ("v", 3), ("w", 3), ("q", 4), ("xn", 3), ("vn", 3),
+                                                       ("wn", 3), ("qn", 4), ("F", 3), ("T", 3), ("I", 9),
+                                                       ("Iinv", 9))] + \
+               [("M", ctypes.c_double), ("g", ctypes.c_double), ("first", ctypes.c_int), ("count", ctypes.c_int),
+                ("r0", ctypes.POINTER(ctypes.c_double))]
+
+
 class Oracle:
     """One oracle run (FP32 or FP64) on host arrays in the reference layout."""
 
@@ -163,6 +172,49 @@ class Oracle:
         self._fn("features")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
                              _p(sc), _p(ap), _p(out))
         return out
+
+    # ---- rigid body (the product's FP64 6DOF coupling, restated) ----------
+    def attach_rigid(self, first, count, mass, vel=(0, 0, 0), omega=(0, 0, 0), q=(1, 0, 0, 0)):
+        """Centroid, inertia (Test_6DOF/equation/rigid_info.cpp:3-39) and
+        body-frame offsets from the current positions of `old`."""
+        st = self.old
+        ids = st["table"] + np.arange(self.p.ptc_num)
+        sel = (st["type"] == 2) & (ids >= first) & (ids < first + count)
+        x = np.zeros((count, 3))
+        x[ids[sel] - first] = st["pos"][sel].astype(np.float64)
+        c = x.mean(0)
+        r = x - c
+        I = np.zeros((3, 3))
+        for a in range(3):
+            for b in range(3):
+                I[a, b] = -(r[:, a] * r[:, b]).sum()
+        I += np.eye(3) * (r * r).sum()
+        I *= mass / count
+        qq = np.asarray(q, np.float64) / np.linalg.norm(q)
+        w, xx, yy, zz = qq
+        R = np.array([[1 - 2 * (yy * yy + zz * zz), 2 * (xx * yy - w * zz), 2 * (xx * zz + w * yy)],
+                      [2 * (xx * yy + w * zz), 1 - 2 * (xx * xx + zz * zz), 2 * (yy * zz - w * xx)],
+                      [2 * (xx * zz - w * yy), 2 * (yy * zz + w * xx), 1 - 2 * (xx * xx + yy * yy)]])
+        self._r0 = np.ascontiguousarray(r @ R)  # R^T r per row
+        Ib = R.T @ I @ R
+        b = ORigid()
+        for name, v in (("x", c), ("xn", c), ("v", vel), ("vn", vel), ("w", omega), ("wn", omega), ("q", qq),
+                        ("qn", qq), ("I", Ib.ravel()), ("Iinv", np.linalg.inv(Ib).ravel())):
+            getattr(b, name)[:] = list(np.asarray(v, np.float64))
+        b.M, b.g, b.first, b.count = mass, self.p.g, first, count
+        b.r0 = self._r0.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self.rigid = b
+        f = self._fn("rigid_place")
+        f(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self.rigid))
+        return b
+
+    def step_rigid(self, nsteps=1, wall_mode=WALLS_FIRST):
+        self._fn("step_rigid")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
+                               ctypes.byref(self._t), ctypes.byref(self.rigid), _I(nsteps), _I(wall_mode))
+
+    def rigid_state(self) -> dict:
+        b = self.rigid
+        return {k: np.array(getattr(b, k)[:]) for k in ("x", "v", "w", "q", "F", "T")}
 
     # simple-SPH equations (the reference's simplesph target); div(v) is the
     # scalar array self.dofv

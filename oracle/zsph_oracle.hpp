@@ -586,4 +586,156 @@ template <class T> void step_simple(const Params& p, State<T>& o, State<T>& w, T
   correction(p, o, t);
 }
 
+// ---- 6DOF rigid body coupled to the fluid (no reference counterpart) ----
+// Restates the product's FP64 body update (zsph_b200/csrc/precise.cu): the
+// fluid's pressure force on each body particle (type 2, original index in
+// [first, first + count)), summed into force and torque about the centre of
+// mass; predictor / corrector of the pose with the angular acceleration of
+// Test_6DOF/equation/acc_alpha.cpp:20-33 and the quaternion rate of
+// Test_6DOF/equation/time_int.cpp:14-15; body particles placed from the pose.
+struct Rigid {
+  double x[3], v[3], w[3], q[4], xn[3], vn[3], wn[3], qn[4], F[3], T[3], I[9], Iinv[9], M, g;
+  int first, count;
+  const double* r0;  // [count][3] body-frame offsets
+};
+
+inline void rig_rot(const double* q, double* R) {
+  const double w = q[0], x = q[1], y = q[2], z = q[3];
+  R[0] = 1 - 2 * (y * y + z * z); R[1] = 2 * (x * y - w * z);     R[2] = 2 * (x * z + w * y);
+  R[3] = 2 * (x * y + w * z);     R[4] = 1 - 2 * (x * x + z * z); R[5] = 2 * (y * z - w * x);
+  R[6] = 2 * (x * z - w * y);     R[7] = 2 * (y * z + w * x);     R[8] = 1 - 2 * (x * x + y * y);
+}
+inline void rig_mv(const double* A, const double* v, double* r) {
+  for (int a = 0; a < 3; ++a) r[a] = A[3 * a] * v[0] + A[3 * a + 1] * v[1] + A[3 * a + 2] * v[2];
+}
+inline void rig_mtv(const double* A, const double* v, double* r) {
+  for (int a = 0; a < 3; ++a) r[a] = A[a] * v[0] + A[3 + a] * v[1] + A[6 + a] * v[2];
+}
+inline void rig_cross(const double* a, const double* b, double* r) {
+  r[0] = a[1] * b[2] - a[2] * b[1];
+  r[1] = a[2] * b[0] - a[0] * b[2];
+  r[2] = a[0] * b[1] - a[1] * b[0];
+}
+inline void rig_quat(const double* q0, const double* w, const double* qr, double dt, double* out) {
+  const double a = -w[0] * qr[1] - w[1] * qr[2] - w[2] * qr[3];
+  const double b = w[0] * qr[0] + w[1] * qr[3] - w[2] * qr[2];
+  const double c = -w[0] * qr[3] + w[1] * qr[0] + w[2] * qr[1];
+  const double d = w[0] * qr[2] - w[1] * qr[1] + w[2] * qr[0];
+  double r[4] = {q0[0] + 0.5 * dt * a, q0[1] + 0.5 * dt * b, q0[2] + 0.5 * dt * c, q0[3] + 0.5 * dt * d};
+  const double inv = 1.0 / std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2] + r[3] * r[3]);
+  for (int k = 0; k < 4; ++k) out[k] = r[k] * inv;
+}
+
+template <class T> void rigid_force(const Params& p, const State<T>& s, const Tmp<T>& t, Rigid& b) {
+  const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m;
+  double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0};
+  for (int i = 0; i < p.ptc_num; ++i) {
+    const int k = s.table[i] + i - b.first;
+    if (s.type[i] != 2 || k < 0 || k >= b.count) continue;
+    const T px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
+    const T r0 = s.rhop[2 * i], p0 = s.rhop[2 * i + 1];
+    T f[3] = {0, 0, 0};
+    for_each_candidate(p, t, i, p.grid_factor, [&](int j) {
+      if (s.type[j] != 1) return;
+      const T dx = px - s.pos[3 * j], dy = py - s.pos[3 * j + 1], dz = pz - s.pos[3 * j + 2];
+      const T rr2 = rr2_of(dx, dy, dz);
+      const T q = std::sqrt(rr2) / h;
+      if (!(q <= (T)2)) return;
+      const T a = (T)1 - q / (T)2;
+      const T fr = (T)-5 * adh * a * a * a / h2;
+      const T vt = -(p0 + s.rhop[2 * j + 1]) * m * fr / (r0 * s.rhop[2 * j]);
+      f[0] += vt * dx;
+      f[1] += vt * dy;
+      f[2] += vt * dz;
+    });
+    const double fv[3] = {(double)m * f[0], (double)m * f[1], (double)m * f[2]};
+    const double r[3] = {(double)px - b.x[0], (double)py - b.x[1], (double)pz - b.x[2]};
+    double tq[3];
+    rig_cross(r, fv, tq);
+    for (int a = 0; a < 3; ++a) {
+      F[a] += fv[a];
+      Tq[a] += tq[a];
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    b.F[a] = F[a];
+    b.T[a] = Tq[a];
+  }
+}
+
+inline void rigid_advance(Rigid& b, int mode, double half_dt) {
+  double acc[3] = {b.F[0] / b.M, b.F[1] / b.M, b.F[2] / b.M + b.g};
+  double R[9], tmp[3], tmp2[3], Iw[3], alpha[3];
+  rig_rot(b.q, R);
+  rig_mtv(R, b.w, tmp);
+  rig_mv(b.I, tmp, tmp2);
+  rig_mv(R, tmp2, Iw);
+  rig_cross(b.w, Iw, tmp);
+  for (int a = 0; a < 3; ++a) tmp[a] = b.T[a] - tmp[a];
+  rig_mtv(R, tmp, tmp2);
+  rig_mv(b.Iinv, tmp2, tmp);
+  rig_mv(R, tmp, alpha);
+  if (mode == 1) {
+    for (int a = 0; a < 3; ++a) { b.xn[a] = b.x[a]; b.vn[a] = b.v[a]; b.wn[a] = b.w[a]; }
+    for (int a = 0; a < 4; ++a) b.qn[a] = b.q[a];
+    double qh[4];
+    rig_quat(b.qn, b.wn, b.qn, half_dt, qh);
+    for (int a = 0; a < 3; ++a) {
+      b.x[a] = b.xn[a] + b.vn[a] * half_dt;
+      b.v[a] = b.vn[a] + acc[a] * half_dt;
+      b.w[a] = b.wn[a] + alpha[a] * half_dt;
+    }
+    for (int a = 0; a < 4; ++a) b.q[a] = qh[a];
+  } else {
+    const double dt = 2.0 * half_dt;
+    double q1[4];
+    rig_quat(b.qn, b.w, b.q, dt, q1);
+    for (int a = 0; a < 3; ++a) {
+      b.x[a] = b.xn[a] + b.v[a] * dt;
+      b.v[a] = b.vn[a] + acc[a] * dt;
+      b.w[a] = b.wn[a] + alpha[a] * dt;
+    }
+    for (int a = 0; a < 4; ++a) b.q[a] = q1[a];
+  }
+}
+
+template <class T> void rigid_place(const Params& p, State<T>& s, const Rigid& b) {
+  double R[9];
+  rig_rot(b.q, R);
+  for (int i = 0; i < p.ptc_num; ++i) {
+    const int k = s.table[i] + i - b.first;
+    if (s.type[i] != 2 || k < 0 || k >= b.count) continue;
+    double r[3], w[3];
+    rig_mv(R, b.r0 + 3 * (size_t)k, r);
+    rig_cross(b.w, r, w);
+    for (int a = 0; a < 3; ++a) {
+      s.pos[3 * i + a] = (T)(b.x[a] + r[a]);
+      s.vel[3 * i + a] = (T)(b.v[a] + w[a]);
+    }
+  }
+}
+
+// One step with the body: the plain step's call order, the body's force,
+// update and placement after each sub-step's governing / integration.
+template <class T> void step_rigid(const Params& p, State<T>& o, State<T>& w, Tmp<T>& t, Rigid& b, int wall_mode) {
+  hash(p, o, t);
+  sort_index(p, t);
+  sort_data(p, o, w, t);
+  boundary(p, w, t, wall_mode);
+  governing(p, w, t);
+  rigid_force(p, w, t, b);
+  rigid_advance(b, 1, (double)p.half_dt);
+  prediction(p, w, t);
+  rigid_place(p, w, b);
+  hash(p, w, t);
+  sort_index(p, t);
+  sort_data(p, w, o, t);
+  boundary(p, o, t, wall_mode);
+  governing(p, o, t);
+  rigid_force(p, o, t, b);
+  rigid_advance(b, 2, (double)p.half_dt);
+  correction(p, o, t);
+  rigid_place(p, o, b);
+}
+
 }  // namespace zsph_oracle

@@ -113,8 +113,26 @@ class LearnRunStats(ctypes.Structure):
                [(n, ctypes.c_float) for n in ("err_max", "err_mean", "err_last")]
 
 
+class RigidBody(ctypes.Structure):
+    """zsph_rigid_t."""
+    _fields_ = [("first", ctypes.c_int), ("count", ctypes.c_int), ("mass", ctypes.c_double)] + \
+               [(n, ctypes.c_double * k) for n, k in (("pos", 3), ("vel", 3), ("omega", 3), ("q", 4), ("force", 3),
+                                                       ("torque", 3), ("inertia", 9))]
+
+
+class Conservation(ctypes.Structure):
+    """zsph_conservation_t."""
+    _fields_ = [("mass", ctypes.c_double), ("volume", ctypes.c_double), ("momentum", ctypes.c_double * 3)] + \
+               [(n, ctypes.c_double) for n in ("kinetic", "potential", "internal", "body_kinetic",
+                                               "body_potential")]
+
+
 def _as_dict(s: ctypes.Structure) -> dict:
-    return {k: getattr(s, k) for k, _ in s._fields_}
+    out = {}
+    for k, _ in s._fields_:
+        v = getattr(s, k)
+        out[k] = np.array(v[:]) if isinstance(v, ctypes.Array) else v
+    return out
 
 
 _HP = ctypes.c_void_p
@@ -180,6 +198,12 @@ _sig = {
     "zsph_learn_train": (_I, [_HP, _VP, _I, _I, _F, ctypes.c_ulonglong, _F, ctypes.POINTER(LearnTrainStats), _VP]),
     "zsph_run_learned": (_I, [_HP, _VP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _F,
                               ctypes.POINTER(LearnRunStats), _VP]),
+    "zsph_set_precision": (_I, [_HP, _I]),
+    "zsph_precise_load": (_I, [_HP, ctypes.POINTER(Ptc), _VP, _VP]),
+    "zsph_precise_positions": (_I, [_HP, ctypes.POINTER(Ptc), _VP, _VP]),
+    "zsph_conservation": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Conservation), _VP]),
+    "zsph_rigid_attach": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(RigidBody), _VP]),
+    "zsph_rigid_get": (_I, [_HP, ctypes.POINTER(RigidBody)]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -431,6 +455,40 @@ class Solver:
 
     def launches_per_step(self) -> int:
         return int(lib.zsph_launches_per_step(self.h))
+
+    # ---- precision form, FP64 sums, rigid body ------------------------------
+    def set_precision(self, on: bool = True, pos64=None) -> None:
+        """Switch the precision form on (cell + offset positions); pos64:
+        exact absolute positions of old_ to load (default: the FP32 ones)."""
+        self._call(lib.zsph_set_precision, 1 if on else 0)
+        if on:
+            if pos64 is None:
+                pos64 = self.download("old").pos
+            p = np.ascontiguousarray(pos64, np.float64)
+            self._call(lib.zsph_precise_load, ctypes.byref(self.old), p.ctypes.data, None)
+
+    def positions64(self, which: str = "old") -> np.ndarray:
+        out = np.empty((self.n, 3), np.float64)
+        self._call(lib.zsph_precise_positions, ctypes.byref(self._buf(which)), out.ctypes.data, None)
+        return out
+
+    def conservation(self) -> dict:
+        c = Conservation()
+        self._call(lib.zsph_conservation, ctypes.byref(self.old), ctypes.byref(c), None)
+        return _as_dict(c)
+
+    def attach_body(self, first: int, count: int, mass: float, vel=(0, 0, 0), omega=(0, 0, 0),
+                    q=(1, 0, 0, 0)) -> dict:
+        b = RigidBody()
+        b.first, b.count, b.mass = int(first), int(count), float(mass)
+        b.vel[:], b.omega[:], b.q[:] = list(map(float, vel)), list(map(float, omega)), list(map(float, q))
+        self._call(lib.zsph_rigid_attach, ctypes.byref(self.old), ctypes.byref(b), None)
+        return self.body()
+
+    def body(self) -> dict:
+        b = RigidBody()
+        self._call(lib.zsph_rigid_get, ctypes.byref(b))
+        return _as_dict(b)
 
     # ---- learned-corrector form (zsph_learn_*, zsph_run_learned) ----------
     def feature_scales(self) -> np.ndarray:

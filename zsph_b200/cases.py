@@ -32,6 +32,8 @@ class Case:
     n_fluid: int
     n_wall: int
     name: str
+    pos64: np.ndarray | None = None  # exact (FP64) positions, for the precision form
+    body: dict | None = None         # rigid body: first, count, mass (floating-body case)
 
     @property
     def n(self) -> int:
@@ -102,6 +104,65 @@ def dam_break(dx: float = 0.02, water=(0.6, 0.6, 1.2), tank=(1.6, 0.6, 1.2), lay
     dt = cfl * h / c0
     js = _json(dx, lx, ly, lz, dt, n, len(pos_f), len(pos_w), end_step, **phys)
     return Case(js, st, len(pos_f), len(pos_w), f"dam_break_dx{dx:g}")
+
+
+def floating_body(dx: float = 0.01, tank=(4.0, 1.0, 1.0), depth: float = 0.5, cube: float = 0.2,
+                  body_rho: float = 500.0, drop: float = 0.05, cube_x: float = 1.0, layers: int = 3,
+                  cfl: float = 0.2, end_step: int = 5000, **phys) -> Case:
+    """Still water of the given depth in a tank, walls as in dam_break, and a
+    cube of side `cube` (type 2 particles on the same lattice) centred at
+    (cube_x, tank_y/2) with its bottom `drop` above the surface.  dx = 0.01
+    gives 2,000,000 fluid, 432,708 wall and 8,000 body particles.  Order:
+    fluid, walls, body; case.body = {first, count, mass}."""
+    g = phys.get("g", -9.81)
+    rho0 = phys.get("rho0", 1000.0)
+    cs_factor = phys.get("cs_factor", 10.0)
+    h_factor = phys.get("h_factor", 1.3)
+    lx, ly, lz = tank
+    nx, ny, nz = (int(round(v / dx)) for v in (lx, ly, depth))
+    tx, ty, tz = (int(round(v / dx)) for v in (lx, ly, lz))
+    i, j, k = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
+    pos_f = (np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64) + 0.5) * dx
+    ii, jj, kk = np.meshgrid(np.arange(-layers, tx + layers), np.arange(-layers, ty + layers),
+                             np.arange(-layers, tz), indexing="ij")
+    ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
+    outside = (ii < 0) | (ii >= tx) | (jj < 0) | (jj >= ty) | (kk < 0)
+    pos_w = (np.stack([ii[outside], jj[outside], kk[outside]], axis=1).astype(np.float64) + 0.5) * dx
+    nc = int(round(cube / dx))
+    a, b, c = np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij")
+    corner = np.array([cube_x - cube / 2, ly / 2 - cube / 2, depth + drop])
+    pos_b = corner + (np.stack([a.ravel(), b.ravel(), c.ravel()], axis=1).astype(np.float64) + 0.5) * dx
+    c0 = cs_factor * math.sqrt(abs(g) * lz)
+    H = nz * dx
+
+    def hydro(z):
+        p = rho0 * abs(g) * np.clip(H - z, 0.0, None)
+        return rho0 + p / (c0 * c0), p
+
+    rf, pf = hydro(pos_f[:, 2])
+    rw, pw = hydro(pos_w[:, 2])
+    rb, pb = np.full(len(pos_b), rho0), np.zeros(len(pos_b))
+    pos64 = np.concatenate([pos_f, pos_w, pos_b])
+    rho = np.concatenate([rf, rw, rb]).astype(np.float32)
+    prs = np.concatenate([pf, pw, pb]).astype(np.float32)
+    typ = np.concatenate([np.ones(len(pos_f), np.int32), np.zeros(len(pos_w), np.int32),
+                          np.full(len(pos_b), 2, np.int32)])
+    n = len(typ)
+    st = State(pos=pos64.astype(np.float32), vel=np.zeros((n, 3), np.float32),
+               rhop=np.stack([rho, prs], axis=1).astype(np.float32), type=typ, table=np.zeros(n, np.int32),
+               tmp_pos=np.zeros((n, 3), np.float32), tmp_vel=np.zeros((n, 3), np.float32),
+               tmp_rhop=np.zeros((n, 2), np.float32))
+    h = h_factor * dx
+    dt = cfl * h / c0
+    js = _json(dx, lx, ly, lz, dt, n, len(pos_f), len(pos_w), end_step, **phys)
+    js.rigid_ptc_num = len(pos_b)
+    body = {"first": len(pos_f) + len(pos_w), "count": len(pos_b), "mass": body_rho * cube ** 3}
+    return Case(js, st, len(pos_f), len(pos_w), f"floating_body_dx{dx:g}", pos64=pos64, body=body)
+
+
+def config2() -> Case:
+    """Floating body at dx = 0.01 m: 2,000,000 fluid + 432,708 wall + 8,000 body particles, 5000 steps."""
+    return floating_body(0.01)
 
 
 def config0() -> Case:

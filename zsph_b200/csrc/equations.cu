@@ -289,11 +289,30 @@ __device__ __forceinline__ bool row_can_hit(const KParams& kp, int c, float4 pi,
   return d2 <= kp.r2hi * 1.001f;
 }
 
+// Precision form: neighbour j's packed shadow moved into the frame of cell
+// ci (positions are offsets from the own cell's corner; neighbouring cells
+// differ by at most two in each coordinate, so k * gs is exact and the sum
+// rounds once, at the scale of a few cells).
+__device__ __forceinline__ float4 shifted(const KParams& kp, float4 pj, int cj, int3 ci) {
+  const int3 c = unpack_cell(cj);
+  const float gs = kp.p.grid_size;
+  pj.x += (float)(c.x - ci.x) * gs;
+  pj.y += (float)(c.y - ci.y) * gs;
+  pj.z += (float)(c.z - ci.z) * gs;
+  return pj;
+}
+template <bool PRECISE>
+__device__ __forceinline__ float4 shadow_pr(const KParams& kp, const Scratch& s, int j, int3 ci) {
+  const float4 pj = s.sh.pr[j];
+  return PRECISE ? shifted(kp, pj, kp.c3n[j], ci) : pj;
+}
+
 // Wall pressure contribution of fluid neighbour j of wall particle i
 // (delta_ns.cu:67-85), with the reference's IEEE sqrt and division.
+template <bool PRECISE = false>
 __device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, float4 pi, int j, float& rsum,
-                                          float& wsum) {
-  const float4 pj = s.sh.pr[j];
+                                          float& wsum, int3 ci = int3{0, 0, 0}) {
+  const float4 pj = shadow_pr<PRECISE>(kp, s, j, ci);
   if (!fluid_of(pj.w)) return;
   const zsph_gpu_param_t& p = kp.p;
   const float dz = pi.z - pj.z;
@@ -349,7 +368,7 @@ constexpr int kLstStride = kMaxNb + 8;   // uint16 entries per lane row of the s
 // With WALL, every non-fluid particle then extrapolates its (rho, p) from
 // the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
 // summed in the reference's visit order, and publishes it in the shadows.
-template <int GF, bool WALL>
+template <int GF, bool WALL, bool PRECISE = false>
 __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   static_assert(NR <= 32, "one lane per stencil row");
@@ -364,6 +383,12 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
   if (c >= kp.G) return;  // uniform per warp
   const int ca = s.cell_lb[c], cb = s.cell_lb[c + 1];
   if (ca >= cb) return;
+  int3 cc{0, 0, 0};  // precision form: the warp's cell, the frame of its particles
+  if (PRECISE) {
+    cc.z = c / kp.XY;
+    cc.y = (c - cc.z * kp.XY) / kp.p.grid_xdim;
+    cc.x = c - cc.z * kp.XY - cc.y * kp.p.grid_xdim;
+  }
   int rs = 0, re = 0;
   if (lane < NR) row_range<GF>(kp, t, c, lane, rs, re);
   s_rows[wid][lane] = rs;
@@ -386,7 +411,7 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
         for (int h = 0; h < 2; ++h) {
           const int j = k0 + 32 * h + lane;
           float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
-          if (j < b) q = s.sh.pr[j];
+          if (j < b) q = shadow_pr<PRECISE>(kp, s, j, cc);
           sx[32 * h + lane] = q.x;
           sy[32 * h + lane] = q.y;
           sz[32 * h + lane] = q.z;
@@ -441,7 +466,8 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
         for (int k = 0; k < cnt; ++k) {
           const unsigned e = lst[k];
           const int r = (int)(e >> kRowShift);
-          if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum);
+          if (Stencil<GF>::boundary_row(r))
+            wall_term<PRECISE>(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum, cc);
         }
       } else {
         for (int r = 0; r < NR; ++r) {
@@ -450,8 +476,9 @@ __global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch 
           row_range<GF>(kp, t, c, r, a, b);
           for (int j = a; j < b; ++j) {
             if (j == i) continue;
-            const float4 pj = s.sh.pr[j];
-            if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+            const float4 pj = shadow_pr<PRECISE>(kp, s, j, cc);
+            if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z)))
+              wall_term<PRECISE>(kp, s, pi, j, rsum, wsum, cc);
           }
         }
       }
@@ -505,15 +532,16 @@ template <int GF> struct PairSmem {
 
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
-template <int GF>
+template <int GF, bool PRECISE = false>
 __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
   extern __shared__ __align__(16) unsigned char dsm[];
   PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
   const bool act = i < kp.n;
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
   bool staged = false;
-  if (GF == 1 && kp.stage_windows) {
+  if (GF == 1 && kp.stage_windows && !PRECISE) {
     const float4* const src[2] = {s.sh.pr, s.sh.vp};
     staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapB, src, act, sm.rs, sm.re, sm.fb, s.flags,
                                              [](int r) { return Stencil<GF>::boundary_row(r); });
@@ -545,7 +573,7 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
                          [&](int q) { return NbB1{win[q], win[kWinCapB + q]}; }, use1);
   else
     walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
-                         [&](int q) { return NbB1{s.sh.pr[q], s.sh.vp[q]}; }, use1);
+                         [&](int q) { return NbB1{shadow_pr<PRECISE>(kp, s, q, ci), s.sh.vp[q]}; }, use1);
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
                     Lxy * Lxy * Lzz;
@@ -580,7 +608,8 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, 
   if (staged)
     walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, [&](int q) { return win[q]; }, use2);
   else
-    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return s.sh.pr[q]; }, use2);
+    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
+                           [&](int q) { return shadow_pr<PRECISE>(kp, s, q, ci); }, use2);
   reinterpret_cast<float4*>(t.dofv_grandrho)[i] = make_float4(gx, gy, gz, divv);
   if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
 }
@@ -610,7 +639,8 @@ struct FeatAcc {
 // correction of the same particle, written into `out` (a different buffer,
 // so neighbours still read the unintegrated state).  FEAT (predictor stage
 // of the learned form) also accumulates and writes the FeatOut aggregates.
-template <int GF, int MODE, bool FEAT = false>
+// PRECISE: precision form (cell + offset positions).
+template <int GF, int MODE, bool FEAT = false, bool PRECISE = false>
 __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
                                                           zsph_ptc_t out, FeatOut fo) {
   extern __shared__ __align__(16) unsigned char dsm[];
@@ -618,9 +648,10 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
   const bool act = i < kp.n;
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
   const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
   bool staged = false;
-  if (GF == 1 && kp.stage_windows) {
+  if (GF == 1 && kp.stage_windows && !PRECISE) {
     const float4* const src[3] = {s.sh.pr, s.sh.vp, dg};
     staged = stage_window<Stencil<GF>::NR, 3>(*sm.wh, sm.win, kWinCapG, src, act, sm.rs, sm.re, sm.fb, s.flags,
                                              [](int) { return true; });
@@ -636,6 +667,8 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   const float4 g0i = g0;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   FeatAcc fa;
+  const bool rig = kp.rigid_f != nullptr && ptc.type[i] == 2;
+  float3 rf = make_float3(0.f, 0.f, 0.f);
   auto use = [&](const NbG& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
     const float rr2 = dist2(dx, dy, dz);
@@ -668,6 +701,11 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
         }
       }
     }
+    if (rig && fluid_of(nb.pr.w)) {  // the fluid's pressure force on a body particle
+      rf.x += vt * dx;
+      rf.y += vt * dy;
+      rf.z += vt * dz;
+    }
     if (fi && fluid_of(nb.pr.w)) {
       const float ire = rcp_fast(rr2 + p.eta2);
       acc.w += p.delta_h_cs * frm * ((r0 - r1) * 2.0f * rr2 * ire - g0.x);
@@ -683,7 +721,8 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
                          [&](int q) { return NbG{win[q], win[kWinCapG + q], win[2 * kWinCapG + q]}; }, use);
   else
     walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
-                         [&](int q) { return NbG{s.sh.pr[q], s.sh.vp[q], dg[q]}; }, use);
+                         [&](int q) { return NbG{shadow_pr<PRECISE>(kp, s, q, ci), s.sh.vp[q], dg[q]}; }, use);
+  if (rig) kp.rigid_f[i] = make_float4(rf.x, rf.y, rf.z, 0.f);
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
   if (!isfinite(acc.x + acc.y + acc.z + acc.w)) atomicOr(s.flags, ZSPH_FLAG_NAN);
@@ -729,7 +768,7 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
     }
     if (fo.acc_copy) fo.acc_copy[i] = acc;
   }
-  if (MODE != 0) integrate_one<MODE>(kp, ptc, out, i, acc);
+  if (MODE != 0) integrate_one<MODE, PRECISE>(kp, ptc, out, i, acc);
 }
 
 // ---- simple-SPH equations (the reference's simplesph target) --------------
@@ -828,6 +867,14 @@ inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 template <int GF>
 cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                         cudaStream_t st, Prof* pf) {
+  if (kp.c3o) {  // precision form (grid factor 1, delta equations)
+    if (GF != 1 || kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
+    k_nblist<1, true, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+    mark(pf, "nblist_wall", st);
+    k_boundary<1, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
+    mark(pf, "boundary", st);
+    return cudaGetLastError();
+  }
   k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
   if (kp.equations == ZSPH_EQ_SIMPLE)
@@ -851,6 +898,16 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
     mark(pf, "governing", st);
     return cudaGetLastError();
   }
+  if (kp.c3o) {  // precision form (grid factor 1, delta equations, no learned features)
+    if (GF != 1 || feat) return cudaErrorInvalidValue;
+    const FeatOut none{};
+    const int s1 = pair_smem<1>(0, 0);
+    if (mode == 0) k_governing<1, 0, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    if (mode == 1) k_governing<1, 1, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    if (mode == 2) k_governing<1, 2, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    mark(pf, "governing", st);
+    return cudaGetLastError();
+  }
   const int sm = pair_smem<GF>(kp.stage_windows ? 3 : 0, kWinCapG);
   if (feat) {
     if (mode != 1) return cudaErrorInvalidValue;
@@ -868,7 +925,12 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
 
 template <int GF>
 cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
-  k_nblist<GF, false><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+  if (kp.c3o) {
+    if (GF != 1) return cudaErrorInvalidValue;
+    k_nblist<1, false, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+  } else {
+    k_nblist<GF, false><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+  }
   return cudaGetLastError();
 }
 

@@ -6,9 +6,27 @@
 
 namespace zsph {
 
+// Precision form: move offset o (cell coordinate c) into [0, gs) again after
+// an update smaller than one cell; a cell outside the grid becomes kCellMask,
+// which the next hash treats as out of the grid.
+__device__ __forceinline__ void renormalize(float& o, int& c, float gs, int dim) {
+  if (o >= gs) {
+    o -= gs;
+    c += 1;
+  } else if (o < 0.0f) {
+    o += gs;
+    c -= 1;
+  }
+  if (c < 0 || c >= dim) c = kCellMask;
+}
+
 // time_int.cu:3-48 / :50-92 for one fluid particle, writing into `out`
 // (which may alias `in`).  Non-fluid particles are copied unchanged.
-template <int MODE>
+// PRECISE (precision form, out != in): positions are cell offsets; the
+// correction is x(n+1) = x(n+1/2) + v(n+1/2) dt - v(n) dt/2 (equal to
+// time_int.cu:65-73 in exact arithmetic, and free of the old cell), and the
+// cell of the result is written to kp.c3o.
+template <int MODE, bool PRECISE = false>
 __device__ __forceinline__ void integrate_one(const KParams& kp, const zsph_ptc_t& in, const zsph_ptc_t& out,
                                               int i, float4 acc) {
   const zsph_gpu_param_t& p = kp.p;
@@ -29,9 +47,15 @@ __device__ __forceinline__ void integrate_one(const KParams& kp, const zsph_ptc_
       nv.x += acc.x * p.half_dt; nv.y += acc.y * p.half_dt; nv.z += acc.z * p.half_dt;
       nrp.x += acc.w * p.half_dt;
     } else {  // correction
-      np.x = tp.x + vel.x * p.half_dt * 2.0f;
-      np.y = tp.y + vel.y * p.half_dt * 2.0f;
-      np.z = tp.z + vel.z * p.half_dt * 2.0f;
+      if (PRECISE) {
+        np.x = pos.x + (vel.x * p.half_dt * 2.0f - tv.x * p.half_dt);
+        np.y = pos.y + (vel.y * p.half_dt * 2.0f - tv.y * p.half_dt);
+        np.z = pos.z + (vel.z * p.half_dt * 2.0f - tv.z * p.half_dt);
+      } else {
+        np.x = tp.x + vel.x * p.half_dt * 2.0f;
+        np.y = tp.y + vel.y * p.half_dt * 2.0f;
+        np.z = tp.z + vel.z * p.half_dt * 2.0f;
+      }
       nv.x = tv.x + acc.x * p.half_dt * 2.0f;
       nv.y = tv.y + acc.y * p.half_dt * 2.0f;
       nv.z = tv.z + acc.z * p.half_dt * 2.0f;
@@ -41,6 +65,17 @@ __device__ __forceinline__ void integrate_one(const KParams& kp, const zsph_ptc_
     nrp.y = p.cs2 * (nrp.x - p.rho0);
   } else if (alias) {
     return;
+  }
+  if (PRECISE) {
+    int c = kp.c3n[i];
+    if (type == 1) {
+      int3 cc = unpack_cell(c);
+      renormalize(np.x, cc.x, p.grid_size, p.grid_xdim);
+      renormalize(np.y, cc.y, p.grid_size, p.grid_ydim);
+      renormalize(np.z, cc.z, p.grid_size, p.grid_zdim);
+      c = pack_cell(cc.x, cc.y, cc.z);
+    }
+    kp.c3o[i] = c;
   }
   out.pos[3 * i] = np.x; out.pos[3 * i + 1] = np.y; out.pos[3 * i + 2] = np.z;
   out.vel[3 * i] = nv.x; out.vel[3 * i + 1] = nv.y; out.vel[3 * i + 2] = nv.z;

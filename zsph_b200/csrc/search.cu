@@ -46,13 +46,29 @@ __device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, flo
 // origin with zero velocity and (rho0, 0); its key becomes 0.
 __device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t& s, int i, int* flags) {
   const zsph_gpu_param_t& p = kp.p;
-  const float x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
-  int h = cell_hash(p, x, y, z);
-  if (h < p.grid_hash_min || h > p.grid_hash_max) {
+  int h;
+  bool out;
+  if (kp.c3o) {  // precision form: the cell is stored, the offset is local
+    const int3 c = unpack_cell(kp.c3o[i]);
+    out = c.x >= p.grid_xdim || c.y >= p.grid_ydim || c.z >= p.grid_zdim;
+    h = (c.z * p.grid_ydim + c.y) * p.grid_xdim + c.x;
+  } else {
+    const float x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
+    h = cell_hash(p, x, y, z);
+    out = h < p.grid_hash_min || h > p.grid_hash_max;
+  }
+  if (out) {
     s.type[i] = 100;
-    s.pos[3 * i] = p.grid_xmin;
-    s.pos[3 * i + 1] = p.grid_ymin;
-    s.pos[3 * i + 2] = p.grid_zmin;
+    if (kp.c3o) {  // the grid origin: cell (0, 0, 0), offset 0
+      kp.c3o[i] = 0;
+      s.pos[3 * i] = 0.0f;
+      s.pos[3 * i + 1] = 0.0f;
+      s.pos[3 * i + 2] = 0.0f;
+    } else {
+      s.pos[3 * i] = p.grid_xmin;
+      s.pos[3 * i + 1] = p.grid_ymin;
+      s.pos[3 * i + 2] = p.grid_zmin;
+    }
     s.vel[3 * i] = 0.0f;
     s.vel[3 * i + 1] = 0.0f;
     s.vel[3 * i + 2] = 0.0f;
@@ -347,6 +363,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratc
   t.index[dst] = i;
   t.hash[dst] = c;
   gather_one(o, w, sc.sh, i, dst);
+  if (kp.c3o) kp.c3n[dst] = kp.c3o[i];
 }
 
 // Drop-in sort_index, last step: sorted keys and carried values.

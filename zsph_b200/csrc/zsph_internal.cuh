@@ -31,7 +31,27 @@ struct KParams {
   float c_fr;            // -5 * adh / h2, the factor of grad W / r
   int stage_windows;     // 1: pair kernels stage neighbour windows in shared memory (TMA bulk copies)
   int equations;         // ZSPH_EQ_DELTA or ZSPH_EQ_SIMPLE
+  // Precision form (null otherwise): a particle's position is its grid cell
+  // (hx | hy << 10 | hz << 20) plus the FP32 offset from that cell's corner
+  // held in pos.  c3o belongs to the buffer searched from (old_), c3n to the
+  // buffer searched into (new_).
+  int* c3o;
+  int* c3n;
+  // Rigid body attached (null otherwise): the governing kernel writes, for
+  // each type-2 particle, the pressure acceleration from its fluid
+  // neighbours alone (the fluid's force on the body per unit particle mass).
+  float4* rigid_f;
 };
+
+// packed integer cell coordinates of the precision form
+constexpr int kCellBits = 10;
+constexpr int kCellMask = (1 << kCellBits) - 1;
+__host__ __device__ __forceinline__ int pack_cell(int hx, int hy, int hz) {
+  return hx | (hy << kCellBits) | (hz << (2 * kCellBits));
+}
+__host__ __device__ __forceinline__ int3 unpack_cell(int c) {
+  return make_int3(c & kCellMask, (c >> kCellBits) & kCellMask, (c >> (2 * kCellBits)) & kCellMask);
+}
 
 // Packed per-particle shadows of the sorted state, written by the gather
 // (16-byte loads in the pair kernels).  pr = {x, y, z, +-rho} with the sign
@@ -105,10 +125,17 @@ struct Handle {
   cudaStream_t graph_stream = nullptr;
   std::string err;
   struct LearnState* learn = nullptr;  // learned-corrector data and scratch (learn.cu)
+  int* c3buf[2] = {nullptr, nullptr};  // precision form: cells of old_ / new_ (precise.cu)
+  struct RigidState* rigid = nullptr;  // attached rigid body (precise.cu)
 };
 
 // learn.cu: frees the handle's learned-corrector state
 void learn_destroy(Handle* h);
+// precise.cu: frees the precision-form and rigid-body state
+void precise_destroy(Handle* h);
+// precise.cu: FP64 force/torque sum, body update and placement after a
+// fused sub-step's governing kernel (mode 1 predictor, 2 corrector)
+cudaError_t rigid_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, int mode, cudaStream_t st);
 
 // api.cu: one sub-step of the fused path (search `from` into `to`, boundary
 // on `to`, governing of `to` with the integration written into `from`)
