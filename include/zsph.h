@@ -372,6 +372,33 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old_, 
                      const zsph_tmp_t* tmp, int nsteps, int judge_every, float tol, zsph_learn_run_stats_t* stats,
                      void* stream);
 
+/* ---- Batched form (no reference counterpart) ------------------------------
+ * One handle over nscenes independent cases (grid_size_factor 1, delta-SPH
+ * equations).  Scene s owns the particles [P_s, P_s + ptc_num_s) of the
+ * handle's buffers, P_s = the sum of the earlier scenes' ptc_num (scenes
+ * stored one after another, each in its own particle order), and its own
+ * cells; every kernel launch of zsph_step / zsph_run covers all scenes, so
+ * a step is one graph whatever the number of scenes.  A particle that
+ * leaves its scene's grid is parked in that scene's first cell.  Per scene
+ * the results are those of a handle created for that scene alone. */
+int zsph_create_batch(const zsph_gpu_param_t* scenes, const int* grid_num, int nscenes, zsph_handle_t** out);
+
+/* ---- Autotuner (no reference counterpart) ----------------------------------
+ * Times every candidate launch shape of the grid-factor-1 step -- cells
+ * (warps) per CTA of the neighbour-list build {2, 4}, minimum resident CTAs
+ * per SM of the governing kernel {1, 6, 8} (its register budget), steps per
+ * graph replay of zsph_run {1, 4} -- for trial_steps steps each on the
+ * handle's buffers, restores old_ and the carried tmp arrays after every
+ * trial, and keeps the fastest for the handle's later zsph_run calls. */
+typedef struct {
+  int list_cells_per_cta, governing_min_ctas, steps_per_graph;
+  float ms_per_step;  /* of the chosen shapes */
+  float ms_default;   /* of the untuned shapes */
+  int candidates;
+} zsph_tune_t;
+int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
+                  int trial_steps, zsph_tune_t* out, void* stream);
+
 /* ---- Precision form (no reference counterpart) ----------------------------
  * zsph_set_precision(h, 1): a particle's position is held as its integer grid
  * cell (one int per particle, kept on the handle for old_ and new_ and moved

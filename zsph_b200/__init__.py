@@ -127,6 +127,13 @@ class Conservation(ctypes.Structure):
                                                "body_potential")]
 
 
+class TuneResult(ctypes.Structure):
+    """zsph_tune_t."""
+    _fields_ = [("list_cells_per_cta", ctypes.c_int), ("governing_min_ctas", ctypes.c_int),
+                ("steps_per_graph", ctypes.c_int), ("ms_per_step", ctypes.c_float), ("ms_default", ctypes.c_float),
+                ("candidates", ctypes.c_int)]
+
+
 def _as_dict(s: ctypes.Structure) -> dict:
     out = {}
     for k, _ in s._fields_:
@@ -204,6 +211,9 @@ _sig = {
     "zsph_conservation": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Conservation), _VP]),
     "zsph_rigid_attach": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(RigidBody), _VP]),
     "zsph_rigid_get": (_I, [_HP, ctypes.POINTER(RigidBody)]),
+    "zsph_create_batch": (_I, [ctypes.POINTER(GpuParam), _IP, _I, ctypes.POINTER(_HP)]),
+    "zsph_autotune": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I,
+                           ctypes.POINTER(TuneResult), _VP]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -313,6 +323,40 @@ class Solver:
         s = cls(gp, cp.grid_num)
         s.upload(case.state)
         return s
+
+    @classmethod
+    def from_batch(cls, case_list) -> "Solver":
+        """Batched form (zsph_create_batch) over independent cases, stored
+        one after another; `scene_ptc` holds each scene's particle count."""
+        gps, gnums = [], []
+        for c in case_list:
+            cp, gp = params_from_json(c.json)
+            gps.append(gp)
+            gnums.append(int(cp.grid_num))
+        arr = (GpuParam * len(gps))(*gps)
+        gn = (ctypes.c_int * len(gnums))(*gnums)
+        s = cls.__new__(cls)
+        s.n = int(sum(int(g.ptc_num) for g in gps))
+        s.G = int(sum(gnums))
+        s.gp = gps[0]
+        s.scene_ptc = [int(g.ptc_num) for g in gps]
+        s.old, s.new, s.tmp = Ptc(), Ptc(), Tmp()
+        check(lib.zsph_alloc_ptc(ctypes.byref(s.old), s.n))
+        check(lib.zsph_alloc_ptc(ctypes.byref(s.new), s.n))
+        check(lib.zsph_alloc_tmp(ctypes.byref(s.tmp), s.n, s.G))
+        h = _HP()
+        check(lib.zsph_create_batch(arr, gn, len(gps), ctypes.byref(h)))
+        s.h = h
+        cat = lambda k: np.concatenate([np.asarray(getattr(c.state, k)) for c in case_list])
+        s.upload(State(pos=cat("pos"), vel=cat("vel"), rhop=cat("rhop"), type=cat("type"), table=cat("table"),
+                       tmp_pos=cat("tmp_pos"), tmp_vel=cat("tmp_vel"), tmp_rhop=cat("tmp_rhop")))
+        return s
+
+    def autotune(self, trial_steps: int = 3, stream=None) -> dict:
+        r = TuneResult()
+        self._call(lib.zsph_autotune, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+                   int(trial_steps), ctypes.byref(r), stream)
+        return _as_dict(r)
 
     def close(self) -> None:
         if getattr(self, "h", None):

@@ -165,6 +165,34 @@ def config2() -> Case:
     return floating_body(0.01)
 
 
+def batch_scenes(nscenes: int = 256, seed: int = 2026, fluid_range=(5000, 60000), max_tries: int = 1_000_000):
+    """Seeded dam-break scenes of uneven sizes: column width w ~ U[0.2, 0.6] m,
+    aspect a = height / width ~ U[0.5, 2], dx ~ U[0.01, 0.02] m, column depth
+    = w, height a w; a draw is kept when the height lies in [0.2, 0.6] m and
+    the fluid count in fluid_range.  Tank 2.5 w x w x 1.2 a w, same physics
+    and walls as dam_break.  Returns (cases, draws)."""
+    rng = np.random.default_rng(seed)
+    out, draws = [], []
+    tries = 0
+    while len(out) < nscenes and tries < max_tries:
+        tries += 1
+        w, a, dx = rng.uniform(0.2, 0.6), rng.uniform(0.5, 2.0), rng.uniform(0.01, 0.02)
+        hgt = a * w
+        if not (0.2 <= hgt <= 0.6):
+            continue
+        n = round(w / dx) * round(w / dx) * round(hgt / dx)
+        if not (fluid_range[0] <= n <= fluid_range[1]):
+            continue
+        c = dam_break(dx, water=(w, w, hgt), tank=(2.5 * w, w, 1.2 * hgt), end_step=1000)
+        if not (fluid_range[0] <= c.n_fluid <= fluid_range[1]):
+            continue
+        out.append(c)
+        draws.append({"w": w, "aspect": a, "dx": dx})
+    if len(out) < nscenes:
+        raise ValueError("not enough scenes within the ranges")
+    return out, draws
+
+
 def config0() -> Case:
     """Plain dam break, dx = 0.02 m: 54,000 fluid + 51,048 wall particles, 2000 steps."""
     return dam_break(0.02, end_step=2000)

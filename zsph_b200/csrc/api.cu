@@ -313,12 +313,76 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   return ZSPH_OK;
 }
 
+int zsph_create_batch(const zsph_gpu_param_t* scenes, const int* grid_num, int nscenes, zsph_handle_t** out) {
+  if (!scenes || !grid_num || !out || nscenes <= 0) return set_err(nullptr, ZSPH_EINVAL, "zsph_create_batch: bad argument");
+  *out = nullptr;
+  std::vector<SceneDev> tab((size_t)nscenes);
+  std::vector<int> base(2 * (size_t)nscenes + 2, 0);
+  long long N = 0, G = 0;
+  for (int s = 0; s < nscenes; ++s) {
+    std::string why;
+    if (validate_gparam(&scenes[s], grid_num[s], why))
+      return set_err(nullptr, ZSPH_EINVAL, "zsph_create_batch: scene " + std::to_string(s) + ": " + why);
+    if (scenes[s].grid_factor != 1)
+      return set_err(nullptr, ZSPH_EINVAL, "zsph_create_batch: every scene needs grid_size_factor 1");
+    KParams k{};
+    fill_kparams(k, scenes[s], grid_num[s]);
+    SceneDev& d = tab[s];
+    d.p = scenes[s];
+    d.p.grid_hash_min = (int)G;  // the scene's cells in batch coordinates
+    d.p.grid_hash_max = (int)(G + grid_num[s] - 1);
+    d.XY = k.XY;
+    d.r2lo = k.r2lo;
+    d.r2hi = k.r2hi;
+    d.r2max = k.r2max;
+    d.inv_h = k.inv_h;
+    d.inv_gs = k.inv_gs;
+    d.c_fr = k.c_fr;
+    base[s] = (int)N;
+    base[nscenes + 1 + s] = (int)G;
+    N += scenes[s].ptc_num;
+    G += grid_num[s];
+    if (N > 0x7fffffffLL / kMaxNb || G > 0x7fffffffLL - 2)
+      return set_err(nullptr, ZSPH_EINVAL, "zsph_create_batch: batch too large");
+  }
+  base[nscenes] = (int)N;
+  base[2 * nscenes + 1] = (int)G;
+  // the handle sees one scene of N particles over a 1-D grid of G cells
+  zsph_gpu_param_t all = scenes[0];
+  all.ptc_num = (int)N;
+  all.grid_xdim = (int)G;
+  all.grid_ydim = 1;
+  all.grid_zdim = 1;
+  all.grid_hash_min = 0;
+  all.grid_hash_max = (int)G - 1;
+  zsph_handle_t* h = nullptr;
+  if (int rc = zsph_create(&all, (int)G, &h)) return rc;
+  cudaError_t e = cudaMalloc(&h->scene_tab, sizeof(SceneDev) * nscenes);
+  if (!e) e = cudaMalloc(&h->scene_base, sizeof(int) * base.size());
+  if (!e) e = cudaMemcpy(h->scene_tab, tab.data(), sizeof(SceneDev) * nscenes, cudaMemcpyHostToDevice);
+  if (!e) e = cudaMemcpy(h->scene_base, base.data(), sizeof(int) * base.size(), cudaMemcpyHostToDevice);
+  if (e) {
+    const int code = cuda_fail(nullptr, "zsph_create_batch", e);
+    zsph_destroy(h);
+    return code;
+  }
+  h->kp.scenes = h->scene_tab;
+  h->kp.scene_pbase = h->scene_base;
+  h->kp.scene_cbase = h->scene_base + nscenes + 1;
+  h->kp.nscenes = nscenes;
+  h->kp.stage_windows = 0;
+  *out = h;
+  return ZSPH_OK;
+}
+
 void zsph_destroy(zsph_handle_t* h) {
   if (!h) return;
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
   learn_destroy(h);
   precise_destroy(h);
+  cudaFree(h->scene_tab);
+  cudaFree(h->scene_base);
   free_scratch(h->s);
   delete h;
 }
@@ -462,7 +526,8 @@ int zsph_run(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const z
     if (!h->graph_stream) ZCHECK(h, "zsph_run stream", cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
     ZCHECK(h, "zsph_run capture", cudaStreamBeginCapture(h->graph_stream, cudaStreamCaptureModeThreadLocal));
-    cudaError_t le = step_launches(h, *o, *w, *tmp, h->graph_stream);
+    cudaError_t le = cudaSuccess;
+    for (int k = 0; k < h->graph_steps && !le; ++k) le = step_launches(h, *o, *w, *tmp, h->graph_stream);
     cudaError_t ce = cudaStreamEndCapture(h->graph_stream, &g);
     if (le) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run launch", le); }
     if (ce) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run end capture", ce); }
@@ -473,7 +538,107 @@ int zsph_run(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const z
     h->graph_new = *w;
     h->graph_tmp = *tmp;
   }
-  for (int k = 0; k < nsteps; ++k) ZCHECK(h, "zsph_run launch", cudaGraphLaunch(h->graph, h->last_stream));
+  const int gs = std::max(h->graph_steps, 1);
+  for (int k = 0; k < nsteps / gs; ++k) ZCHECK(h, "zsph_run launch", cudaGraphLaunch(h->graph, h->last_stream));
+  for (int k = 0; k < nsteps % gs; ++k) ZCHECK(h, "zsph_run step", step_launches(h, *o, *w, *tmp, h->last_stream));
+  return ZSPH_OK;
+}
+
+int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp, int trial_steps,
+                  zsph_tune_t* out, void* stream) {
+  ENTRY_CHECKS(h);
+  if (trial_steps <= 0) return set_err(h, ZSPH_EINVAL, "zsph_autotune: trial_steps must be positive");
+  if (int rc = check_ptc(h, o)) return rc;
+  if (int rc = check_ptc(h, w)) return rc;
+  if (int rc = check_tmp(h, tmp)) return rc;
+  if (h->rigid) return set_err(h, ZSPH_EINVAL, "zsph_autotune: detach the rigid body first");
+  cudaStream_t st = as_stream(stream);
+  h->last_stream = st;
+  const size_t n = (size_t)h->kp.n, G = (size_t)h->kp.G;
+  // the state a step reads or carries over: old_, the cell bounds, the precision cells
+  struct Piece { void* p; size_t bytes; };
+  const Piece pieces[] = {{o->pos, 12 * n}, {o->vel, 12 * n}, {o->rhop, 8 * n}, {o->tmp_pos, 12 * n},
+                          {o->tmp_vel, 12 * n}, {o->tmp_rhop, 8 * n}, {o->type, 4 * n}, {o->table, 4 * n},
+                          {tmp->acc_drhodt, 16 * n}, {tmp->dofv_grandrho, 16 * n}, {tmp->grid_start, 4 * G},
+                          {tmp->grid_end, 4 * G}, {h->kp.c3o, h->kp.c3o ? 4 * n : 0}};
+  size_t total = 0;
+  for (const Piece& pc : pieces) total += pc.p ? pc.bytes : 0;
+  unsigned char* save = nullptr;
+  ZCHECK(h, "zsph_autotune save", cudaMalloc(&save, total ? total : 1));
+  auto copy = [&](bool to_save) -> cudaError_t {
+    size_t off = 0;
+    for (const Piece& pc : pieces) {
+      if (!pc.p || !pc.bytes) continue;
+      cudaError_t e = to_save ? cudaMemcpyAsync(save + off, pc.p, pc.bytes, cudaMemcpyDeviceToDevice, st)
+                              : cudaMemcpyAsync(pc.p, save + off, pc.bytes, cudaMemcpyDeviceToDevice, st);
+      if (e) return e;
+      off += pc.bytes;
+    }
+    return cudaSuccess;
+  };
+  const int cws[] = {2, 4}, minbs[] = {1, 6, 8}, spgs[] = {1, 4};
+  zsph_tune_t best{};
+  best.ms_per_step = 1e30f;
+  float ms_default = 0.f;
+  int count = 0;
+  const KParams kp0 = h->kp;
+  const int gs0 = h->graph_steps;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = copy(true);
+  if (!e) e = cudaEventCreate(&e0);
+  if (!e) e = cudaEventCreate(&e1);
+  for (int cw : cws)
+    for (int mb : minbs)
+      for (int spg : spgs) {
+        if (e) break;
+        h->kp.tune_cw = cw;
+        h->kp.tune_minb = mb;
+        h->graph_steps = spg;
+        if (h->graph) {
+          cudaGraphExecDestroy(h->graph);
+          h->graph = nullptr;
+        }
+        e = copy(false);
+        if (!e && zsph_run(h, o, w, tmp, spg, stream) != ZSPH_OK) e = cudaErrorUnknown;  // capture + warm-up
+        const int launches = (trial_steps + spg - 1) / spg;
+        if (!e) e = cudaEventRecord(e0, st);
+        if (!e && zsph_run(h, o, w, tmp, launches * spg, stream) != ZSPH_OK) e = cudaErrorUnknown;
+        if (!e) e = cudaEventRecord(e1, st);
+        if (!e) e = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (!e) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e) break;
+        ms /= (float)(launches * spg);
+        ++count;
+        if (cw == 4 && mb == (h->kp.scenes ? 1 : 6) && spg == 1) ms_default = ms;  // the untuned shapes
+        if (ms < best.ms_per_step) {
+          best.ms_per_step = ms;
+          best.list_cells_per_cta = cw;
+          best.governing_min_ctas = mb;
+          best.steps_per_graph = spg;
+        }
+      }
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  cudaError_t re = copy(false);
+  if (!re) re = cudaStreamSynchronize(st);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(save);
+  if (e || re || count == 0) {
+    h->kp = kp0;
+    h->graph_steps = gs0;
+    if (e == cudaErrorUnknown) return ZSPH_ECUDA;  // the run's own error is in zsph_last_error
+    return cuda_fail(h, "zsph_autotune", e ? e : re);
+  }
+  h->kp.tune_cw = best.list_cells_per_cta;
+  h->kp.tune_minb = best.governing_min_ctas;
+  h->graph_steps = best.steps_per_graph;
+  best.candidates = count;
+  best.ms_default = ms_default;
+  if (out) *out = best;
   return ZSPH_OK;
 }
 

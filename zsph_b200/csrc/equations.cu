@@ -368,19 +368,22 @@ constexpr int kLstStride = kMaxNb + 8;   // uint16 entries per lane row of the s
 // With WALL, every non-fluid particle then extrapolates its (rho, p) from
 // the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
 // summed in the reference's visit order, and publishes it in the shadows.
-template <int GF, bool WALL, bool PRECISE = false>
-__global__ void __launch_bounds__(kCellWarps * 32) k_nblist(KParams kp, Scratch s, zsph_tmp_t t) {
+template <int GF, bool WALL, bool PRECISE = false, bool BATCH = false, int CW = kCellWarps>
+__global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   static_assert(NR <= 32, "one lane per stencil row");
-  __shared__ __align__(16) float s_x[kCellWarps][64];
-  __shared__ __align__(16) float s_y[kCellWarps][64];
-  __shared__ __align__(16) float s_z[kCellWarps][64];
-  __shared__ __align__(16) uint16_t s_lst[kCellWarps][32][kLstStride];
-  __shared__ int s_rows[kCellWarps][32];
-  __shared__ int s_cnt[kCellWarps][32];
+  __shared__ __align__(16) float s_x[CW][64];
+  __shared__ __align__(16) float s_y[CW][64];
+  __shared__ __align__(16) float s_z[CW][64];
+  __shared__ __align__(16) uint16_t s_lst[CW][32][kLstStride];
+  __shared__ int s_rows[CW][32];
+  __shared__ int s_cnt[CW][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int c = blockIdx.x * kCellWarps + wid;
-  if (c >= kp.G) return;  // uniform per warp
+  const int c = blockIdx.x * CW + wid;
+  if (c >= kp_arg.G) return;  // uniform per warp
+  KParams kp_scene;  // batched form: the parameters of the cell's scene
+  if constexpr (BATCH) kp_scene = kp_of_cell(kp_arg, c);
+  const KParams& kp = BATCH ? kp_scene : kp_arg;
   const int ca = s.cell_lb[c], cb = s.cell_lb[c + 1];
   if (ca >= cb) return;
   int3 cc{0, 0, 0};  // precision form: the warp's cell, the frame of its particles
@@ -532,11 +535,14 @@ template <int GF> struct PairSmem {
 
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
-template <int GF, bool PRECISE = false>
-__global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
+template <int GF, bool PRECISE = false, bool BATCH = false>
+__global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
   extern __shared__ __align__(16) unsigned char dsm[];
   PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  KParams kp_scene;  // batched form: the parameters of the particle's scene
+  if constexpr (BATCH) kp_scene = kp_of_particle(kp_arg, i);
+  const KParams& kp = BATCH ? kp_scene : kp_arg;
   const bool act = i < kp.n;
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
@@ -640,12 +646,18 @@ struct FeatAcc {
 // so neighbours still read the unintegrated state).  FEAT (predictor stage
 // of the learned form) also accumulates and writes the FeatOut aggregates.
 // PRECISE: precision form (cell + offset positions).
-template <int GF, int MODE, bool FEAT = false, bool PRECISE = false>
-__global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
-                                                          zsph_ptc_t out, FeatOut fo) {
+// MINB: minimum resident CTAs per SM (register budget); the default six
+// give 80 registers without spills for the plain variants.
+template <int GF, int MODE, bool FEAT = false, bool PRECISE = false, bool BATCH = false, bool RIGID = false,
+          int MINB = (FEAT || BATCH) ? 1 : 6>
+__global__ void __launch_bounds__(kPairBlock, MINB)
+    k_governing(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t, zsph_ptc_t out, FeatOut fo) {
   extern __shared__ __align__(16) unsigned char dsm[];
   PairSmem<GF> sm(dsm);
   const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  KParams kp_scene;  // batched form: the parameters of the particle's scene
+  if constexpr (BATCH) kp_scene = kp_of_particle(kp_arg, i);
+  const KParams& kp = BATCH ? kp_scene : kp_arg;
   const bool act = i < kp.n;
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
@@ -667,7 +679,7 @@ __global__ void __launch_bounds__(kPairBlock) k_governing(KParams kp, Scratch s,
   const float4 g0i = g0;
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   FeatAcc fa;
-  const bool rig = kp.rigid_f != nullptr && ptc.type[i] == 2;
+  const bool rig = RIGID && ptc.type[i] == 2;
   float3 rf = make_float3(0.f, 0.f, 0.f);
   auto use = [&](const NbG& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
@@ -864,9 +876,42 @@ __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc
 inline int cell_blocks(int G) { return (G + kCellWarps - 1) / kCellWarps; }
 inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 
+// list build (grid factor 1) with the tuned number of cells per CTA
+template <bool WALL, bool BATCH>
+void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
+  // (eight cells per CTA would exceed the 48 KB of static shared memory)
+  switch (kp.tune_cw) {
+    case 2: k_nblist<1, WALL, false, BATCH, 2><<<(kp.G + 1) / 2, 64, 0, st>>>(kp, s, t); break;
+    default: k_nblist<1, WALL, false, BATCH, 4><<<(kp.G + 3) / 4, 128, 0, st>>>(kp, s, t); break;
+  }
+}
+
+// governing (grid factor 1, fused prediction / correction, no shared-memory
+// windows) with the tuned register budget
+template <int MODE, bool BATCH>
+void launch_governing_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                            const zsph_ptc_t& out, cudaStream_t st) {
+  const FeatOut none{};
+  const int nb = thread_blocks(kp.n), sm = pair_smem<1>(0, 0);
+  switch (kp.tune_minb) {
+    case 1: k_governing<1, MODE, false, false, BATCH, false, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
+    case 6: k_governing<1, MODE, false, false, BATCH, false, 6><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
+    case 8: k_governing<1, MODE, false, false, BATCH, false, 8><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
+    default: k_governing<1, MODE, false, false, BATCH><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
+  }
+}
+
 template <int GF>
 cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                         cudaStream_t st, Prof* pf) {
+  if (kp.scenes) {  // batched form (grid factor 1, delta equations)
+    if (GF != 1 || kp.equations != ZSPH_EQ_DELTA || kp.c3o) return cudaErrorInvalidValue;
+    launch_nblist_tuned<true, true>(kp, s, t, st);
+    mark(pf, "nblist_wall", st);
+    k_boundary<1, false, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
+    mark(pf, "boundary", st);
+    return cudaGetLastError();
+  }
   if (kp.c3o) {  // precision form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
     k_nblist<1, true, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
@@ -875,7 +920,8 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
     mark(pf, "boundary", st);
     return cudaGetLastError();
   }
-  k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+  if (GF == 1) launch_nblist_tuned<true, false>(kp, s, t, st);
+  else k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
   if (kp.equations == ZSPH_EQ_SIMPLE)
     k_boundary_simple<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, ptc, t);
@@ -898,13 +944,28 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
     mark(pf, "governing", st);
     return cudaGetLastError();
   }
+  if (kp.scenes) {  // batched form (grid factor 1, delta equations, no learned features)
+    if (GF != 1 || feat || kp.c3o) return cudaErrorInvalidValue;
+    const FeatOut none{};
+    const int s1 = pair_smem<1>(0, 0);
+    if (mode == 0) k_governing<1, 0, false, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    if (mode == 1) launch_governing_tuned<1, true>(kp, s, ptc, t, out, st);
+    if (mode == 2) launch_governing_tuned<2, true>(kp, s, ptc, t, out, st);
+    mark(pf, "governing", st);
+    return cudaGetLastError();
+  }
   if (kp.c3o) {  // precision form (grid factor 1, delta equations, no learned features)
     if (GF != 1 || feat) return cudaErrorInvalidValue;
     const FeatOut none{};
     const int s1 = pair_smem<1>(0, 0);
     if (mode == 0) k_governing<1, 0, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
-    if (mode == 1) k_governing<1, 1, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
-    if (mode == 2) k_governing<1, 2, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    if (kp.rigid_f) {  // floating body: also the fluid's force on its particles
+      if (mode == 1) k_governing<1, 1, false, true, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+      if (mode == 2) k_governing<1, 2, false, true, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    } else {
+      if (mode == 1) k_governing<1, 1, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+      if (mode == 2) k_governing<1, 2, false, true><<<nb, kPairBlock, s1, st>>>(kp, s, ptc, t, out, none);
+    }
     mark(pf, "governing", st);
     return cudaGetLastError();
   }
@@ -916,6 +977,19 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
     return cudaGetLastError();
   }
   const FeatOut none{};
+  if (kp.rigid_f && mode != 0) {  // floating body, absolute positions
+    if (GF != 1) return cudaErrorInvalidValue;
+    if (mode == 1) k_governing<1, 1, false, false, false, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
+    if (mode == 2) k_governing<1, 2, false, false, false, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
+    mark(pf, "governing", st);
+    return cudaGetLastError();
+  }
+  if (GF == 1 && !kp.stage_windows && mode != 0) {
+    if (mode == 1) launch_governing_tuned<1, false>(kp, s, ptc, t, out, st);
+    if (mode == 2) launch_governing_tuned<2, false>(kp, s, ptc, t, out, st);
+    mark(pf, "governing", st);
+    return cudaGetLastError();
+  }
   if (mode == 0) k_governing<GF, 0><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
   if (mode == 1) k_governing<GF, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
   if (mode == 2) k_governing<GF, 2><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none);
@@ -925,7 +999,10 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
 
 template <int GF>
 cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
-  if (kp.c3o) {
+  if (kp.scenes) {
+    if (GF != 1) return cudaErrorInvalidValue;
+    launch_nblist_tuned<false, true>(kp, s, t, st);
+  } else if (kp.c3o) {
     if (GF != 1) return cudaErrorInvalidValue;
     k_nblist<1, false, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   } else {
@@ -969,6 +1046,8 @@ cudaError_t init_pair_kernels() {
   setb(k_governing<2, 1>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<2, 2>, pair_smem<2>(3, kWinCapG));
   setb(k_governing<1, 1, true>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<1, 1, false, false, false, true>, pair_smem<1>(3, kWinCapG));
+  setb(k_governing<1, 2, false, false, false, true>, pair_smem<1>(3, kWinCapG));
   setb(k_governing<2, 1, true>, pair_smem<2>(3, kWinCapG));
   setb(k_boundary_simple<1>, pair_smem<1>(0, 0));
   setb(k_boundary_simple<2>, pair_smem<2>(0, 0));

@@ -53,9 +53,11 @@ __device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t
     out = c.x >= p.grid_xdim || c.y >= p.grid_ydim || c.z >= p.grid_zdim;
     h = (c.z * p.grid_ydim + c.y) * p.grid_xdim + c.x;
   } else {
+    // batched form: the scene's cells start at grid_hash_min (0 for one scene)
     const float x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
     h = cell_hash(p, x, y, z);
-    out = h < p.grid_hash_min || h > p.grid_hash_max;
+    out = h < 0 || h > p.grid_hash_max - p.grid_hash_min;
+    h += p.grid_hash_min;
   }
   if (out) {
     s.type[i] = 100;
@@ -74,7 +76,7 @@ __device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t
     s.vel[3 * i + 2] = 0.0f;
     s.rhop[2 * i] = p.rho0;
     s.rhop[2 * i + 1] = 0.0f;
-    h = 0;
+    h = kp.scenes ? p.grid_hash_min : 0;  // the scene's first cell (batched form)
     atomicOr(flags, ZSPH_FLAG_KILLED);
   }
   return h;
@@ -94,18 +96,20 @@ __device__ __forceinline__ int warp_ticket(int* cnt, int key, unsigned active) {
 }
 
 // Drop-in cuda_ptc_hash: hash + identity index (hash.cu:3-26).
-__global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp, zsph_ptc_t s, zsph_tmp_t t, int* flags) {
+__global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp_in, zsph_ptc_t s, zsph_tmp_t t, int* flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= kp.n) return;
+  if (i >= kp_in.n) return;
+  const KParams kp = kp_of_particle(kp_in, i);
   t.hash[i] = hash_and_kill(kp, s, i, flags);
   t.index[i] = i;
 }
 
 // Fused search, step 1: hash + kill + per-cell ticket.
-__global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp, zsph_ptc_t s, Scratch sc) {
+__global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp_in, zsph_ptc_t s, Scratch sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned active = __ballot_sync(0xffffffffu, i < kp.n);
-  if (i >= kp.n) return;
+  const unsigned active = __ballot_sync(0xffffffffu, i < kp_in.n);
+  if (i >= kp_in.n) return;
+  const KParams kp = kp_of_particle(kp_in, i);
   const int h = hash_and_kill(kp, s, i, sc.flags);
   sc.key[i] = h;
   sc.ticket[i] = warp_ticket(sc.cnt, h, active);

@@ -41,7 +41,57 @@ struct KParams {
   // each type-2 particle, the pressure acceleration from its fluid
   // neighbours alone (the fluid's force on the body per unit particle mass).
   float4* rigid_f;
+  // Batched form (null otherwise): independent scenes, scene s owning the
+  // particles [pbase[s], pbase[s+1]) and the cells [cbase[s], cbase[s+1]);
+  // kernels resolve their scene and use its parameters (scene_kp).
+  const struct SceneDev* scenes;
+  const int* scene_pbase;
+  const int* scene_cbase;
+  int nscenes;
+  // Launch shapes chosen by zsph_autotune (0 = the default): cells (warps)
+  // per CTA of the list build (2, 4) and the governing kernel's minimum
+  // resident CTAs per SM (1, 6, 8), i.e. its register budget.
+  int tune_cw;
+  int tune_minb;
 };
+
+// One scene of the batched form: its case constants as KParams holds them.
+struct SceneDev {
+  zsph_gpu_param_t p;  // grid_hash_min/max: the scene's cells in batch coordinates
+  int XY;
+  float r2lo, r2hi, r2max, inv_h, inv_gs, c_fr;
+};
+
+// scene owning index v: the last s with base[s] <= v (base ascending, nscenes + 1 entries)
+__device__ __forceinline__ int scene_of(const int* base, int nscenes, int v) {
+  int lo = 0, hi = nscenes - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(base + mid) <= v) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+// the kernel parameters of scene s (batch-wide particle and cell counts)
+__device__ __forceinline__ KParams scene_kp(const KParams& kp, int s) {
+  KParams r = kp;
+  const SceneDev& d = kp.scenes[s];
+  r.p = d.p;
+  r.XY = d.XY;
+  r.r2lo = d.r2lo;
+  r.r2hi = d.r2hi;
+  r.r2max = d.r2max;
+  r.inv_h = d.inv_h;
+  r.inv_gs = d.inv_gs;
+  r.c_fr = d.c_fr;
+  return r;
+}
+__device__ __forceinline__ KParams kp_of_particle(const KParams& kp, int i) {
+  return (kp.scenes && i < kp.n) ? scene_kp(kp, scene_of(kp.scene_pbase, kp.nscenes, i)) : kp;
+}
+__device__ __forceinline__ KParams kp_of_cell(const KParams& kp, int c) {
+  return (kp.scenes && c < kp.G) ? scene_kp(kp, scene_of(kp.scene_cbase, kp.nscenes, c)) : kp;
+}
 
 // packed integer cell coordinates of the precision form
 constexpr int kCellBits = 10;
@@ -127,6 +177,9 @@ struct Handle {
   struct LearnState* learn = nullptr;  // learned-corrector data and scratch (learn.cu)
   int* c3buf[2] = {nullptr, nullptr};  // precision form: cells of old_ / new_ (precise.cu)
   struct RigidState* rigid = nullptr;  // attached rigid body (precise.cu)
+  SceneDev* scene_tab = nullptr;       // batched form: scene table and bases (device)
+  int* scene_base = nullptr;           // [2][nscenes + 1]: particle bases, then cell bases
+  int graph_steps = 1;                 // steps per replay of zsph_run's graph (zsph_autotune)
 };
 
 // learn.cu: frees the handle's learned-corrector state
