@@ -13,6 +13,12 @@ With N > 1 (torchrun) every rank runs an independent replica of the case:
 the path does not shard (replicas only), so there is no collective on the
 data path; only the barrier and the max-over-ranks timing reduction.
 
+Two more keys time the other forms of the step on the same GPU: `learned`
+(learned corrector, trained first on dam-break snapshots at dx = 0.02, then
+run on this case with and without the judging plain corrector) and
+`batched` (256 uneven dam-break scenes in one batched handle vs the same
+scenes looped through single-scene handles).
+
 --impl reference times the reference solver's equations on the host cores
 (the CPU oracle, an OpenMP restatement of the reference's CUDA kernels; the
 reference has no CPU path of its own) and, beside it, the reference's own
@@ -51,6 +57,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=20.0, help="target CPU-baseline sample duration")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-corrector leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-form leg")
     ap.add_argument("--learn-epochs", type=int, default=20)
     return ap.parse_args()
 
@@ -237,13 +244,67 @@ def learned_leg(args, dist, sol, stream, sptr, n, ms_plain):
     net.close()
     v_j, v_u = dist.world * n * K / (ms_j / 1e3), dist.world * n * K / (ms_u / 1e3)
     return {"value": v_j, "unit": "particle-steps/s", "ms_per_step": ms_j / K,
-            "speedup_vs_plain": ms_plain / ms_j, "judge_every": 10, "tol": 1e-2, "run": rj,
-            "unjudged": {"value": v_u, "ms_per_step": ms_u / K, "speedup_vs_plain": ms_plain / ms_u, "run": ru},
+            "speedup_vs_plain": ms_plain / (ms_j / K), "judge_every": 10, "tol": 1e-2, "run": rj,
+            "unjudged": {"value": v_u, "ms_per_step": ms_u / K, "speedup_vs_plain": ms_plain / (ms_u / K),
+                         "run": ru},
             "train": dict(train, snapshots=snaps, data="dam break dx=0.02 (105,048 particles), plain steps 100-2100, "
                                                        "every 10th step", prep_seconds=prep_s),
             "what": "corrector stage = predictor-stage value + (value - previous corrector value) + network "
                     "residual; judged steps run the plain corrector, compare accelerations (relative L2, fluid) "
                     "and keep the plain result; above tol the plain corrector runs until a judged step passes"}
+
+
+# ---------------------------------------------------------------- batched form
+def batched_leg(args, dist, stream, sptr):
+    """256 seeded dam-break scenes of uneven sizes (cases.batch_scenes, seed
+    2026) advanced together: one batched handle whose every kernel launch
+    covers all scenes, K steps replayed from its CUDA graph after the
+    autotuner picked the launch shapes; beside it the same scenes stepped
+    one after another with 256 single-scene handles (one graph replay per
+    scene and step).  Both timed with CUDA events on the same stream."""
+    import torch
+    import zsph_b200 as z
+    from zsph_b200 import cases
+    scenes, _ = cases.batch_scenes(256, seed=2026)
+    n = sum(c.n for c in scenes)
+    K, W = args.steps, args.warmup
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        dist.barrier()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return dist.max(a.elapsed_time(b))
+
+    bt = z.Solver.from_batch(scenes)
+    tune = bt.autotune(3, stream=sptr)
+    bt.run(W, sptr)
+    ms_b = timed(lambda: bt.run(K, sptr))
+    flags_b = bt.status()
+    bt.close()
+    solo = [z.Solver.from_case(c) for c in scenes]
+    for s in solo:
+        s.run(W, sptr)
+
+    def loop():
+        for _ in range(K):
+            for s in solo:
+                s.run(1, sptr)
+
+    ms_l = timed(loop)
+    for s in solo:
+        s.close()
+    nf = [c.n_fluid for c in scenes]
+    return {"value": dist.world * n * K / (ms_b / 1e3), "unit": "particle-steps/s", "ms_per_step": ms_b / K,
+            "loop_value": dist.world * n * K / (ms_l / 1e3), "loop_ms_per_step": ms_l / K,
+            "speedup_vs_loop": ms_l / ms_b, "scenes": len(scenes), "particles": n,
+            "fluid_per_scene": {"min": min(nf), "max": max(nf), "sum": sum(nf)}, "tune": tune,
+            "status_flags": flags_b,
+            "what": "aggregate particle-steps/s of 256 scenes (widths U[0.2,0.6] m, aspect U[0.5,2], dx U[0.01,0.02] m, "
+                    "seed 2026) in one batched handle, vs the same scenes looped through single-scene handles"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -342,6 +403,7 @@ def run_ours(args, dist: Dist):
                    "host wall clock, max over ranks"}
 
     learned = None if args.no_learned else learned_leg(args, dist, sol, stream, sptr, n, ms / K)
+    batched = None if args.no_batched else batched_leg(args, dist, stream, sptr)
 
     cpu = None
     if dist.rank == 0 and not args.no_cpu_baseline:
@@ -357,7 +419,7 @@ def run_ours(args, dist: Dist):
                    "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
         "roofline": roofline, "dominant_kernel": dominant, "kernels": kern, "cpu_baseline": cpu,
-        "learned": learned, "status_flags": flags,
+        "learned": learned, "batched": batched, "status_flags": flags,
     }
     sol.close()
     return line
