@@ -210,6 +210,14 @@ int zsph_neighbor_counts(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp
  * comma-separated kernel names into names (may be NULL). */
 int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
                        void* stream, float* ms, int cap, int* count, char* names, int names_len);
+/* As zsph_step_profiled, with events only at the end of each sub-step's
+ * neighbour search ("search": hash, scan, scatter, rank + gather) and of its
+ * pair kernels ("pair": list build, boundary, governing), so that the
+ * durations carry one event's overhead per group instead of one per kernel.
+ * No reference counterpart (measurement only). */
+int zsph_step_profiled_groups(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_,
+                              const zsph_tmp_t* tmp, void* stream, float* ms, int cap, int* count, char* names,
+                              int names_len);
 /* Number of kernel launches one zsph_step issues. */
 int zsph_launches_per_step(zsph_handle_t* h);
 

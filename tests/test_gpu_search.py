@@ -137,3 +137,55 @@ def test_search_twice_reuses_scratch():
     assert np.array_equal(t["grid_end"], o.tmp["grid_end"])
     assert np.array_equal(sol.download("old").pos, o.old["pos"])
     sol.close()
+
+
+def test_fused_search_many_scan_tiles():
+    # dx = 0.0075: 190,060 cells = 47 one-pass scan tiles, so the look-back
+    # crosses more than one 32-tile window
+    c = cases.dam_break(0.0075, end_step=500)
+    sol = z.Solver.from_case(c)
+    sol.neighbor_search("old", "new")
+    sol.sync()
+    _assert_same(sol, _oracle_search(c), "medium ")
+    sol.close()
+
+
+def test_dropin_sort_between_fused_searches():
+    # the drop-in sort and the fused search share the counting-sort scratch
+    c = cases.random_cloud(5000, 21, kill_frac=0.01)
+    sol = z.Solver.from_case(c)
+    o = po.Oracle(c.json, c.state, np.float32)
+    sol.neighbor_search("old", "new")
+    o.search("old", "new")
+    sol.hash("new")
+    sol.sort_index()
+    o.hash("new")
+    o.sort_index()
+    t = sol.download_tmp()
+    assert np.array_equal(t["index"], o.tmp["index"])
+    sol.neighbor_search("new", "old")
+    o.search("new", "old")
+    t = sol.download_tmp()
+    for k in ("hash", "index", "grid_start", "grid_end"):
+        assert np.array_equal(t[k], o.tmp[k]), k
+    sol.close()
+
+
+def test_profiled_steps_report_every_launch_and_group():
+    c = cases.small(0.04)
+    a = z.Solver.from_case(c)
+    b = z.Solver.from_case(c)
+    per = a.step_profiled()
+    names = [k for k, _ in per]
+    sub = ["hash_count", "scan", "scatter", "rank_gather", "nblist_wall", "boundary", "governing"]
+    assert names == sub + sub
+    assert len(names) == a.launches_per_step()
+    grp = a.step_profiled(groups=True)
+    assert [k for k, _ in grp] == ["search", "pair", "search", "pair"]
+    assert all(t > 0 for _, t in per + grp)
+    b.step()
+    b.step()
+    sa, sb = a.download("old"), b.download("old")
+    assert np.array_equal(sa.pos, sb.pos) and np.array_equal(sa.table, sb.table)
+    a.close()
+    b.close()

@@ -174,6 +174,8 @@ _sig = {
     "zsph_launches_per_step": (_I, [_HP]),
     "zsph_step_profiled": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _FP, _I,
                                 _IP, ctypes.c_char_p, _I]),
+    "zsph_step_profiled_groups": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _VP, _FP, _I,
+                                _IP, ctypes.c_char_p, _I]),
     "zsph_last_error": (_I, [_HP, ctypes.c_char_p, _I]),
     "zsph_version": (ctypes.c_char_p, []),
     "zsph_memcpy": (_I, [_VP, _VP, ctypes.c_size_t, _I, _VP]),
@@ -479,13 +481,15 @@ class Solver:
                    nb_g.ptr, None)
         return nb_b.get(), nb_g.get()
 
-    def step_profiled(self, stream=None) -> list[tuple[str, float]]:
-        """One step with per-launch CUDA-event timing: [(kernel, ms), ...]."""
+    def step_profiled(self, stream=None, groups: bool = False) -> list[tuple[str, float]]:
+        """One step with CUDA-event timing: [(kernel, ms), ...] per launch, or,
+        with groups=True, [(group, ms), ...] per sub-step's search and pair kernels."""
         cap = 64
         ms = (ctypes.c_float * cap)()
         cnt = ctypes.c_int(0)
         names = ctypes.create_string_buffer(4096)
-        self._call(lib.zsph_step_profiled, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
+        fn = lib.zsph_step_profiled_groups if groups else lib.zsph_step_profiled
+        self._call(fn, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
                    stream, ms, cap, ctypes.byref(cnt), names, len(names))
         nm = names.value.decode().split(",")
         return [(nm[k], float(ms[k])) for k in range(cnt.value)]

@@ -120,7 +120,7 @@ int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
 
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
-                  s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp};
+                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(&s, 0, sizeof s);
@@ -291,6 +291,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.tile_sum, (size_t)h->tiles);
   if (!e) e = dalloc(s.tile_off, (size_t)h->tiles);
   if (!e) e = dalloc(s.tile_last, (size_t)h->tiles);
+  if (!e) e = dalloc(s.tile_state, (size_t)h->tiles);
   if (!e) e = dalloc(s.misc, 8);
   if (!e) e = dalloc(s.big_list, (size_t)kBigListCap);
   if (!e) e = dalloc(s.nb, (size_t)kMaxNb * n);
@@ -300,6 +301,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.sh.vp, n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
   if (!e) e = cudaMemset(s.misc, 0, 8 * sizeof(int));
+  if (!e) e = cudaMemset(s.tile_state, 0, (size_t)h->tiles * sizeof(unsigned long long));
   if (!e) e = cudaMemset(s.flags, 0, sizeof(int));
   if (!e) e = cudaMemset(s.nb_cnt, 0, n ? n : 1);
   if (!e) e = cudaDeviceSynchronize();
@@ -693,8 +695,11 @@ int zsph_device_synchronize(void) {
   return ZSPH_OK;
 }
 
-int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp,
-                       void* stream, float* ms, int cap, int* count, char* names, int names_len) {
+}  // extern "C"
+
+namespace {
+int step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp, void* stream,
+                  float* ms, int cap, int* count, char* names, int names_len, bool groups) {
   ENTRY_CHECKS(h);
   if (int rc = check_ptc(h, o)) return rc;
   if (int rc = check_ptc(h, w)) return rc;
@@ -706,13 +711,36 @@ int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* 
   std::vector<cudaEvent_t> ev(slots);
   std::vector<const char*> nm(slots, "");
   for (auto& e : ev) ZCHECK(h, "zsph_step_profiled event", cudaEventCreate(&e));
+  // The step is captured into a graph whose event-record nodes bracket each
+  // launch, then replayed once: the event intervals are then GPU time of each
+  // kernel plus the graph's own gap to the next node, free of host launch cost.
   Prof pf;
   pf.ev = ev.data() + 1;
   pf.cap = cap;
   pf.names = nm.data() + 1;
-  cudaEventRecord(ev[0], st);
-  cudaError_t le = step_launches(h, *o, *w, *tmp, st, &pf);
+  pf.external = true;
+  pf.groups = groups;
+  if (!h->graph_stream) {
+    cudaError_t cs = cudaStreamCreateWithFlags(&h->graph_stream, cudaStreamNonBlocking);
+    if (cs) {
+      for (auto& e : ev) cudaEventDestroy(e);
+      return cuda_fail(h, "zsph_step_profiled stream", cs);
+    }
+  }
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t gx = nullptr;
+  cudaError_t le = cudaStreamBeginCapture(h->graph_stream, cudaStreamCaptureModeThreadLocal);
+  if (!le) {
+    le = cudaEventRecordWithFlags(ev[0], h->graph_stream, cudaEventRecordExternal);
+    if (!le) le = step_launches(h, *o, *w, *tmp, h->graph_stream, &pf);
+    const cudaError_t ce = cudaStreamEndCapture(h->graph_stream, &g);
+    if (!le) le = ce;
+  }
+  if (!le) le = cudaGraphInstantiate(&gx, g, 0);
+  if (!le) le = cudaGraphLaunch(gx, st);
   cudaError_t se = cudaStreamSynchronize(st);
+  if (gx) cudaGraphExecDestroy(gx);
+  if (g) cudaGraphDestroy(g);
   const int n = pf.n;
   std::string all;
   for (int k = 0; k < n; ++k) {
@@ -730,11 +758,24 @@ int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* 
   return ZSPH_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int zsph_step_profiled(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp,
+                       void* stream, float* ms, int cap, int* count, char* names, int names_len) {
+  return step_profiled(h, o, w, tmp, stream, ms, cap, count, names, names_len, false);
+}
+
+int zsph_step_profiled_groups(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* tmp,
+                              void* stream, float* ms, int cap, int* count, char* names, int names_len) {
+  return step_profiled(h, o, w, tmp, stream, ms, cap, count, names, names_len, true);
+}
+
 int zsph_launches_per_step(zsph_handle_t* h) {
   (void)h;
-  // per sub-step: hash_count, scan_reduce, scan_cells, scatter, sort_big_cells,
-  // rank_gather, nblist, boundary, governing
-  return 2 * 9;
+  // per sub-step: hash_count, scan, scatter, rank_gather, nblist, boundary, governing
+  return 2 * 7;
 }
 
 }  // extern "C"

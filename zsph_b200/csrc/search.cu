@@ -4,7 +4,7 @@
 // Reference path replaced (single_gpu_sph_src/):
 //   lib/hash.cu:3-26     cuda_ptc_hash      -> k_hash (drop-in) / k_hash_count (fused)
 //   lib/sort.cu:3-6      thrust::sort_by_key-> counting sort: count -> scan -> scatter -> rank
-//   lib/sort.cu:8-84     cuda_sort_data     -> k_scan_cells (bounds) + k_rank_gather (reorder)
+//   lib/sort.cu:8-84     cuda_sort_data     -> k_scan_onepass / k_scan_cells (bounds) + k_rank_gather (reorder)
 //
 // The reference sorts all 32 key bits with a generic radix sort.  Here the
 // keys are cell ids in [0, G), so a counting sort needs one histogram, one
@@ -27,6 +27,10 @@
 namespace zsph {
 namespace {
 
+constexpr int kHashItems = 4;             // particles per thread in the fused hash
+constexpr int kScatterItems = 4;          // particles per thread in the fused scatter
+constexpr unsigned kLookbackSpins = 1u << 20;  // bound on the one-pass scan's wait for a predecessor tile
+
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -43,18 +47,20 @@ __device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, flo
 }
 
 // hash.cu:16-23: a particle outside the grid becomes type 100 at the grid
-// origin with zero velocity and (rho0, 0); its key becomes 0.
-__device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t& s, int i, int* flags) {
+// origin with zero velocity and (rho0, 0); its key becomes 0.  Takes the
+// particle's position (x, y, z) or, in the precision form, its packed cell
+// (cpk), already loaded.
+__device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_ptc_t& s, int i, float x, float y,
+                                                float z, int cpk, int* flags) {
   const zsph_gpu_param_t& p = kp.p;
   int h;
   bool out;
   if (kp.c3o) {  // precision form: the cell is stored, the offset is local
-    const int3 c = unpack_cell(kp.c3o[i]);
+    const int3 c = unpack_cell(cpk);
     out = c.x >= p.grid_xdim || c.y >= p.grid_ydim || c.z >= p.grid_zdim;
     h = (c.z * p.grid_ydim + c.y) * p.grid_xdim + c.x;
   } else {
     // batched form: the scene's cells start at grid_hash_min (0 for one scene)
-    const float x = s.pos[3 * i], y = s.pos[3 * i + 1], z = s.pos[3 * i + 2];
     h = cell_hash(p, x, y, z);
     out = h < 0 || h > p.grid_hash_max - p.grid_hash_min;
     h += p.grid_hash_min;
@@ -82,6 +88,19 @@ __device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t
   return h;
 }
 
+__device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t& s, int i, int* flags) {
+  float x = 0.0f, y = 0.0f, z = 0.0f;
+  int cpk = 0;
+  if (kp.c3o) {
+    cpk = kp.c3o[i];
+  } else {
+    x = s.pos[3 * i];
+    y = s.pos[3 * i + 1];
+    z = s.pos[3 * i + 2];
+  }
+  return hash_and_kill_at(kp, s, i, x, y, z, cpk, flags);
+}
+
 // One atomic per distinct key per warp; returns this lane's ticket (its
 // arrival rank inside the key's cell).  Lanes of one warp that share a key
 // get consecutive tickets in lane order.
@@ -104,15 +123,89 @@ __global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp_in, zsph_ptc_t
   t.index[i] = i;
 }
 
-// Fused search, step 1: hash + kill + per-cell ticket.
+// Fused search, step 1: hash + kill + per-cell ticket, kHashItems particles
+// per thread (i = tile base + k * kSearchBlock + thread, so each warp access
+// stays coalesced).  All positions are loaded before any hash is formed and
+// all ticket atomics are issued before any result is used, so a thread keeps
+// kHashItems loads and atomics in flight.  Also prepares the one-pass scan:
+// the largest key (misc[4]), a fresh tile counter (misc[5]), the next epoch
+// (misc[6]) and an empty big-cell list (misc[3]).
 __global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp_in, zsph_ptc_t s, Scratch sc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const unsigned active = __ballot_sync(0xffffffffu, i < kp_in.n);
-  if (i >= kp_in.n) return;
-  const KParams kp = kp_of_particle(kp_in, i);
-  const int h = hash_and_kill(kp, s, i, sc.flags);
-  sc.key[i] = h;
-  sc.ticket[i] = warp_ticket(sc.cnt, h, active);
+  __shared__ int s_max[kSearchBlock / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int base = blockIdx.x * (kSearchBlock * kHashItems) + threadIdx.x;
+  const int n = kp_in.n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc.misc[3] = 0;
+    sc.misc[5] = 0;
+    sc.misc[6] = (int)((unsigned)sc.misc[6] + 1u);
+  }
+  float x[kHashItems], y[kHashItems], z[kHashItems];
+  int cpk[kHashItems];
+#pragma unroll
+  for (int k = 0; k < kHashItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    x[k] = y[k] = z[k] = 0.0f;
+    cpk[k] = 0;
+    if (i < n) {
+      if (kp_in.c3o) {
+        cpk[k] = kp_in.c3o[i];
+      } else {
+        x[k] = s.pos[3 * i];
+        y[k] = s.pos[3 * i + 1];
+        z[k] = s.pos[3 * i + 2];
+      }
+    }
+  }
+  int h[kHashItems];
+  int kmax = -1;
+#pragma unroll
+  for (int k = 0; k < kHashItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    h[k] = 0;
+    if (i < n) {
+      const KParams kp = kp_of_particle(kp_in, i);
+      h[k] = hash_and_kill_at(kp, s, i, x[k], y[k], z[k], cpk[k], sc.flags);
+      sc.key[i] = h[k];
+      kmax = max(kmax, h[k]);
+    }
+  }
+  // Tickets: one atomic per run of equal keys among a warp's consecutive
+  // particles (the particles are nearly sorted by cell, so a warp holds a few
+  // runs).  Lanes of a run get consecutive tickets in lane order; two runs of
+  // one key draw separate ranges.  The ranking step restores stability.
+  unsigned heads[kHashItems];
+  int got[kHashItems];
+#pragma unroll
+  for (int k = 0; k < kHashItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    const int prev = __shfl_up_sync(0xffffffffu, h[k], 1);
+    // active lanes form a prefix of the warp; an inactive lane counts as a head
+    const bool head = i >= n || lane == 0 || prev != h[k];
+    heads[k] = __ballot_sync(0xffffffffu, head);
+    got[k] = 0;
+    if (i < n && head) {
+      const unsigned after = heads[k] & ~((2u << lane) - 1u);  // heads above this lane (lane 31: none)
+      const int next = after ? __ffs(after) - 1 : 32;
+      got[k] = atomicAdd(&sc.cnt[h[k]], next - lane);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kHashItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    const int lead = 31 - __clz(heads[k] & ((2u << lane) - 1u));  // this lane's run head
+    const int b = __shfl_sync(0xffffffffu, got[k], lead);
+    if (i < n) sc.ticket[i] = b + lane - lead;
+  }
+  kmax = __reduce_max_sync(0xffffffffu, kmax);
+  if (lane == 0) s_max[warp] = kmax;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int m = -1;
+#pragma unroll
+    for (int w = 0; w < kSearchBlock / 32; ++w) m = max(m, s_max[w]);
+    if (m >= 0) atomicMax(&sc.misc[4], m);
+  }
 }
 
 // Drop-in sort_index, step 1: copy keys and carried values, count.
@@ -261,6 +354,143 @@ __global__ void __launch_bounds__(kSearchBlock) k_scan_cells(KParams kp, Scratch
   }
 }
 
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Fused search, step 2: one-pass scan of the per-cell counts with decoupled
+// look-back, writing cell_lb, grid_start/grid_end in closed form and the
+// big-cell list, and zeroing the counts (all but the last occupied cell's,
+// which every tile reads; the scatter zeroes that one).
+//
+// A tile is kOneTile cells, kOneItems consecutive cells per thread, read and
+// written with 16-byte vector accesses.  Tiles are claimed in launch order
+// through an atomic counter (misc[5]), so every predecessor of a tile belongs
+// to a CTA that is already running.  A tile publishes its aggregate at once,
+// then its inclusive prefix after looking back; the status word of a tile is
+// (tag << 32) | value with tag 2e+1 (aggregate) or 2e+2 (inclusive prefix)
+// for this search's epoch e (misc[6]), so the words never need clearing.
+// The look-back wait is bounded: a tile that gives up raises
+// ZSPH_FLAG_TIMEOUT and carries on (the sort is then wrong, and flagged).
+// The last occupied cell comes from the hash's atomic maximum (misc[4]).
+constexpr int kOneItems = 16;
+constexpr int kOneTile = kSearchBlock * kOneItems;
+
+__device__ __forceinline__ void st4(int* p, int a, int b, int c, int d) {
+  *reinterpret_cast<int4*>(p) = make_int4(a, b, c, d);
+}
+
+__global__ void __launch_bounds__(kSearchBlock) k_scan_onepass(KParams kp, Scratch sc, zsph_tmp_t t) {
+  __shared__ int sw[kSearchBlock / 32];
+  __shared__ int s_tile, s_excl;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_tile = atomicAdd(&sc.misc[5], 1);
+  __syncthreads();
+  const int tile = s_tile;
+  const unsigned epoch = (unsigned)sc.misc[6];
+  const unsigned tag_agg = 2u * epoch + 1u, tag_inc = 2u * epoch + 2u;
+  const int G = kp.G, n = kp.n;
+  const int klast = sc.misc[4];
+  const bool last_single = sc.cnt[klast] == 1;
+  const int base = tile * kOneTile + threadIdx.x * kOneItems;
+  const bool full = base + kOneItems <= G;  // 16-byte aligned: base is a multiple of 16 cells
+  int v[kOneItems];
+  if (full) {
+#pragma unroll
+    for (int q = 0; q < kOneItems / 4; ++q) {
+      const int4 a = *reinterpret_cast<const int4*>(sc.cnt + base + 4 * q);
+      v[4 * q] = a.x; v[4 * q + 1] = a.y; v[4 * q + 2] = a.z; v[4 * q + 3] = a.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kOneItems; ++k) v[k] = base + k < G ? sc.cnt[base + k] : 0;
+  }
+  int sum = 0;
+#pragma unroll
+  for (int k = 0; k < kOneItems; ++k) sum += v[k];
+  int total;
+  const int ex = block_exclusive_scan(sum, sw, total);
+  if (warp == 0) {
+    unsigned long long* ts = sc.tile_state;
+    int excl = 0;
+    if (tile == 0) {
+      if (lane == 0) st_relaxed_u64(ts, ((unsigned long long)tag_inc << 32) | (unsigned)total);
+    } else {
+      if (lane == 0) st_relaxed_u64(ts + tile, ((unsigned long long)tag_agg << 32) | (unsigned)total);
+      int j = tile - 1;  // nearest predecessor not yet added
+      unsigned spins = 0;
+      for (;;) {
+        const int idx = j - lane;
+        unsigned long long w;
+        for (;;) {
+          w = idx >= 0 ? ld_relaxed_u64(ts + idx) : ((unsigned long long)tag_inc << 32);
+          const unsigned tg = (unsigned)(w >> 32);
+          if (__all_sync(0xffffffffu, tg == tag_agg || tg == tag_inc)) break;
+          if (++spins >= kLookbackSpins) break;
+          if (spins > 64) __nanosleep(32);
+        }
+        if (spins >= kLookbackSpins) {
+          if (lane == 0) atomicOr(sc.flags, ZSPH_FLAG_TIMEOUT);
+          break;
+        }
+        const unsigned inc = __ballot_sync(0xffffffffu, (unsigned)(w >> 32) == tag_inc);
+        int val = (int)(unsigned)(w & 0xffffffffu);
+        if (inc) {
+          const int f = __ffs(inc) - 1;  // nearest tile holding an inclusive prefix
+          if (lane > f) val = 0;
+          excl += __reduce_add_sync(0xffffffffu, val);
+          break;
+        }
+        excl += __reduce_add_sync(0xffffffffu, val);
+        j -= 32;
+      }
+      if (lane == 0) st_relaxed_u64(ts + tile, ((unsigned long long)tag_inc << 32) | (unsigned)(excl + total));
+    }
+    if (lane == 0) s_excl = excl;
+  }
+  __syncthreads();
+  int lb[kOneItems + 1];
+  lb[0] = s_excl + ex;
+#pragma unroll
+  for (int k = 0; k < kOneItems; ++k) lb[k + 1] = lb[k] + v[k];
+  // the stale-bounds rule touches only cells >= klast of a single last particle
+  const bool plain = full && !(last_single && base + kOneItems > klast) && (klast < base || klast >= base + kOneItems);
+  if (plain) {
+#pragma unroll
+    for (int q = 0; q < kOneItems / 4; ++q) {
+      const int k = 4 * q;
+      st4(sc.cell_lb + base + k, lb[k], lb[k + 1], lb[k + 2], lb[k + 3]);
+      st4(t.grid_start + base + k, min(lb[k], n - 1), min(lb[k + 1], n - 1), min(lb[k + 2], n - 1),
+          min(lb[k + 3], n - 1));
+      st4(t.grid_end + base + k, min(lb[k + 1], n - 1), min(lb[k + 2], n - 1), min(lb[k + 3], n - 1),
+          min(lb[k + 4], n - 1));
+      st4(sc.cnt + base + k, 0, 0, 0, 0);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kOneItems; ++k) {
+    const int c = base + k;
+    if (c < G) {
+      if (!plain) {
+        sc.cell_lb[c] = lb[k];
+        if (!(last_single && c > klast)) t.grid_start[c] = min(lb[k], n - 1);
+        if (!(last_single && c >= klast)) t.grid_end[c] = min(lb[k + 1], n - 1);
+        if (v[k] != 0 && c != klast) sc.cnt[c] = 0;
+      }
+      if (v[k] > kBigSegment) {
+        const int slot = atomicAdd(&sc.misc[3], 1);
+        if (slot < kBigListCap) sc.big_list[slot] = c;
+      }
+      if (c == G - 1) sc.cell_lb[G] = lb[k + 1];
+    }
+  }
+}
+
 // Scatter by ticket (unstable inside a cell until ranked).
 __global__ void __launch_bounds__(kSearchBlock) k_scatter(KParams kp, Scratch sc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -268,10 +498,11 @@ __global__ void __launch_bounds__(kSearchBlock) k_scatter(KParams kp, Scratch sc
   sc.perm[sc.cell_lb[sc.key[i]] + sc.ticket[i]] = i;
 }
 
-// Sorts perm[a, a+n) ascending in place with one CTA: a bitonic network in
+// Sorts v[0, n) ascending in place with one CTA: a bitonic network in
 // which every comparator puts the minimum at the lower index, so virtual
 // +inf padding beyond n never has to be stored.
-__device__ void cta_sort_segment(int* v, int n) {
+template <class Ptr>
+__device__ void cta_sort_segment(Ptr v, int n) {
   int P = 1;
   while (P < n) P <<= 1;
   for (int k = 2; k <= P; k <<= 1) {
@@ -299,8 +530,61 @@ __device__ void cta_sort_segment(int* v, int n) {
   }
 }
 
+// Fused search, step 3: scatter by ticket, kScatterItems particles per
+// thread.  Also zeroes the last occupied cell's count and the largest key
+// left for the next search by the one-pass scan.  When the scan listed
+// crowded cells (more than kBigSegment members), the last CTA to finish
+// (counter misc[7]) pre-sorts their members, reading the other CTAs' scatter
+// through volatile accesses after a fence; otherwise no CTA takes part in
+// that protocol, and the common case costs no extra launch.
+__global__ void __launch_bounds__(kSearchBlock) k_scatter_fused(KParams kp, Scratch sc) {
+  __shared__ bool s_last;
+  const bool crowded = sc.misc[3] != 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sc.cnt[sc.misc[4]] = 0;
+    sc.misc[4] = 0;
+  }
+  const int base = blockIdx.x * (kSearchBlock * kScatterItems) + threadIdx.x;
+  int key[kScatterItems], tk[kScatterItems];
+#pragma unroll
+  for (int k = 0; k < kScatterItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    key[k] = i < kp.n ? sc.key[i] : 0;
+    tk[k] = i < kp.n ? sc.ticket[i] : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < kScatterItems; ++k) {
+    const int i = base + k * kSearchBlock;
+    if (i < kp.n) sc.perm[sc.cell_lb[key[k]] + tk[k]] = i;
+  }
+  if (!crowded) return;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&sc.misc[7], 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (threadIdx.x == 0) sc.misc[7] = 0;
+  const int listed = sc.misc[3];
+  volatile int* perm = sc.perm;
+  if (listed <= kBigListCap) {
+    for (int e = 0; e < listed; ++e) {
+      const int c = sc.big_list[e];
+      const int a = sc.cell_lb[c], b = sc.cell_lb[c + 1];
+      cta_sort_segment(perm + a, b - a);
+    }
+  } else {
+    for (int c = 0; c < kp.G; ++c) {
+      const int a = sc.cell_lb[c], b = sc.cell_lb[c + 1];
+      if (b - a > kBigSegment) cta_sort_segment(perm + a, b - a);
+    }
+  }
+}
+
 // Pre-sorts the members of crowded cells (more than kBigSegment particles).
-// Uses the list built by k_scan_cells, or every cell if the list overflowed.
+// Uses the list built by the scan, or every cell if the list overflowed.
 __global__ void __launch_bounds__(1024) k_sort_big_cells(KParams kp, Scratch sc) {
   const int listed = sc.misc[3];
   if (listed == 0) return;
@@ -355,19 +639,58 @@ __device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t
   sh.vp[dst] = make_float4(vx, vy, vz, rp.y);
 }
 
+// One particle's record of the eight reference arrays (72 bytes).
+struct PtcRec {
+  float x, y, z, vx, vy, vz;
+  float2 rp;
+  float tx, ty, tz, ux, uy, uz;
+  float2 trp;
+  int type, table;
+};
+
+__device__ __forceinline__ void load_rec(const zsph_ptc_t& o, int src, PtcRec& r) {
+  r.x = o.pos[3 * src]; r.y = o.pos[3 * src + 1]; r.z = o.pos[3 * src + 2];
+  r.vx = o.vel[3 * src]; r.vy = o.vel[3 * src + 1]; r.vz = o.vel[3 * src + 2];
+  r.rp = reinterpret_cast<const float2*>(o.rhop)[src];
+  r.tx = o.tmp_pos[3 * src]; r.ty = o.tmp_pos[3 * src + 1]; r.tz = o.tmp_pos[3 * src + 2];
+  r.ux = o.tmp_vel[3 * src]; r.uy = o.tmp_vel[3 * src + 1]; r.uz = o.tmp_vel[3 * src + 2];
+  r.trp = reinterpret_cast<const float2*>(o.tmp_rhop)[src];
+  r.type = o.type[src];
+  r.table = o.table[src];
+}
+
+__device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const Shadow& sh, const PtcRec& r, int src, int dst) {
+  w.pos[3 * dst] = r.x; w.pos[3 * dst + 1] = r.y; w.pos[3 * dst + 2] = r.z;
+  w.vel[3 * dst] = r.vx; w.vel[3 * dst + 1] = r.vy; w.vel[3 * dst + 2] = r.vz;
+  reinterpret_cast<float2*>(w.rhop)[dst] = r.rp;
+  w.tmp_pos[3 * dst] = r.tx; w.tmp_pos[3 * dst + 1] = r.ty; w.tmp_pos[3 * dst + 2] = r.tz;
+  w.tmp_vel[3 * dst] = r.ux; w.tmp_vel[3 * dst + 1] = r.uy; w.tmp_vel[3 * dst + 2] = r.uz;
+  reinterpret_cast<float2*>(w.tmp_rhop)[dst] = r.trp;
+  w.type[dst] = r.type;
+  w.table[dst] = r.table + src - dst;  // sort.cu:82
+  sh.pr[dst] = make_float4(r.x, r.y, r.z, packed_rho(r.rp.x, r.type));
+  sh.vp[dst] = make_float4(r.vx, r.vy, r.vz, r.rp.y);
+}
+
 // Fused search, last step: rank, write sorted hash/index, gather the eight
-// particle arrays (sort.cu:62-82) and the packed shadows.
+// particle arrays (sort.cu:62-82) and the packed shadows.  The source record's
+// loads are issued as soon as the source is known, before the rank (which
+// needs the key, the cell's range and its members) is counted, so they
+// overlap that dependent chain.
 __global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
                                                               zsph_tmp_t t) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= kp.n) return;
   const int i = sc.perm[slot];
+  PtcRec r;
+  load_rec(o, i, r);
+  const int cpk = kp.c3o ? kp.c3o[i] : 0;
   const int c = sc.key[i];
   const int dst = ranked_slot(sc, slot, i, c);
   t.index[dst] = i;
   t.hash[dst] = c;
-  gather_one(o, w, sc.sh, i, dst);
-  if (kp.c3o) kp.c3n[dst] = kp.c3o[i];
+  store_rec(w, sc.sh, r, i, dst);
+  if (kp.c3o) kp.c3n[dst] = cpk;
 }
 
 // Drop-in sort_index, last step: sorted keys and carried values.
@@ -391,7 +714,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_gather_by_index(KParams kp, Sc
 
 // Exact per-cell particle ranges [cell_lb[c], cell_lb[c+1]) of an already
 // sorted key array (drop-in pair entry points, whose caller sorted the
-// particles; the fused search produces them in k_scan_cells).  Each particle
+// particles; the fused search produces them in its scan).  Each particle
 // that starts a new key fills the offsets of the cells since the previous key.
 __global__ void __launch_bounds__(kSearchBlock) k_cell_lb(KParams kp, Scratch sc, zsph_tmp_t t) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -462,16 +785,13 @@ cudaError_t launch_sort_data(const KParams& kp, const Scratch& s, int tiles, con
 cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
                           const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf) {
   if (kp.n == 0) return cudaSuccess;
-  const int nb = blocks_for(kp.n, kSearchBlock);
-  k_hash_count<<<nb, kSearchBlock, 0, st>>>(kp, o, s);
+  k_hash_count<<<blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st>>>(kp, o, s);
   mark(pf, "hash_count", st);
-  cudaError_t e = launch_scan(kp, s, tiles, tmp, 1, st, pf);
-  if (e) return e;
-  k_scatter<<<nb, kSearchBlock, 0, st>>>(kp, s);
+  k_scan_onepass<<<(kp.G + kOneTile - 1) / kOneTile, kSearchBlock, 0, st>>>(kp, s, tmp);
+  mark(pf, "scan", st);
+  k_scatter_fused<<<blocks_for(kp.n, kSearchBlock * kScatterItems), kSearchBlock, 0, st>>>(kp, s);
   mark(pf, "scatter", st);
-  k_sort_big_cells<<<kBigSortCtas, 1024, 0, st>>>(kp, s);
-  mark(pf, "sort_big_cells", st);
-  k_rank_gather<<<nb, kSearchBlock, 0, st>>>(kp, s, o, w, tmp);
+  k_rank_gather<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s, o, w, tmp);
   mark(pf, "rank_gather", st);
   return cudaGetLastError();
 }

@@ -122,7 +122,9 @@ struct Scratch {
   int* tile_sum;     // [tiles]
   int* tile_off;     // [tiles]
   int* tile_last;    // [tiles] last occupied cell of each tile (-1 if none)
-  int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length
+  int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length,
+                     //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch
+  unsigned long long* tile_state;  // [tiles] one-pass scan: (tag << 32) | prefix value, tag from the epoch
   int* big_list;     // [kBigListCap]
   uint16_t* nb;      // [n * kMaxNb] neighbour lists, row-major (entry k of particle i at i*kMaxNb+k)
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
@@ -148,19 +150,31 @@ struct FeatOut {
 };
 
 // Optional per-launch event markers (profiling): after each kernel launch the
-// launcher records the next event, so event k-1 -> k brackets launch k.
+// launcher records the next event, so event k-1 -> k brackets launch k.  With
+// `external` set the launches are being captured into a graph and the marks
+// become event-record nodes of that graph.  With `groups` set only the ends of
+// the launch groups are marked: the neighbour search (after rank_gather,
+// labelled "search") and the pair kernels (after governing, labelled "pair").
 struct Prof {
   cudaEvent_t* ev = nullptr;
   int cap = 0;
   int n = 0;
   const char** names = nullptr;
+  bool external = false;
+  bool groups = false;
 };
 
 inline void mark(Prof* pf, const char* name, cudaStream_t st) {
-  if (pf && pf->n < pf->cap) {
-    pf->names[pf->n] = name;
-    cudaEventRecord(pf->ev[pf->n++], st);
+  if (!pf || pf->n >= pf->cap) return;
+  if (pf->groups) {
+    const std::string k(name);
+    if (k == "rank_gather") name = "search";
+    else if (k == "governing" || k == "governing_feat") name = "pair";
+    else return;
   }
+  pf->names[pf->n] = name;
+  if (pf->external) cudaEventRecordWithFlags(pf->ev[pf->n++], st, cudaEventRecordExternal);
+  else cudaEventRecord(pf->ev[pf->n++], st);
 }
 
 struct Handle {
