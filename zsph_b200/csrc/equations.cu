@@ -512,11 +512,15 @@ constexpr int kWinCapB = 1536;  // boundary window capacity (candidates), 3x3 st
 constexpr int kWinCapG = 2048;  // governing window capacity (candidates), 3x3 stencil
 constexpr int kHdrBytes = (int)((sizeof(WinHdr) + 15) / 16 * 16);
 
-// Dynamic shared memory of a pair kernel: per-thread row starts, row ends
-// and fetch bases (NR columns of kPairBlock), the window header and, for the
-// 3x3 stencil, the window of NARR packed arrays.
+// Dynamic shared memory of a pair kernel: per-thread row starts and row ends
+// (NR columns of kPairBlock); when windows are staged (narr > 0), also the
+// fetch bases, the window header and, for the 3x3 stencil, the window of
+// NARR packed arrays.  Without windows the rest of the layout is never
+// touched, and leaving it out leaves more of the SM's SRAM to the L1 cache
+// that serves the neighbour loads.
 template <int GF> constexpr int pair_smem(int narr, int cap) {
-  return 3 * Stencil<GF>::NR * kPairBlock * 4 + kHdrBytes + (GF == 1 ? narr * cap * 16 : 0);
+  return narr == 0 ? 2 * Stencil<GF>::NR * kPairBlock * 4
+                   : 3 * Stencil<GF>::NR * kPairBlock * 4 + kHdrBytes + (GF == 1 ? narr * cap * 16 : 0);
 }
 
 template <int GF> struct PairSmem {
@@ -559,15 +563,24 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   const bool fi = fluid_of(pi.w);
   const float rho_self = reinterpret_cast<const float2*>(ptc.rhop)[i].x;  // old own density
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
+  // The reference's second loop (delta_ns.cu:133-175) walks the same
+  // neighbours with a constant matrix M: sum_j (M x_ij) f_j = M sum_j x_ij f_j,
+  // so its sums (sx, sy, sz) ride along in the first walk and M is applied
+  // once afterwards (same value, summed in a different rounding order).
   float Lxx = 0.f, Lxy = 0.f, Lxz = 0.f, Lyy = 0.f, Lyz = 0.f, Lzz = 0.f, divv = 0.f;
+  float sx = 0.f, sy = 0.f, sz = 0.f;
   auto use1 = [&](const NbB1& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
     const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
     const float a = 1.0f - 0.5f * q;
     const float fr = c_fr * (a * a * a);
-    const float tl = fr * m * rcp_fast(fabsf(nb.pr.w));
+    const float r1 = fabsf(nb.pr.w);
+    const float frm = fr * m * rcp_fast(r1);
+    const float tl = frm;
     Lxx -= dx * dx * tl; Lxy -= dx * dy * tl; Lxz -= dx * dz * tl;
     Lyy -= dy * dy * tl; Lyz -= dy * dz * tl; Lzz -= dz * dz * tl;
+    const float f2 = frm * (r1 - rho_self);  // delta_ns.cu:163-164
+    sx += dx * f2; sy += dy * f2; sz += dz * f2;
     if (fi && fluid_of(nb.pr.w)) {
       const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
       divv -= tl * dvdx;
@@ -600,22 +613,9 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
     M10 = 0.f; M11 = 1.f; M12 = 0.f;
     M20 = 0.f; M21 = 0.f; M22 = 1.f;
   }
-  float gx = 0.f, gy = 0.f, gz = 0.f;
-  auto use2 = [&](const float4& pj) {
-    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-    const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
-    const float a = 1.0f - 0.5f * q;
-    const float r1 = fabsf(pj.w);
-    const float fr = c_fr * (a * a * a) * ((r1 - rho_self) * m * rcp_fast(r1));
-    gx += (M00 * dx + M01 * dy + M02 * dz) * fr;
-    gy += (M10 * dx + M11 * dy + M12 * dz) * fr;
-    gz += (M20 * dx + M21 * dy + M22 * dz) * fr;
-  };
-  if (staged)
-    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, [&](int q) { return win[q]; }, use2);
-  else
-    walk<GF, true, float4>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
-                           [&](int q) { return shadow_pr<PRECISE>(kp, s, q, ci); }, use2);
+  const float gx = M00 * sx + M01 * sy + M02 * sz;
+  const float gy = M10 * sx + M11 * sy + M12 * sz;
+  const float gz = M20 * sx + M21 * sy + M22 * sz;
   reinterpret_cast<float4*>(t.dofv_grandrho)[i] = make_float4(gx, gy, gz, divv);
   if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
 }
