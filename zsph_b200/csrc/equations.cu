@@ -43,6 +43,8 @@
 // ptc.rhop at the end, when no reader is left.
 #include <cuda_bf16.h>
 
+#include <climits>
+
 #include "integrate.cuh"
 #include "zsph_internal.cuh"
 
@@ -71,11 +73,6 @@ __device__ __forceinline__ float sqrt_fast(float x) {
   return r;
 }
 __device__ __forceinline__ bool fluid_of(float w) { return !signbit(w); }
-__device__ __forceinline__ unsigned lanemask_lt() {
-  unsigned m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
 
 __device__ __forceinline__ float dist2(float dx, float dy, float dz) {
   return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
@@ -263,31 +260,6 @@ __device__ bool stage_window(WinHdr& wh, float4* win, int cap, const float4* con
   return __syncthreads_and(done ? 1 : 0) != 0;
 }
 
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-// A stencil row whose y-z slab lies farther than 2h from the particle cannot
-// hold a neighbour and is skipped (with a 0.1% margin on r^2, far above the
-// rounding of cell assignment); rows that wrap around in x (the reference's
-// linear hash aliases x overflow into the next row) are never skipped.
-template <int GF>
-__device__ __forceinline__ bool row_can_hit(const KParams& kp, int c, float4 pi, int r) {
-  const zsph_gpu_param_t& p = kp.p;
-  const int X = p.grid_xdim;
-  const int cz = c / kp.XY, cy = (c - cz * kp.XY) / X, cx = c - cz * kp.XY - cy * X;
-  if (cx - GF < 0 || cx + GF > X - 1) return true;
-  const int z = r / Stencil<GF>::W - GF, y = r % Stencil<GF>::W - GF;
-  // distance (in cell units) from the particle's actual position to the
-  // row's slab [cy+y, cy+y+1) x [cz+z, cz+z+1); zero if inside
-  const float uy = (pi.y - p.grid_ymin) * kp.inv_gs, uz = (pi.z - p.grid_zmin) * kp.inv_gs;
-  const float dy = fmaxf(fmaxf((float)(cy + y) - uy, uy - (float)(cy + y + 1)), 0.0f);
-  const float dz = fmaxf(fmaxf((float)(cz + z) - uz, uz - (float)(cz + z + 1)), 0.0f);
-  const float d2 = (dy * dy + dz * dz) * p.grid_size * p.grid_size;
-  return d2 <= kp.r2hi * 1.001f;
-}
 
 // Precision form: neighbour j's packed shadow moved into the frame of cell
 // ci (positions are offsets from the own cell's corner; neighbouring cells
@@ -502,6 +474,173 @@ __global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, z
     if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
     __syncwarp();
   }
+}
+
+// Builds the neighbour lists of 32 consecutive sorted particles per warp,
+// one lane per particle (the plain form).  A cell holds about 18 particles,
+// so one warp per cell leaves about half the lanes idle; here every lane has
+// a particle.  The warp's lanes are split into segments whose cells lie
+// within three consecutive linear cell indices (usually one segment per
+// warp).  For each stencil row a segment tests the union of its lanes' row
+// ranges, which is contiguous in the sorted order because every lane's row
+// range is: 64 candidates at a time staged in shared memory as x/y/z arrays,
+// tested two per step with packed f32x2 arithmetic, in blocks of eight so a
+// short row is not padded to 64.  Each lane keeps only the hits inside its
+// own row range (delta_ns.cu:39-46), so its neighbour set and visit order are
+// those of the per-cell build, and list entries are offsets from the lane's
+// own row start.  Hits are emitted into a padded per-lane list buffer in
+// shared memory and written out with coalesced 16-byte stores.
+//
+// With WALL, every non-fluid particle then extrapolates its (rho, p) from
+// the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
+// summed in the reference's visit order, and publishes it in the shadows.
+// warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
+template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
+
+template <int GF, bool WALL, int CW = kCellWarps>
+__global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, zsph_tmp_t t) {
+  constexpr int NR = Stencil<GF>::NR;
+  __shared__ __align__(16) float s_x[CW][64];
+  __shared__ __align__(16) float s_y[CW][64];
+  __shared__ __align__(16) float s_z[CW][64];
+  __shared__ __align__(16) uint16_t s_lst[CW][32][kLstStride];
+  __shared__ int s_rs[CW][NR][32];
+  __shared__ int s_cnt[CW][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int p0 = (blockIdx.x * CW + wid) * 32;
+  if (p0 >= kp.n) return;  // uniform per warp
+  const int i = p0 + lane;
+  const bool act = i < kp.n;
+  const int c = act ? t.hash[i] : INT_MAX;  // sorted: non-decreasing over the lanes
+  const float4 pi = s.sh.pr[act ? i : p0];
+  const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
+  const float r2max = kp.r2max;
+  float* sx = s_x[wid];
+  float* sy = s_y[wid];
+  float* sz = s_z[wid];
+  uint16_t* lst = s_lst[wid][lane];
+  int cnt = 0;
+  bool ovf = false;
+  unsigned todo = __ballot_sync(0xffffffffu, act);
+  while (todo) {
+    const int f = __ffs(todo) - 1;
+    const int cf = __shfl_sync(0xffffffffu, c, f);
+    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2;
+    todo &= ~__ballot_sync(0xffffffffu, inseg);
+    for (int r = 0; r < NR; ++r) {
+      int sl = 0, el = 0;
+      if (inseg) {
+        row_range<GF>(kp, t, c, r, sl, el);
+        s_rs[wid][r][lane] = sl;
+      }
+      const bool has = inseg && sl < el;
+      const int a = __reduce_min_sync(0xffffffffu, has ? sl : INT_MAX);
+      const int b = __reduce_max_sync(0xffffffffu, has ? el : INT_MIN);
+      for (int k0 = a; k0 < b; k0 += 64) {
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int j = k0 + 32 * h + lane;
+          float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
+          if (j < b) q = s.sh.pr[j];
+          sx[32 * h + lane] = q.x;
+          sy[32 * h + lane] = q.y;
+          sz[32 * h + lane] = q.z;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int base = k0 + 32 * h;
+          if (base >= b) break;  // uniform
+          unsigned mh = 0u;
+#pragma unroll
+          for (int blk = 0; blk < 4; ++blk) {
+            if (base + 8 * blk >= b) break;  // uniform: the rest is padding
+#pragma unroll
+            for (int tt = 8 * blk; tt < 8 * blk + 8; tt += 2) {
+              const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
+              const u64 y2 = *reinterpret_cast<const u64*>(&sy[32 * h + tt]);
+              const u64 z2 = *reinterpret_cast<const u64*>(&sz[32 * h + tt]);
+              const u64 dx = sub2(px, x2), dy = sub2(py, y2), dz = sub2(pz, z2);
+              const u64 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+              float r0, r1;
+              upk2(d2, r0, r1);
+              if (r0 <= r2max) mh |= 1u << tt;
+              if (r1 <= r2max) mh |= 2u << tt;
+            }
+          }
+          // keep the hits inside this lane's own row range [sl, el), not itself
+          const int lo = sl - base, hi = el - base;
+          unsigned keep = 0u;
+          if (has && hi > 0 && lo < 32) {
+            const unsigned up = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
+            const unsigned dn = lo <= 0 ? 0xffffffffu : ~((1u << lo) - 1u);
+            keep = up & dn;
+          }
+          if (i >= base && i < base + 32) keep &= ~(1u << (i - base));
+          mh &= keep;
+          if (!mh) continue;
+          const int off0 = base - sl;  // >= -bit of the lowest kept hit, so every offset is >= 0
+          if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
+            const unsigned ent0 = ((unsigned)r << kRowShift) + (unsigned)off0;
+            while (mh) {
+              const int bb = __ffs(mh) - 1;
+              mh &= mh - 1;
+              lst[cnt++] = (uint16_t)(ent0 + bb);
+            }
+          } else {
+            while (mh) {
+              const int bb = __ffs(mh) - 1;
+              mh &= mh - 1;
+              const int off = off0 + bb;
+              if (cnt < kMaxNb && off <= kOffMask)
+                lst[cnt] = (uint16_t)((r << kRowShift) | off);
+              else
+                ovf = true;
+              ++cnt;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (cnt > 254) ovf = true;
+  s_cnt[wid][lane] = (act && !ovf) ? cnt : 0;
+  if (WALL && act && !fluid_of(pi.w)) {
+    float rsum = 0.0f, wsum = 0.0f;
+    if (!ovf) {
+      for (int k = 0; k < cnt; ++k) {
+        const unsigned e = lst[k];
+        const int r = (int)(e >> kRowShift);
+        if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rs[wid][r][lane] + (int)(e & kOffMask), rsum, wsum);
+      }
+    } else {
+      for (int r = 0; r < NR; ++r) {
+        if (!Stencil<GF>::boundary_row(r)) continue;
+        int a, b;
+        row_range<GF>(kp, t, c, r, a, b);
+        for (int j = a; j < b; ++j) {
+          if (j == i) continue;
+          const float4 pj = s.sh.pr[j];
+          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+        }
+      }
+    }
+    const zsph_gpu_param_t& p = kp.p;
+    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+    if (rsum < 0.0f) rsum = 0.0f;
+    s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+    s.sh.vp[i].w = rsum;
+  }
+  __syncwarp();
+  // coalesced copy of the valid list prefixes: two 256-byte rows per store
+  for (int q = lane; q < 32 * (kMaxNb / 8); q += 32) {
+    const int row = q / (kMaxNb / 8), col = q % (kMaxNb / 8);
+    if (col * 8 < s_cnt[wid][row])
+      reinterpret_cast<uint4*>(s.nb + (size_t)(p0 + row) * kMaxNb)[col] =
+          *reinterpret_cast<const uint4*>(&s_lst[wid][row][col * 8]);
+  }
+  if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
 
 struct NbB1 {  // boundary loop 1
@@ -881,8 +1020,14 @@ template <bool WALL, bool BATCH>
 void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
   switch (kp.tune_cw) {
-    case 2: k_nblist<1, WALL, false, BATCH, 2><<<(kp.G + 1) / 2, 64, 0, st>>>(kp, s, t); break;
-    default: k_nblist<1, WALL, false, BATCH, 4><<<(kp.G + 3) / 4, 128, 0, st>>>(kp, s, t); break;
+    case 2:
+      if (BATCH) k_nblist<1, WALL, false, BATCH, 2><<<(kp.G + 1) / 2, 64, 0, st>>>(kp, s, t);
+      else k_nblist_seq<1, WALL, 2><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t);
+      break;
+    default:
+      if (BATCH) k_nblist<1, WALL, false, BATCH, 4><<<(kp.G + 3) / 4, 128, 0, st>>>(kp, s, t);
+      else k_nblist_seq<1, WALL, 4><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t);
+      break;
   }
 }
 
@@ -921,7 +1066,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
     return cudaGetLastError();
   }
   if (GF == 1) launch_nblist_tuned<true, false>(kp, s, t, st);
-  else k_nblist<GF, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+  else k_nblist_seq<GF, true, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, t);
   mark(pf, "nblist_wall", st);
   if (kp.equations == ZSPH_EQ_SIMPLE)
     k_boundary_simple<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, ptc, t);
@@ -1006,7 +1151,7 @@ cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, 
     if (GF != 1) return cudaErrorInvalidValue;
     k_nblist<1, false, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
   } else {
-    k_nblist<GF, false><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<GF, false, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, t);
   }
   return cudaGetLastError();
 }
