@@ -294,7 +294,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.tile_state, (size_t)h->tiles);
   if (!e) e = dalloc(s.misc, 8);
   if (!e) e = dalloc(s.big_list, (size_t)kBigListCap);
-  if (!e) e = dalloc(s.nb, (size_t)kMaxNb * n);
+  if (!e) e = dalloc(s.nb, (size_t)kMaxNb * ((n + 31) & ~(size_t)31));  // whole 32-particle list groups
   if (!e) e = dalloc(s.nb_cnt, n);
   if (!e) e = dalloc(s.flags, 1);
   if (!e) e = dalloc(s.sh.pr, n);

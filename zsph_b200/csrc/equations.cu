@@ -9,17 +9,20 @@
 // of its three neighbour loops per sub-step, one thread per particle, and
 // every lane of a warp pays for the full pair arithmetic whenever any lane
 // has a neighbour.  Here:
-//  * k_nblist filters the candidates ONCE per sub-step (the governing stencil
-//    is a superset of the boundary stencil).  One warp per particle: the
-//    lanes test 32 consecutive candidates of a stencil row at a time
-//    (coalesced 16-byte loads), and a ballot compacts the hits in candidate
-//    order into the particle's list, so the list is in the reference's visit
-//    order: stencil rows in (z, y) order, inside a row the sorted particle
-//    range.  Entries are 16-bit, row << 11 | offset inside the row's range,
-//    row-major (128 entries per particle), read back 8 per 16-byte load.
+//  * The list build filters the candidates ONCE per sub-step (the governing
+//    stencil is a superset of the boundary stencil).  k_nblist_seq (plain
+//    form) gives each warp 32 consecutive sorted particles, one per lane;
+//    k_nblist (precision and batched forms) one warp per cell.  Candidates
+//    are staged 64 at a time in shared memory and tested two per step with
+//    packed f32x2 arithmetic; the hits are emitted in candidate order, so a
+//    list is in the reference's visit order: stencil rows in (z, y) order,
+//    inside a row the sorted particle range.  Entries are 16-bit,
+//    row << 11 | offset inside the particle's row range, 128 per particle,
+//    stored blocked by 32-particle groups (nb_vec) and read 8 per 16-byte load.
 //  * k_boundary and k_governing walk their particle's list with one thread
 //    per particle, all lanes converged, loading the next four neighbours'
-//    packed data before doing their arithmetic.  The visit order is the
+//    packed data before doing their arithmetic.  k_boundary folds the
+//    reference's second loop into its first walk.  The visit order is the
 //    reference's, so the order-dependent recurrence on grad(rho).x
 //    (delta_ns.cu:244-245) sees the same sequence.
 //  * The pair arithmetic uses hardware reciprocal and square-root
@@ -61,6 +64,14 @@ constexpr int kRowShift = 11;
 constexpr int kOffMask = (1 << kRowShift) - 1;
 constexpr uint8_t kOverflow = 255;
 constexpr int kListVec = kMaxNb / 8;  // uint4 per particle list
+
+// Lists are stored blocked by groups of 32 consecutive particles: entries
+// 8b..8b+7 of particle i (one uint4) sit at uint4 index nb_vec(i, b), so the
+// 32 lanes of a warp walking 32 consecutive particles read 512 contiguous
+// bytes per list load, and the list build writes them the same way.
+__device__ __forceinline__ size_t nb_vec(int i, int b) {
+  return ((size_t)(i >> 5) * kListVec + (size_t)b) * 32 + (size_t)(i & 31);
+}
 
 __device__ __forceinline__ float rcp_fast(float x) {
   float r;
@@ -121,9 +132,9 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
                                      const int* re, const int* fb, int fdummy, Fetch&& fetch, Use&& use) {
   const int cnt = s.nb_cnt[i];
   if (cnt != kOverflow) {
-    const uint4* lst = reinterpret_cast<const uint4*>(s.nb) + (size_t)i * kListVec;
+    const uint4* lst = reinterpret_cast<const uint4*>(s.nb);
     for (int k = 0; k < cnt; k += 8) {
-      const uint4 v = lst[k >> 3];
+      const uint4 v = lst[nb_vec(i, k >> 3)];
       const unsigned wv[4] = {v.x, v.y, v.z, v.w};
       int js[8];
 #pragma unroll
@@ -464,13 +475,11 @@ __global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, z
       s.sh.vp[i].w = rsum;
     }
     __syncwarp();
-    // coalesced copy of the valid list prefixes: two 256-byte rows per store
-    for (int q = lane; q < 32 * (kMaxNb / 8); q += 32) {
-      const int row = q / (kMaxNb / 8), col = q % (kMaxNb / 8);
-      if (col * 8 < s_cnt[wid][row])
-        reinterpret_cast<uint4*>(s.nb + (size_t)(p0 + row) * kMaxNb)[col] =
-            *reinterpret_cast<const uint4*>(&s_lst[wid][row][col * 8]);
-    }
+    // copy of the valid list prefixes, one 16-byte block of every lane's list per store
+    for (int col = 0; col < kListVec; ++col)
+      if (col * 8 < s_cnt[wid][lane])
+        reinterpret_cast<uint4*>(s.nb)[nb_vec(p0 + lane, col)] =
+            *reinterpret_cast<const uint4*>(&s_lst[wid][lane][col * 8]);
     if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
     __syncwarp();
   }
@@ -633,13 +642,12 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
     s.sh.vp[i].w = rsum;
   }
   __syncwarp();
-  // coalesced copy of the valid list prefixes: two 256-byte rows per store
-  for (int q = lane; q < 32 * (kMaxNb / 8); q += 32) {
-    const int row = q / (kMaxNb / 8), col = q % (kMaxNb / 8);
-    if (col * 8 < s_cnt[wid][row])
-      reinterpret_cast<uint4*>(s.nb + (size_t)(p0 + row) * kMaxNb)[col] =
-          *reinterpret_cast<const uint4*>(&s_lst[wid][row][col * 8]);
-  }
+  // coalesced copy of the valid list prefixes: the warp's 32 particles form
+  // one list group, so each store writes 512 contiguous bytes
+  for (int col = 0; col < kListVec; ++col)
+    if (col * 8 < s_cnt[wid][lane])
+      reinterpret_cast<uint4*>(s.nb)[nb_vec(p0 + lane, col)] =
+          *reinterpret_cast<const uint4*>(&s_lst[wid][lane][col * 8]);
   if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
 
@@ -1170,7 +1178,8 @@ __global__ void __launch_bounds__(kSearchBlock) k_nb_counts(KParams kp, Scratch 
     return;
   }
   int b = 0;
-  for (int k = 0; k < cnt; ++k) b += Stencil<GF>::boundary_row((int)(s.nb[(size_t)i * kMaxNb + k] >> kRowShift));
+  for (int k = 0; k < cnt; ++k)
+    b += Stencil<GF>::boundary_row((int)(s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)] >> kRowShift));
   if (nb_boundary) nb_boundary[i] = b;
   if (nb_governing) nb_governing[i] = cnt;
 }

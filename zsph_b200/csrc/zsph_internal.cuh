@@ -126,7 +126,7 @@ struct Scratch {
                      //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch
   unsigned long long* tile_state;  // [tiles] one-pass scan: (tag << 32) | prefix value, tag from the epoch
   int* big_list;     // [kBigListCap]
-  uint16_t* nb;      // [n * kMaxNb] neighbour lists, row-major (entry k of particle i at i*kMaxNb+k)
+  uint16_t* nb;      // [ceil(n/32)*32 * kMaxNb] neighbour lists, blocked by 32-particle groups (equations.cu)
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
   int* flags;        // [1]   ZSPH_FLAG_* bits
   Shadow sh;
