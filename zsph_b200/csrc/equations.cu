@@ -512,9 +512,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
   __shared__ __align__(16) float s_x[CW][64];
   __shared__ __align__(16) float s_y[CW][64];
   __shared__ __align__(16) float s_z[CW][64];
-  __shared__ __align__(16) uint16_t s_lst[CW][32][kLstStride];
+  __shared__ __align__(16) uint16_t s_ring[CW][32][16];  // per lane: the list's current and previous 8-entry block
   __shared__ int s_rs[CW][NR][32];
-  __shared__ int s_cnt[CW][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int p0 = (blockIdx.x * CW + wid) * 32;
   if (p0 >= kp.n) return;  // uniform per warp
@@ -527,9 +526,15 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
   float* sx = s_x[wid];
   float* sy = s_y[wid];
   float* sz = s_z[wid];
-  uint16_t* lst = s_lst[wid][lane];
+  uint16_t* ring = s_ring[wid][lane];
+  uint4* nbv = reinterpret_cast<uint4*>(s.nb);
   int cnt = 0;
   bool ovf = false;
+  // stores entry number cnt (< kMaxNb); a completed 8-entry block goes to global memory
+  auto put = [&](unsigned e) {
+    ring[cnt & 15] = (uint16_t)e;
+    if ((cnt & 7) == 7) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & 8));
+  };
   unsigned todo = __ballot_sync(0xffffffffu, act);
   while (todo) {
     const int f = __ffs(todo) - 1;
@@ -595,15 +600,16 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
             while (mh) {
               const int bb = __ffs(mh) - 1;
               mh &= mh - 1;
-              lst[cnt++] = (uint16_t)(ent0 + bb);
+              put(ent0 + bb);
+              ++cnt;
             }
           } else {
             while (mh) {
               const int bb = __ffs(mh) - 1;
               mh &= mh - 1;
               const int off = off0 + bb;
-              if (cnt < kMaxNb && off <= kOffMask)
-                lst[cnt] = (uint16_t)((r << kRowShift) | off);
+              if (cnt < kMaxNb && off <= kOffMask && !ovf)
+                put(((unsigned)r << kRowShift) | (unsigned)off);
               else
                 ovf = true;
               ++cnt;
@@ -614,12 +620,12 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
     }
   }
   if (cnt > 254) ovf = true;
-  s_cnt[wid][lane] = (act && !ovf) ? cnt : 0;
+  if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & 8));
   if (WALL && act && !fluid_of(pi.w)) {
     float rsum = 0.0f, wsum = 0.0f;
     if (!ovf) {
-      for (int k = 0; k < cnt; ++k) {
-        const unsigned e = lst[k];
+      for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
+        const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
         const int r = (int)(e >> kRowShift);
         if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rs[wid][r][lane] + (int)(e & kOffMask), rsum, wsum);
       }
@@ -641,13 +647,6 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
     s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
     s.sh.vp[i].w = rsum;
   }
-  __syncwarp();
-  // coalesced copy of the valid list prefixes: the warp's 32 particles form
-  // one list group, so each store writes 512 contiguous bytes
-  for (int col = 0; col < kListVec; ++col)
-    if (col * 8 < s_cnt[wid][lane])
-      reinterpret_cast<uint4*>(s.nb)[nb_vec(p0 + lane, col)] =
-          *reinterpret_cast<const uint4*>(&s_lst[wid][lane][col * 8]);
   if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
 
