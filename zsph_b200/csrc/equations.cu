@@ -506,8 +506,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, z
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 
-template <int GF, bool WALL, int CW = kCellWarps>
-__global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, zsph_tmp_t t) {
+template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false>
+__global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   __shared__ __align__(16) float s_x[CW][64];
   __shared__ __align__(16) float s_y[CW][64];
@@ -516,13 +516,14 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
   __shared__ int s_rs[CW][NR][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int p0 = (blockIdx.x * CW + wid) * 32;
-  if (p0 >= kp.n) return;  // uniform per warp
+  if (p0 >= kp_arg.n) return;  // uniform per warp
   const int i = p0 + lane;
-  const bool act = i < kp.n;
+  const bool act = i < kp_arg.n;
   const int c = act ? t.hash[i] : INT_MAX;  // sorted: non-decreasing over the lanes
+  // batched form: the scene of the lane's cell (scenes own disjoint cell ranges)
+  const int scn = BATCH && act ? scene_of(kp_arg.scene_cbase, kp_arg.nscenes, c) : 0;
   const float4 pi = s.sh.pr[act ? i : p0];
   const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
-  const float r2max = kp.r2max;
   float* sx = s_x[wid];
   float* sy = s_y[wid];
   float* sz = s_z[wid];
@@ -539,8 +540,11 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
   while (todo) {
     const int f = __ffs(todo) - 1;
     const int cf = __shfl_sync(0xffffffffu, c, f);
-    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2;
+    const int sf = BATCH ? __shfl_sync(0xffffffffu, scn, f) : 0;
+    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2 && (!BATCH || scn == sf);
     todo &= ~__ballot_sync(0xffffffffu, inseg);
+    const KParams kp = BATCH ? scene_kp(kp_arg, sf) : kp_arg;  // the segment's scene
+    const float r2max = kp.r2max;
     for (int r = 0; r < NR; ++r) {
       int sl = 0, el = 0;
       if (inseg) {
@@ -622,6 +626,7 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp, Scratch s, z
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & 8));
   if (WALL && act && !fluid_of(pi.w)) {
+    const KParams kp = BATCH ? scene_kp(kp_arg, scn) : kp_arg;
     float rsum = 0.0f, wsum = 0.0f;
     if (!ovf) {
       for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
@@ -1027,14 +1032,8 @@ template <bool WALL, bool BATCH>
 void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
   switch (kp.tune_cw) {
-    case 2:
-      if (BATCH) k_nblist<1, WALL, false, BATCH, 2><<<(kp.G + 1) / 2, 64, 0, st>>>(kp, s, t);
-      else k_nblist_seq<1, WALL, 2><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t);
-      break;
-    default:
-      if (BATCH) k_nblist<1, WALL, false, BATCH, 4><<<(kp.G + 3) / 4, 128, 0, st>>>(kp, s, t);
-      else k_nblist_seq<1, WALL, 4><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t);
-      break;
+    case 2: k_nblist_seq<1, WALL, 2, BATCH><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t); break;
+    default: k_nblist_seq<1, WALL, 4, BATCH><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t); break;
   }
 }
 
