@@ -1,7 +1,7 @@
 // delta-SPH pair-interaction kernels for sm_100a.
 //
 // Reference path replaced (single_gpu_sph_src/):
-//   equation/delta_ns.cu:5-177   cuda_boundary_ns  -> k_nblist (list + wall pressure) + k_boundary
+//   equation/delta_ns.cu:5-177   cuda_boundary_ns  -> k_nblist_seq (list + wall pressure) + k_boundary
 //   equation/delta_ns.cu:179-267 cuda_govering_ns  -> k_governing (optionally fused with time_int.cu)
 //   lib/time_int.cu:3-92         cuda_prediction / cuda_correction -> k_integrate or k_governing epilogue
 //
@@ -10,9 +10,8 @@
 // every lane of a warp pays for the full pair arithmetic whenever any lane
 // has a neighbour.  Here:
 //  * The list build filters the candidates ONCE per sub-step (the governing
-//    stencil is a superset of the boundary stencil).  k_nblist_seq (plain
-//    form) gives each warp 32 consecutive sorted particles, one per lane;
-//    k_nblist (precision and batched forms) one warp per cell.  Candidates
+//    stencil is a superset of the boundary stencil).  k_nblist_seq gives
+//    each warp 32 consecutive sorted particles, one per lane.  Candidates
 //    are staged 64 at a time in shared memory and tested two per step with
 //    packed f32x2 arithmetic; the hits are emitted in candidate order, so a
 //    list is in the reference's visit order: stencil rows in (z, y) order,
@@ -39,7 +38,7 @@
 // non-fluid particles (densities are non-negative).
 //
 // Wall densities: the reference writes them in place while neighbours read
-// them (a race, delta_ns.cu:65,130,151).  Here k_nblist extrapolates every
+// them (a race, delta_ns.cu:65,130,151).  Here k_nblist_seq extrapolates every
 // wall's (rho, p) first and publishes it in the packed shadows; k_boundary
 // reads neighbours' densities from the shadows (new wall values) and a
 // wall's own old density from ptc.rhop, and writes the new wall values to
@@ -334,157 +333,7 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
   return r;
 }
 
-constexpr int kCellWarps = 4;            // cells (warps) per CTA in the list build
-constexpr int kLstStride = kMaxNb + 8;   // uint16 entries per lane row of the shared list buffer (272 bytes)
-
-// Builds the neighbour lists, one warp per grid cell and one lane per
-// particle of the cell (chunks of 32 for crowded cells).  All particles of
-// a cell share the cell's stencil rows (delta_ns.cu:39-46), so the warp
-// walks each row's candidates once: 64 candidates at a time are staged in
-// shared memory as separate x/y/z arrays and every lane tests two of them per
-// step with packed f32x2 arithmetic, collecting hit bits.  The hits are then
-// emitted in candidate order (= the reference's visit order) into a padded
-// per-lane list buffer in shared memory and written out with coalesced
-// 16-byte stores.  The exact threshold test runs only for candidates whose
-// r^2 lies within 1e-5 of (2h)^2.
-//
-// With WALL, every non-fluid particle then extrapolates its (rho, p) from
-// the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
-// summed in the reference's visit order, and publishes it in the shadows.
-template <int GF, bool WALL, bool PRECISE = false, bool BATCH = false, int CW = kCellWarps>
-__global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, zsph_tmp_t t) {
-  constexpr int NR = Stencil<GF>::NR;
-  static_assert(NR <= 32, "one lane per stencil row");
-  __shared__ __align__(16) float s_x[CW][64];
-  __shared__ __align__(16) float s_y[CW][64];
-  __shared__ __align__(16) float s_z[CW][64];
-  __shared__ __align__(16) uint16_t s_lst[CW][32][kLstStride];
-  __shared__ int s_rows[CW][32];
-  __shared__ int s_cnt[CW][32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int c = blockIdx.x * CW + wid;
-  if (c >= kp_arg.G) return;  // uniform per warp
-  KParams kp_scene;  // batched form: the parameters of the cell's scene
-  if constexpr (BATCH) kp_scene = kp_of_cell(kp_arg, c);
-  const KParams& kp = BATCH ? kp_scene : kp_arg;
-  const int ca = s.cell_lb[c], cb = s.cell_lb[c + 1];
-  if (ca >= cb) return;
-  int3 cc{0, 0, 0};  // precision form: the warp's cell, the frame of its particles
-  if (PRECISE) {
-    cc.z = c / kp.XY;
-    cc.y = (c - cc.z * kp.XY) / kp.p.grid_xdim;
-    cc.x = c - cc.z * kp.XY - cc.y * kp.p.grid_xdim;
-  }
-  int rs = 0, re = 0;
-  if (lane < NR) row_range<GF>(kp, t, c, lane, rs, re);
-  s_rows[wid][lane] = rs;
-  float* sx = s_x[wid];
-  float* sy = s_y[wid];
-  float* sz = s_z[wid];
-  uint16_t* lst = s_lst[wid][lane];
-  for (int p0 = ca; p0 < cb; p0 += 32) {
-    const int i = p0 + lane;
-    const bool act = i < cb;
-    const float4 pi = s.sh.pr[act ? i : p0];
-    const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
-    int cnt = 0;
-    bool ovf = false;
-    for (int r = 0; r < NR; ++r) {
-      const int a = __shfl_sync(0xffffffffu, rs, r), b = __shfl_sync(0xffffffffu, re, r);
-      for (int k0 = a; k0 < b; k0 += 64) {
-        __syncwarp();
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int j = k0 + 32 * h + lane;
-          float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
-          if (j < b) q = shadow_pr<PRECISE>(kp, s, j, cc);
-          sx[32 * h + lane] = q.x;
-          sy[32 * h + lane] = q.y;
-          sz[32 * h + lane] = q.z;
-        }
-        __syncwarp();
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          unsigned mh = 0u;
-#pragma unroll
-          for (int tt = 0; tt < 32; tt += 2) {
-            const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
-            const u64 y2 = *reinterpret_cast<const u64*>(&sy[32 * h + tt]);
-            const u64 z2 = *reinterpret_cast<const u64*>(&sz[32 * h + tt]);
-            const u64 dx = sub2(px, x2), dy = sub2(py, y2), dz = sub2(pz, z2);
-            const u64 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
-            float r0, r1;
-            upk2(d2, r0, r1);
-            if (r0 <= kp.r2max) mh |= 1u << tt;
-            if (r1 <= kp.r2max) mh |= 2u << tt;
-          }
-          const int base = k0 + 32 * h;
-          if (i >= base && i < base + 32) mh &= ~(1u << (i - base));  // the particle itself
-          if (!act) mh = 0u;
-          const int off0 = base - a;
-          if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
-            const unsigned ent0 = ((unsigned)r << kRowShift) | (unsigned)off0;
-            while (mh) {
-              const int bb = __ffs(mh) - 1;
-              mh &= mh - 1;
-              lst[cnt++] = (uint16_t)(ent0 + bb);
-            }
-          } else {
-            while (mh) {
-              const int bb = __ffs(mh) - 1;
-              mh &= mh - 1;
-              const int off = off0 + bb;
-              if (cnt < kMaxNb && off <= kOffMask)
-                lst[cnt] = (uint16_t)((r << kRowShift) | off);
-              else
-                ovf = true;
-              ++cnt;
-            }
-          }
-        }
-      }
-    }
-    if (cnt > 254) ovf = true;
-    s_cnt[wid][lane] = (act && !ovf) ? cnt : 0;
-    if (WALL && act && !fluid_of(pi.w)) {
-      float rsum = 0.0f, wsum = 0.0f;
-      if (!ovf) {
-        for (int k = 0; k < cnt; ++k) {
-          const unsigned e = lst[k];
-          const int r = (int)(e >> kRowShift);
-          if (Stencil<GF>::boundary_row(r))
-            wall_term<PRECISE>(kp, s, pi, s_rows[wid][r] + (int)(e & kOffMask), rsum, wsum, cc);
-        }
-      } else {
-        for (int r = 0; r < NR; ++r) {
-          if (!Stencil<GF>::boundary_row(r)) continue;
-          int a, b;
-          row_range<GF>(kp, t, c, r, a, b);
-          for (int j = a; j < b; ++j) {
-            if (j == i) continue;
-            const float4 pj = shadow_pr<PRECISE>(kp, s, j, cc);
-            if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z)))
-              wall_term<PRECISE>(kp, s, pi, j, rsum, wsum, cc);
-          }
-        }
-      }
-      const zsph_gpu_param_t& p = kp.p;
-      if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-      if (rsum < 0.0f) rsum = 0.0f;
-      s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-      s.sh.vp[i].w = rsum;
-    }
-    __syncwarp();
-    // copy of the valid list prefixes, one 16-byte block of every lane's list per store
-    for (int col = 0; col < kListVec; ++col)
-      if (col * 8 < s_cnt[wid][lane])
-        reinterpret_cast<uint4*>(s.nb)[nb_vec(p0 + lane, col)] =
-            *reinterpret_cast<const uint4*>(&s_lst[wid][lane][col * 8]);
-    if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
-    __syncwarp();
-  }
-}
-
+constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // Builds the neighbour lists of 32 consecutive sorted particles per warp,
 // one lane per particle (the plain form).  A cell holds about 18 particles,
 // so one warp per cell leaves about half the lanes idle; here every lane has
@@ -506,7 +355,7 @@ __global__ void __launch_bounds__(CW * 32) k_nblist(KParams kp_arg, Scratch s, z
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 
-template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false>
+template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
 __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
   __shared__ __align__(16) float s_x[CW][64];
@@ -523,7 +372,9 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   // batched form: the scene of the lane's cell (scenes own disjoint cell ranges)
   const int scn = BATCH && act ? scene_of(kp_arg.scene_cbase, kp_arg.nscenes, c) : 0;
   const float4 pi = s.sh.pr[act ? i : p0];
-  const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
+  // precision form: the lane's own cell (its position is the offset from that cell's corner)
+  const int3 ci = PRECISE && act ? unpack_cell(kp_arg.c3n[i]) : int3{0, 0, 0};
+  u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
   float* sx = s_x[wid];
   float* sy = s_y[wid];
   float* sz = s_z[wid];
@@ -541,10 +392,23 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
     const int f = __ffs(todo) - 1;
     const int cf = __shfl_sync(0xffffffffu, c, f);
     const int sf = BATCH ? __shfl_sync(0xffffffffu, scn, f) : 0;
-    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2 && (!BATCH || scn == sf);
+    const int xd = kp_arg.p.grid_xdim;
+    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2 && (!BATCH || scn == sf) && (!PRECISE || c / xd == cf / xd);
     todo &= ~__ballot_sync(0xffffffffu, inseg);
     const KParams kp = BATCH ? scene_kp(kp_arg, sf) : kp_arg;  // the segment's scene
     const float r2max = kp.r2max;
+    // Precision form: positions are compared in the frame of the cell one
+    // step in x past the segment's first cell.  The segment's cells are that
+    // cell's x-neighbours (shift -1, 0 or +1 cell) and every candidate lies
+    // within two cells of it, so each shift k * gs is exact and one rounding
+    // forms every coordinate.
+    int3 mid{0, 0, 0};
+    if (PRECISE) {
+      const int cfx = __shfl_sync(0xffffffffu, ci.x, f);
+      mid = make_int3(cfx + 1, __shfl_sync(0xffffffffu, ci.y, f), __shfl_sync(0xffffffffu, ci.z, f));
+      const float sx0 = pi.x + (float)(ci.x - mid.x) * kp.p.grid_size;
+      px = pk2(sx0, sx0);
+    }
     for (int r = 0; r < NR; ++r) {
       int sl = 0, el = 0;
       if (inseg) {
@@ -560,7 +424,7 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
         for (int h = 0; h < 2; ++h) {
           const int j = k0 + 32 * h + lane;
           float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
-          if (j < b) q = s.sh.pr[j];
+          if (j < b) q = shadow_pr<PRECISE>(kp, s, j, mid);
           sx[32 * h + lane] = q.x;
           sy[32 * h + lane] = q.y;
           sz[32 * h + lane] = q.z;
@@ -632,7 +496,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
       for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
         const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
         const int r = (int)(e >> kRowShift);
-        if (Stencil<GF>::boundary_row(r)) wall_term(kp, s, pi, s_rs[wid][r][lane] + (int)(e & kOffMask), rsum, wsum);
+        if (Stencil<GF>::boundary_row(r))
+          wall_term<PRECISE>(kp, s, pi, s_rs[wid][r][lane] + (int)(e & kOffMask), rsum, wsum, ci);
       }
     } else {
       for (int r = 0; r < NR; ++r) {
@@ -641,8 +506,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
         row_range<GF>(kp, t, c, r, a, b);
         for (int j = a; j < b; ++j) {
           if (j == i) continue;
-          const float4 pj = s.sh.pr[j];
-          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term(kp, s, pi, j, rsum, wsum);
+          const float4 pj = shadow_pr<PRECISE>(kp, s, j, ci);
+          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term<PRECISE>(kp, s, pi, j, rsum, wsum, ci);
         }
       }
     }
@@ -943,7 +808,7 @@ struct NbS {  // simple boundary / governing
 
 // single_gpu_sph_src/equation/simple_ns.cu:3-97: scalar div(v) over fluid
 // pairs of the boundary stencil into tmp.dofv; new wall (rho, p) (computed
-// by k_nblist) into ptc.rhop.  Walls read only fluid densities here, so the
+// by k_nblist_seq) into ptc.rhop.  Walls read only fluid densities here, so the
 // reference has no wall-density race in this kernel.
 template <int GF>
 __global__ void __launch_bounds__(kPairBlock) k_boundary_simple(KParams kp, Scratch s, zsph_ptc_t ptc,
@@ -1024,7 +889,6 @@ __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc
   integrate_one<MODE>(kp, ptc, ptc, i, reinterpret_cast<const float4*>(t.acc_drhodt)[i]);
 }
 
-inline int cell_blocks(int G) { return (G + kCellWarps - 1) / kCellWarps; }
 inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 
 // list build (grid factor 1) with the tuned number of cells per CTA
@@ -1065,7 +929,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
   }
   if (kp.c3o) {  // precision form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
-    k_nblist<1, true, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<1, true, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, t);
     mark(pf, "nblist_wall", st);
     k_boundary<1, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
     mark(pf, "boundary", st);
@@ -1155,7 +1019,7 @@ cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, 
     launch_nblist_tuned<false, true>(kp, s, t, st);
   } else if (kp.c3o) {
     if (GF != 1) return cudaErrorInvalidValue;
-    k_nblist<1, false, true><<<cell_blocks(kp.G), kCellWarps * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<1, false, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, t);
   } else {
     k_nblist_seq<GF, false, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, t);
   }
