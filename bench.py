@@ -183,6 +183,64 @@ def ncu_traffic(kernel_group: str):
     return d.get(kernel_group)
 
 
+# ---------------------------------------------------------------- pair kernels
+# FP32 operations per interacting pair, counted from the pair arithmetic of
+# k_boundary (L matrix, div v, the folded gradient sums) and k_governing
+# (continuity, delta diffusion with its recurrence, pressure, viscosity) for a
+# fluid-fluid pair; an FMA counts 2, a MUFU reciprocal or square root 1.
+FLOP_PER_PAIR = {"boundary": 54, "governing": 68}
+
+
+def stencil_candidates(sol, n):
+    """Candidates per particle in the governing stencil (3x3 rows of 3 cells,
+    delta_ns.cu:200-212) of the sorted state, from the search's cell bounds."""
+    import numpy as np
+    t = sol.download_tmp()
+    gs, ge, h = t["grid_start"].astype(np.int64), t["grid_end"].astype(np.int64), t["hash"].astype(np.int64)
+    gp = sol.gp
+    X, XY = gp.grid_xdim, gp.grid_xdim * gp.grid_ydim
+    tot = np.zeros(n, np.int64)
+    for z in (-1, 0, 1):
+        for y in (-1, 0, 1):
+            c = h + z * XY + y * X
+            cs, ce = c - 1, c + 1
+            ok = (cs >= gp.grid_hash_min) & (ce <= gp.grid_hash_max)
+            s = gs[np.clip(cs, 0, len(gs) - 1)]
+            e = ge[np.clip(ce, 0, len(ge) - 1)]
+            tot += np.where(ok, np.maximum(e - s, 0), 0)
+    return float(tot.mean())
+
+
+def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks):
+    """Rates of the pair kernels: candidate tests/s of the list build,
+    interacting pair evaluations/s and FP32 FLOP/s of boundary and governing
+    against the nominal FP32 peak (148 SMs x 128 lanes x 2 x max SM clock),
+    and DRAM GB/s from the committed ncu traffic."""
+    import numpy as np
+    mhz = (clocks or {}).get("sm_max_mhz") or 1965.0
+    fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    cand = stencil_candidates(sol, n)
+    out = {"fp32_peak_tflops_nominal": fp32_peak}
+    t_nb = kern.get("nblist_wall", {}).get("ms_per_step", 0) / 2e3
+    if t_nb:
+        tr = ncu_traffic("nblist_wall")
+        out["nblist_wall"] = {"ms_per_substep": t_nb * 1e3, "stencil_candidates_per_particle": cand,
+                              "candidate_tests_per_s": cand * n / t_nb,
+                              "dram_gbs": tr / t_nb / 1e9 if tr else None}
+    for name, nb in (("boundary", nb_b), ("governing", nb_g)):
+        t = kern.get(name, {}).get("ms_per_step", 0) / 2e3
+        if not t:
+            continue
+        pairs = float(np.mean(nb[nb >= 0]))
+        evals = pairs * n / t
+        tr = ncu_traffic(name)
+        out[name] = {"ms_per_substep": t * 1e3, "interacting_pairs_per_particle": pairs, "pair_evals_per_s": evals,
+                     "fp32_tflops": evals * FLOP_PER_PAIR[name] / 1e12,
+                     "fp32_frac_of_nominal_peak": evals * FLOP_PER_PAIR[name] / 1e12 / fp32_peak,
+                     "dram_gbs": tr / t / 1e9 if tr else None}
+    return out
+
+
 # ---------------------------------------------------------------- CPU baseline
 def cpu_baseline(case, target_s: float) -> dict:
     """The FP32 CPU oracle (OpenMP restatement of the reference's kernels) on
@@ -377,6 +435,7 @@ def run_ours(args, dist: Dist):
                 "peak_source": f"{peaks['source']} hbm_gbs (copy test)",
                 "traffic": ncu_traffic("search_group")}
     gov_ms = kern.get("governing", {}).get("ms_per_step", 0) / 2
+    pair = pair_kernel_rates(sol, kern, nb_b, nb_g, n, ck)
     dominant = {"kernel": dom[0], "ms_per_step": dom[1]["ms_per_step"], "share": dom[1]["share"],
                 "bound": "fp32 pair arithmetic / latency (not hbm, no tensor-core work on the pair path)",
                 "interacting_pairs_per_particle": pairs_gov,
@@ -424,7 +483,7 @@ def run_ours(args, dist: Dist):
                    "l2": "inputs larger than L2 (particle state 0.76 GB + scratch per step)",
                    "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
-        "roofline": roofline, "dominant_kernel": dominant, "kernels": kern, "cpu_baseline": cpu,
+        "roofline": roofline, "dominant_kernel": dominant, "pair_kernels": pair, "kernels": kern, "cpu_baseline": cpu,
         "learned": learned, "batched": batched, "status_flags": flags,
     }
     sol.close()
