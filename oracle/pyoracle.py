@@ -177,32 +177,7 @@ class Oracle:
     def attach_rigid(self, first, count, mass, vel=(0, 0, 0), omega=(0, 0, 0), q=(1, 0, 0, 0)):
         """Centroid, inertia (Test_6DOF/equation/rigid_info.cpp:3-39) and
         body-frame offsets from the current positions of `old`."""
-        st = self.old
-        ids = st["table"] + np.arange(self.p.ptc_num)
-        sel = (st["type"] == 2) & (ids >= first) & (ids < first + count)
-        x = np.zeros((count, 3))
-        x[ids[sel] - first] = st["pos"][sel].astype(np.float64)
-        c = x.mean(0)
-        r = x - c
-        I = np.zeros((3, 3))
-        for a in range(3):
-            for b in range(3):
-                I[a, b] = -(r[:, a] * r[:, b]).sum()
-        I += np.eye(3) * (r * r).sum()
-        I *= mass / count
-        qq = np.asarray(q, np.float64) / np.linalg.norm(q)
-        w, xx, yy, zz = qq
-        R = np.array([[1 - 2 * (yy * yy + zz * zz), 2 * (xx * yy - w * zz), 2 * (xx * zz + w * yy)],
-                      [2 * (xx * yy + w * zz), 1 - 2 * (xx * xx + zz * zz), 2 * (yy * zz - w * xx)],
-                      [2 * (xx * zz - w * yy), 2 * (yy * zz + w * xx), 1 - 2 * (xx * xx + yy * yy)]])
-        self._r0 = np.ascontiguousarray(r @ R)  # R^T r per row
-        Ib = R.T @ I @ R
-        b = ORigid()
-        for name, v in (("x", c), ("xn", c), ("v", vel), ("vn", vel), ("w", omega), ("wn", omega), ("q", qq),
-                        ("qn", qq), ("I", Ib.ravel()), ("Iinv", np.linalg.inv(Ib).ravel())):
-            getattr(b, name)[:] = list(np.asarray(v, np.float64))
-        b.M, b.g, b.first, b.count = mass, self.p.g, first, count
-        b.r0 = self._r0.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        b, self._r0 = rigid_from(self.p, self.old, first, count, mass, vel, omega, q)
         self.rigid = b
         f = self._fn("rigid_place")
         f(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self.rigid))
@@ -241,6 +216,122 @@ class Oracle:
         self._fn("neighbor_count")(ctypes.byref(self.p), ctypes.byref(self._s(which)), ctypes.byref(self._t),
                                    _I(ylast), _p(out))
         return out
+
+
+def rigid_from(p, st, first, count, mass, vel=(0, 0, 0), omega=(0, 0, 0), q=(1, 0, 0, 0)):
+    """The oracle's body (ORigid) and its body-frame offsets r0[count][3] from
+    the positions of the state dict st: centroid, inertia about it
+    (Test_6DOF/equation/rigid_info.cpp:3-39) and the pose q."""
+    ids = st["table"] + np.arange(p.ptc_num)
+    sel = (st["type"] == 2) & (ids >= first) & (ids < first + count)
+    x = np.zeros((count, 3))
+    x[ids[sel] - first] = st["pos"][sel].astype(np.float64)
+    c = x.mean(0)
+    r = x - c
+    I = np.zeros((3, 3))
+    for a in range(3):
+        for b in range(3):
+            I[a, b] = -(r[:, a] * r[:, b]).sum()
+    I += np.eye(3) * (r * r).sum()
+    I *= mass / count
+    qq = np.asarray(q, np.float64) / np.linalg.norm(q)
+    w, xx, yy, zz = qq
+    R = np.array([[1 - 2 * (yy * yy + zz * zz), 2 * (xx * yy - w * zz), 2 * (xx * zz + w * yy)],
+                  [2 * (xx * yy + w * zz), 1 - 2 * (xx * xx + zz * zz), 2 * (yy * zz - w * xx)],
+                  [2 * (xx * zz - w * yy), 2 * (yy * zz + w * xx), 1 - 2 * (xx * xx + yy * yy)]])
+    r0 = np.ascontiguousarray(r @ R)  # R^T r per row
+    Ib = R.T @ I @ R
+    b = ORigid()
+    for name, v in (("x", c), ("xn", c), ("v", vel), ("vn", vel), ("w", omega), ("wn", omega), ("q", qq),
+                    ("qn", qq), ("I", Ib.ravel()), ("Iinv", np.linalg.inv(Ib).ravel())):
+        getattr(b, name)[:] = list(np.asarray(v, np.float64))
+    b.M, b.g, b.first, b.count = mass, p.g, first, count
+    b.r0 = r0.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    return b, r0
+
+
+GPU_ORACLE_SO = os.path.join(HERE, "libgpu_oracle.so")
+_gpu = None
+
+
+def gpu_lib() -> ctypes.CDLL:
+    global _gpu
+    if _gpu is None:
+        _gpu = ctypes.CDLL(GPU_ORACLE_SO)
+        _gpu.gor_create.restype = _VP
+        _gpu.gor_create.argtypes = [ctypes.POINTER(OParams)] + [_VP] * 8
+        _gpu.gor_error.restype = ctypes.c_char_p
+        _gpu.gor_error.argtypes = [_VP]
+        for f in ("gor_attach_rigid", "gor_step", "gor_download"):
+            getattr(_gpu, f).restype = _I
+        _gpu.gor_attach_rigid.argtypes = [_VP, ctypes.POINTER(ORigid)]
+        _gpu.gor_step.argtypes = [_VP, _I]
+        _gpu.gor_download.argtypes = [_VP] * 6
+        _gpu.gor_rigid.argtypes = [_VP, ctypes.POINTER(ORigid)]
+        _gpu.gor_destroy.argtypes = [_VP]
+    return _gpu
+
+
+class GpuOracle64:
+    """The FP64 oracle run on the GPU (oracle/gpu_oracle.cu, test
+    infrastructure): the T = double instance of the same restatement with the
+    same arithmetic and visit order, for cases too large for the CPU oracle.
+    Steps use the WALLS_FIRST order; with a body attached, every step is the
+    oracle's step_rigid."""
+
+    def __init__(self, json, state):
+        rc, self.p = params(json)
+        if rc != 0:
+            raise ValueError("dt > dt_max")
+        n = self.p.ptc_num
+        cv = lambda a, shape: (np.zeros(shape) if a is None else np.ascontiguousarray(a, np.float64))
+        self._host = dict(pos=cv(state.pos, (n, 3)), vel=cv(state.vel, (n, 3)), rhop=cv(state.rhop, (n, 2)),
+                          tmp_pos=cv(state.tmp_pos, (n, 3)), tmp_vel=cv(state.tmp_vel, (n, 3)),
+                          tmp_rhop=cv(state.tmp_rhop, (n, 2)),
+                          type=np.ascontiguousarray(state.type, np.int32), table=np.ascontiguousarray(state.table, np.int32))
+        L = gpu_lib()
+        h = self._host
+        self.h = L.gor_create(ctypes.byref(self.p), *[_p(h[k]) for k in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel",
+                                                                          "tmp_rhop", "type", "table")])
+        if not self.h:
+            raise RuntimeError("gor_create failed")
+        self.rigid = None
+
+    def _check(self, rc):
+        if rc != 0:
+            raise RuntimeError(gpu_lib().gor_error(self.h).decode())
+
+    def attach_rigid(self, first, count, mass, vel=(0, 0, 0), omega=(0, 0, 0), q=(1, 0, 0, 0)):
+        b, self._r0 = rigid_from(self.p, self._host, first, count, mass, vel, omega, q)
+        self._check(gpu_lib().gor_attach_rigid(self.h, ctypes.byref(b)))
+        self.rigid = b
+        return b
+
+    def step(self, nsteps=1):
+        self._check(gpu_lib().gor_step(self.h, int(nsteps)))
+
+    def download(self) -> dict:
+        n = self.p.ptc_num
+        out = dict(pos=np.empty((n, 3)), vel=np.empty((n, 3)), rhop=np.empty((n, 2)),
+                   type=np.empty(n, np.int32), table=np.empty(n, np.int32))
+        self._check(gpu_lib().gor_download(self.h, *[_p(out[k]) for k in ("pos", "vel", "rhop", "type", "table")]))
+        return out
+
+    def rigid_state(self) -> dict:
+        b = ORigid()
+        gpu_lib().gor_rigid(self.h, ctypes.byref(b))
+        return {k: np.array(getattr(b, k)[:]) for k in ("x", "v", "w", "q", "F", "T")}
+
+    def close(self):
+        if self.h:
+            gpu_lib().gor_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def set_threads(n: int) -> None:

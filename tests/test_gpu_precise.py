@@ -103,3 +103,113 @@ def test_floating_body_matches_fp64_oracle(precise):
     assert np.max(np.abs(heave - ref)) < 2e-3
     assert np.all(np.isfinite(s.download("old").vel))
     s.close()
+
+
+# ---- the FP64 GPU checker and the config[2] floating-body comparison --------
+
+def _state_of(d):
+    return {k: d[k] for k in ("pos", "vel", "rhop", "type", "table")}
+
+
+@pytest.mark.parametrize("body", [False, True])
+def test_gpu_fp64_checker_matches_cpu_fp64_oracle(body):
+    # the GPU instance of the FP64 oracle repeats the CPU oracle's arithmetic
+    c = cases.floating_body(0.04, end_step=1000) if body else cases.dam_break(0.04, end_step=100)
+    nsteps = 20
+    cpu = po.Oracle(c.json, _exact_state(c), dtype=np.float64)
+    gpu = po.GpuOracle64(c.json, _exact_state(c))
+    if body:
+        cpu.attach_rigid(c.body["first"], c.body["count"], c.body["mass"])
+        gpu.attach_rigid(c.body["first"], c.body["count"], c.body["mass"])
+        cpu.step_rigid(nsteps)
+    else:
+        cpu.step(nsteps)
+    gpu.step(nsteps)
+    g = gpu.download()
+    for k in ("type", "table"):
+        assert np.array_equal(g[k], cpu.old[k]), k
+    for k in ("pos", "vel", "rhop"):
+        d = float(np.max(np.abs(g[k] - cpu.old[k])))
+        assert d == 0.0, f"{k}: max |gpu - cpu| = {d}"
+    if body:
+        rc, rg = cpu.rigid_state(), gpu.rigid_state()
+        for k in ("x", "v", "w", "q"):
+            assert np.array_equal(rc[k], rg[k]), k
+    gpu.close()
+
+
+def _pitch(q):
+    """Rotation of the body about the y axis (rad) from its quaternion (w, x, y, z)."""
+    w, x, y, z = q
+    return float(np.arcsin(np.clip(2.0 * (w * y - z * x), -1.0, 1.0)))
+
+
+def _floating_body_comparison(dx, nsteps, every):
+    """The floating cube of config[2] (same tank, cube and drop) run by the
+    FP64 GPU checker and by the product in the plain FP32 form and in the
+    precision form; returns the final max and RMS errors against FP64 and the
+    heave and pitch trajectories."""
+    c = cases.floating_body(dx, end_step=nsteps)
+    first, count, mass = c.body["first"], c.body["count"], c.body["mass"]
+    ref = po.GpuOracle64(c.json, _exact_state(c))
+    ref.attach_rigid(first, count, mass)
+    runs = {"fp64": ref}
+    for precise in (False, True):
+        s = _solver(c, precise)
+        s.attach_body(first, count, mass)
+        runs["precision" if precise else "plain"] = s
+    traj = {k: {"heave": [], "pitch": []} for k in runs}
+    for _ in range(nsteps // every):
+        for k, r in runs.items():
+            if k == "fp64":
+                r.step(every)
+                b = r.rigid_state()
+                traj[k]["heave"].append(float(b["x"][2]))
+                traj[k]["pitch"].append(_pitch(b["q"]))
+            else:
+                r.run(every)
+                b = r.body()
+                traj[k]["heave"].append(float(b["pos"][2]))
+                traj[k]["pitch"].append(_pitch(b["q"]))
+    want = ref.download()
+    ids_w = want["table"] + np.arange(c.n)
+    out = {"particles": c.n, "steps": nsteps, "dx": dx}
+    for k in ("plain", "precision"):
+        s = runs[k]
+        st = s.download("old")
+        ids = st.table + np.arange(c.n)
+        got = {"pos": s.positions64() if k == "precision" else st.pos.astype(np.float64),
+               "vel": st.vel.astype(np.float64), "rho": st.rhop[:, 0].astype(np.float64)}
+        ref_by_id = {"pos": np.empty((c.n, 3)), "vel": np.empty((c.n, 3)), "rho": np.empty(c.n)}
+        ref_by_id["pos"][ids_w] = want["pos"]
+        ref_by_id["vel"][ids_w] = want["vel"]
+        ref_by_id["rho"][ids_w] = want["rhop"][:, 0]
+        fluid = np.zeros(c.n, bool)
+        fluid[ids[st.type == 1]] = True
+        e = {}
+        for q in ("pos", "vel", "rho"):
+            g = np.empty_like(ref_by_id[q])
+            g[ids] = got[q]
+            d = np.abs(g - ref_by_id[q])[fluid]
+            d = d.reshape(len(d), -1)
+            e[q] = {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d)))}
+        e["heave_max_diff"] = float(np.max(np.abs(np.array(traj[k]["heave"]) - np.array(traj["fp64"]["heave"]))))
+        e["pitch_max_diff"] = float(np.max(np.abs(np.array(traj[k]["pitch"]) - np.array(traj["fp64"]["pitch"]))))
+        out[k] = e
+        s.close()
+    out["heave_fp64"] = traj["fp64"]["heave"]
+    out["pitch_fp64"] = traj["fp64"]["pitch"]
+    ref.close()
+    return out
+
+
+def test_floating_body_against_fp64_checker():
+    # config[2]'s tank, cube and drop at dx = 0.02 over 500 steps; the full
+    # dx = 0.01 case over 5000 steps runs with ZSPH_FULL_CONFIG2=1
+    import json
+    import os
+    full = os.environ.get("ZSPH_FULL_CONFIG2") == "1"
+    r = _floating_body_comparison(0.01, 5000, 100) if full else _floating_body_comparison(0.02, 500, 50)
+    print("config2 comparison", json.dumps(r))
+    assert r["precision"]["pos"]["rms"] <= r["plain"]["pos"]["rms"]
+    assert r["precision"]["heave_max_diff"] < 2e-3 and r["plain"]["heave_max_diff"] < 2e-3
