@@ -34,7 +34,7 @@ struct DS {  // one particle buffer (reference layout, FP64)
 };
 
 struct DT {  // scratch of the step
-  double *acc, *dg, *rho_new, *p_new, *fv, *fvc, *ft;
+  double *acc, *dg, *rho_new, *p_new, *fv, *fvc;
   int *index, *hash, *gs, *ge, *flag;
 };
 
