@@ -8,12 +8,19 @@
 //
 // The reference sorts all 32 key bits with a generic radix sort.  Here the
 // keys are cell ids in [0, G), so a counting sort needs one histogram, one
-// scan over G cells and one scatter.  The scatter uses warp-aggregated
-// atomic tickets, which are not ordered across warps; stability (ties in
-// prior position order, the reference's sort_by_key contract) is restored
-// by ranking each particle among the members of its cell by original
-// position.  Cells with more than kBigSegment members are first sorted in
-// place by one CTA each.  The cell bounds are written from the scanned
+// scan over G cells and one scatter.  The scatter uses atomic tickets (one
+// atomic per run of equal keys in a warp), which are not ordered across
+// warps; stability (ties in prior position order, the reference's
+// sort_by_key contract) is restored by ranking each particle among the
+// members of its cell by original position.  Cells with more than
+// kBigSegment members are first sorted in place by one CTA each.
+//
+// The fused search of a sub-step is four launches: k_hash_count (hash, kill,
+// tickets, largest key), k_scan_onepass (decoupled look-back scan and cell
+// bounds), k_scatter_fused (scatter; crowded cells pre-sorted by its last
+// CTA) and k_rank_gather (rank and reorder).  The drop-in entry points
+// (zsph_sort_index, zsph_sort_data and the allocation-free sort) use the
+// two-kernel scan k_scan_reduce + k_scan_cells.  The cell bounds are written from the scanned
 // offsets in closed form, including the reference's end-of-array rules
 // (sort.cu:30-60): with lb(c) the number of particles whose key is below c,
 //   grid_start[c] = min(lb(c),   N-1)
