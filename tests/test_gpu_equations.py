@@ -159,3 +159,39 @@ def test_nan_input_is_reported():
     flags = sol.status()
     assert flags & z.FLAG_NAN
     sol.close()
+
+
+def test_long_runs_against_fp64_checker():
+    """config[0] (dx = 0.02, 105,048 particles) for its 2000 steps, and with
+    ZSPH_FULL_CONFIG1=1 config[1] (dx = 0.005, 4,221,468 particles) for its
+    500 steps: this build and the reference's own CUDA build, both FP32,
+    against the FP64 GPU checker of the same equations.  The stated FP32
+    tolerance: the max and RMS errors of position, velocity and density are
+    each at most twice the reference build's own."""
+    import json
+    import os
+    runs = [(cases.config0(), 2000)]
+    if os.environ.get("ZSPH_FULL_CONFIG1") == "1":
+        runs.append((cases.config1(), 500))
+    for c, nsteps in runs:
+        ref64 = po.GpuOracle64(c.json, c.state)
+        ref64.step(nsteps)
+        w = ref64.download()
+        ref64.close()
+        sol = z.Solver.from_case(c)
+        sol.run(nsteps)
+        assert sol.status() & z.FLAG_NAN == 0
+        g = sol.download("old")
+        sol.close()
+        r32, _, _ = po.ref_run(c.json, c.state, nsteps)
+        fluid = _by_id(np.asarray(w["type"]) == 1, w["table"])
+        report = {"case": c.name, "particles": c.n, "steps": nsteps}
+        for k, col in (("pos", slice(None)), ("vel", slice(None)), ("rhop", 0)):
+            v64 = _by_id(w[k], w["table"])[:, col]
+            ours = _by_id(getattr(g, k), g.table)[:, col].astype(np.float64)
+            refc = _by_id(r32[k], r32["table"])[:, col].astype(np.float64)
+            e_ours = err_norms(ours[fluid], v64[fluid])
+            e_ref = err_norms(refc[fluid], v64[fluid])
+            report[k] = {"ours_max": e_ours[0], "ours_rms": e_ours[1], "ref_max": e_ref[0], "ref_rms": e_ref[1]}
+            assert e_ours[0] <= 2 * e_ref[0] and e_ours[1] <= 2 * e_ref[1], (k, e_ours, e_ref)
+        print("long run vs FP64", json.dumps(report))
