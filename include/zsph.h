@@ -262,6 +262,20 @@ int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthr
 int zsph_writer_submit(zsph_writer_t* w, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int step, void* stream);
 int zsph_writer_destroy(zsph_writer_t* w);
 
+/* ---- the reference's driver program ---------------------------------------- */
+
+/* single_gpu_sph_src/deltasph/main.cu:8-147 on this library: reads the case
+ * (json_path, then input_path/input.vtk as read_vkt.cu:5 does), selects
+ * gpu_id, runs steps start_step .. end_step-1 and writes
+ * output_path/zsph<i>.vtk every output_step through the writer pool.
+ * ZSPH_COMPAT_SEPARATE issues the reference's twelve launches per step
+ * (main.cu:63-88) through the drop-in entry points; ZSPH_COMPAT_FUSED one
+ * zsph_step per step.  *steps_done (may be NULL) receives the number of steps
+ * completed.  Nothing is printed; errors are statuses with the message in
+ * zsph_last_error(NULL, ...). */
+enum { ZSPH_COMPAT_SEPARATE = 0, ZSPH_COMPAT_FUSED = 1 };
+int zsph_compat_run(const char* json_path, int mode, int* steps_done);
+
 /* ---- Learned-corrector network (no reference counterpart) -----------------
  * A per-particle MLP 32 -> 128 -> 128 -> 4 with SiLU, bf16 weights and fp32
  * accumulation on the fifth-generation tensor cores.  Its fp32 master

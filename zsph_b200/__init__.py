@@ -145,6 +145,7 @@ def _as_dict(s: ctypes.Structure) -> dict:
 _HP = ctypes.c_void_p
 _sig = {
     "zsph_read_json": (_I, [ctypes.c_char_p, ctypes.POINTER(JsonCase), ctypes.c_char_p, _I]),
+    "zsph_compat_run": (_I, [ctypes.c_char_p, _I, _IP]),
     "zsph_set_cpu_param": (_I, [ctypes.POINTER(CpuParam), ctypes.POINTER(JsonCase)]),
     "zsph_set_gpu_param": (_I, [ctypes.POINTER(GpuParam), ctypes.POINTER(CpuParam)]),
     "zsph_check_dt": (_I, [ctypes.POINTER(CpuParam), _FP]),
@@ -258,6 +259,17 @@ def check(rc: int, handle=None) -> None:
 
 def _ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+COMPAT_SEPARATE, COMPAT_FUSED = 0, 1
+
+
+def compat_run(json_path: str, mode: int = COMPAT_SEPARATE) -> int:
+    """zsph_compat_run: the reference's driver program (deltasph/main.cu) on
+    this library; returns the number of steps run."""
+    steps = ctypes.c_int(0)
+    check(lib.zsph_compat_run(json_path.encode(), int(mode), ctypes.byref(steps)))
+    return steps.value
 
 
 def read_json(path: str) -> JsonCase:

@@ -1,0 +1,140 @@
+// zsph_compat_run: the reference's driver program on this library's C ABI.
+//
+// Restates single_gpu_sph_src/deltasph/main.cu:8-147 step for step with the
+// public entry points, so a reference case directory runs unchanged:
+//   read_json            -> zsph_read_json(json_path)
+//   set_cpu_param        -> zsph_set_cpu_param (includes check_dt, init.cu:218)
+//   read_vtk             -> zsph_read_vtk(input_path + "/input.vtk")  (read_vkt.cu:5)
+//   cudaSetDevice(gpu_id)
+//   set_gpu_param, alloc_gpu_*, cpu_to_gpu
+//   mul_thread_creat     -> zsph_writer_create(output_path, thread_num writers)
+//   step loop            -> the twelve launches of main.cu:63-88 through the
+//                           drop-in entry points (ZSPH_COMPAT_SEPARATE), or one
+//                           zsph_step per step (ZSPH_COMPAT_FUSED)
+//   output every output_step -> zsph_writer_submit (output_path/zsph<i>.vtk)
+// Differences: no per-step console output and no exit(): every failure is a
+// ZSPH_* status with its message in zsph_last_error(NULL, ...).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "zsph_internal.cuh"
+
+namespace {
+
+int fail(int code, const std::string& m) {
+  zsph::record_library_error("zsph_compat_run: " + m);
+  return code;
+}
+
+std::string last_error(zsph_handle_t* h) {
+  char b[512];
+  zsph_last_error(h, b, (int)sizeof b);
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
+  if (steps_done) *steps_done = 0;
+  if (!json_path) return fail(ZSPH_EINVAL, "null json path");
+  if (mode != ZSPH_COMPAT_SEPARATE && mode != ZSPH_COMPAT_FUSED) return fail(ZSPH_EINVAL, "unknown mode");
+  zsph_json_t j;
+  char err[256] = {0};
+  int rc = zsph_read_json(json_path, &j, err, (int)sizeof err);
+  if (rc) return fail(rc, std::string("read_json: ") + err);
+  zsph_cpu_param_t cp;
+  rc = zsph_set_cpu_param(&cp, &j);
+  if (rc) return fail(rc, "set_cpu_param: " + last_error(nullptr));
+  const int n = cp.ptc_num;
+  std::vector<float> pos(3 * (size_t)n), vel(3 * (size_t)n), rhop(2 * (size_t)n), acc(4 * (size_t)n);
+  std::vector<int> type((size_t)n), table((size_t)n);
+  const std::string input = std::string(cp.input_path) + "/input.vtk";
+  rc = zsph_read_vtk(input.c_str(), n, cp.rho0, 0, pos.data(), vel.data(), rhop.data(), acc.data(), type.data(),
+                     table.data());
+  if (rc) return fail(rc, "read_vtk: " + last_error(nullptr));
+  cudaError_t ce = cudaSetDevice(cp.gpu_id);
+  if (ce) return fail(ZSPH_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(ce));
+  zsph_gpu_param_t gp;
+  rc = zsph_set_gpu_param(&gp, &cp);
+  if (rc) return fail(rc, "set_gpu_param: " + last_error(nullptr));
+
+  zsph_ptc_t o{}, w{};
+  zsph_tmp_t t{};
+  zsph_handle_t* h = nullptr;
+  zsph_writer_t* wr = nullptr;
+  cudaStream_t st = nullptr;
+  int done = 0;
+  std::string what;
+  rc = zsph_alloc_ptc(&o, n);
+  if (!rc) rc = zsph_alloc_ptc(&w, n);
+  if (!rc) rc = zsph_alloc_tmp(&t, n, cp.grid_num);
+  if (!rc) rc = zsph_cpu_to_gpu(&o, &t, pos.data(), vel.data(), rhop.data(), type.data(), table.data(), acc.data(),
+                                n, nullptr);
+  if (rc) what = "device buffers: " + last_error(nullptr);
+  if (!rc && (ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)) != cudaSuccess) {
+    rc = ZSPH_ECUDA;
+    what = std::string("stream: ") + cudaGetErrorString(ce);
+  }
+  if (!rc) {
+    rc = zsph_create(&gp, cp.grid_num, &h);
+    if (rc) what = "create: " + last_error(nullptr);
+  }
+  if (!rc) {
+    rc = zsph_writer_create(cp.output_path, n, ZSPH_OUT_REFERENCE, cp.thread_num > 0 ? cp.thread_num : 1, &wr);
+    if (rc) what = "writer: " + last_error(nullptr);
+  }
+  void* s = st;
+  for (int i = cp.start_step; !rc && i < cp.end_step; ++i) {
+    if (mode == ZSPH_COMPAT_FUSED) {
+      rc = zsph_step(h, &o, &w, &t, s);
+    } else {  // main.cu:63-88
+      rc = zsph_hash(h, &o, &t, s);
+      if (!rc) rc = zsph_sort_index(h, &t, s);
+      if (!rc) rc = zsph_sort_data(h, &o, &w, &t, s);
+      if (!rc) rc = zsph_boundary(h, &w, &t, s);
+      if (!rc) rc = zsph_governing(h, &w, &t, s);
+      if (!rc) rc = zsph_prediction(h, &w, &t, s);
+      if (!rc) rc = zsph_hash(h, &w, &t, s);
+      if (!rc) rc = zsph_sort_index(h, &t, s);
+      if (!rc) rc = zsph_sort_data(h, &w, &o, &t, s);
+      if (!rc) rc = zsph_boundary(h, &o, &t, s);
+      if (!rc) rc = zsph_governing(h, &o, &t, s);
+      if (!rc) rc = zsph_correction(h, &o, &t, s);
+    }
+    if (rc) {
+      what = "step " + std::to_string(i) + ": " + last_error(h);
+      break;
+    }
+    if (cp.output_step > 0 && i % cp.output_step == 0) {  // main.cu:95-124
+      rc = zsph_writer_submit(wr, &o, &t, i, s);
+      if (rc) what = "output: " + last_error(nullptr);
+    }
+    ++done;
+  }
+  if (!rc && h) {
+    int flags = 0;
+    rc = zsph_status(h, &flags, 0);
+    if (rc) what = "status: " + last_error(h);
+  }
+  if (wr) {
+    const int wrc = zsph_writer_destroy(wr);  // writes the pending files
+    if (!rc && wrc) {
+      rc = wrc;
+      what = "writer: " + last_error(nullptr);
+    }
+  }
+  if (h) zsph_destroy(h);
+  if (st) cudaStreamDestroy(st);
+  zsph_free_ptc(&o);
+  zsph_free_ptc(&w);
+  zsph_free_tmp(&t);
+  if (steps_done) *steps_done = done;
+  return rc ? fail(rc, what) : ZSPH_OK;
+}
+
+}  // extern "C"
