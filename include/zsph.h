@@ -270,10 +270,12 @@ int zsph_writer_destroy(zsph_writer_t* w);
  * output_path/zsph<i>.vtk every output_step through the writer pool.
  * ZSPH_COMPAT_SEPARATE issues the reference's twelve launches per step
  * (main.cu:63-88) through the drop-in entry points; ZSPH_COMPAT_FUSED one
- * zsph_step per step.  *steps_done (may be NULL) receives the number of steps
+ * zsph_step per step.  Or-ing ZSPH_COMPAT_SIMPLE selects the simple-SPH
+ * equations (the reference's simplesph program: the same main.cu linked with
+ * equation/simple_ns.cu).  *steps_done (may be NULL) receives the number of steps
  * completed.  Nothing is printed; errors are statuses with the message in
  * zsph_last_error(NULL, ...). */
-enum { ZSPH_COMPAT_SEPARATE = 0, ZSPH_COMPAT_FUSED = 1 };
+enum { ZSPH_COMPAT_SEPARATE = 0, ZSPH_COMPAT_FUSED = 1, ZSPH_COMPAT_SIMPLE = 2 };
 int zsph_compat_run(const char* json_path, int mode, int* steps_done);
 
 /* ---- Learned-corrector network (no reference counterpart) -----------------

@@ -46,7 +46,8 @@ def _write_case(root, c, end_step, output_step):
     return path, out
 
 
-@pytest.mark.parametrize("mode", [z.COMPAT_SEPARATE, z.COMPAT_FUSED])
+@pytest.mark.parametrize("mode", [z.COMPAT_SEPARATE, z.COMPAT_FUSED, z.COMPAT_SEPARATE | z.COMPAT_SIMPLE,
+                                  z.COMPAT_FUSED | z.COMPAT_SIMPLE])
 def test_compat_run_matches_solver(tmp_path, mode):
     c = cases.small(0.04)
     nsteps, every = 12, 5
@@ -56,6 +57,8 @@ def test_compat_run_matches_solver(tmp_path, mode):
     assert names == sorted(f"zsph{i}.vtk" for i in range(0, nsteps, every)), names
     # output at i = 10 holds the state after 11 steps
     sol = z.Solver.from_case(c)
+    if mode & z.COMPAT_SIMPLE:
+        sol.set_equations(z.EQ_SIMPLE)
     sol.run(11)
     want = sol.download("old")
     sol.close()

@@ -261,7 +261,7 @@ def _ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
 
 
-COMPAT_SEPARATE, COMPAT_FUSED = 0, 1
+COMPAT_SEPARATE, COMPAT_FUSED, COMPAT_SIMPLE = 0, 1, 2
 
 
 def compat_run(json_path: str, mode: int = COMPAT_SEPARATE) -> int:

@@ -12,6 +12,8 @@
 //                           drop-in entry points (ZSPH_COMPAT_SEPARATE), or one
 //                           zsph_step per step (ZSPH_COMPAT_FUSED)
 //   output every output_step -> zsph_writer_submit (output_path/zsph<i>.vtk)
+// The reference's simplesph program is the same driver linked with
+// equation/simple_ns.cu; ZSPH_COMPAT_SIMPLE selects those equations.
 // Differences: no per-step console output and no exit(): every failure is a
 // ZSPH_* status with its message in zsph_last_error(NULL, ...).
 #include <cuda_runtime.h>
@@ -42,6 +44,8 @@ extern "C" {
 int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
   if (steps_done) *steps_done = 0;
   if (!json_path) return fail(ZSPH_EINVAL, "null json path");
+  const bool simple = (mode & ZSPH_COMPAT_SIMPLE) != 0;
+  mode &= ~ZSPH_COMPAT_SIMPLE;
   if (mode != ZSPH_COMPAT_SEPARATE && mode != ZSPH_COMPAT_FUSED) return fail(ZSPH_EINVAL, "unknown mode");
   zsph_json_t j;
   char err[256] = {0};
@@ -83,6 +87,10 @@ int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
   if (!rc) {
     rc = zsph_create(&gp, cp.grid_num, &h);
     if (rc) what = "create: " + last_error(nullptr);
+  }
+  if (!rc && simple) {
+    rc = zsph_set_equations(h, ZSPH_EQ_SIMPLE);
+    if (rc) what = "set_equations: " + last_error(h);
   }
   if (!rc) {
     rc = zsph_writer_create(cp.output_path, n, ZSPH_OUT_REFERENCE, cp.thread_num > 0 ? cp.thread_num : 1, &wr);

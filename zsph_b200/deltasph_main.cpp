@@ -1,9 +1,10 @@
 // zsph_deltasph: the reference's deltasph program (single_gpu_sph_src/deltasph/
-// main.cu) on this library.  Usage: zsph_deltasph [case.json] [--fused]
+// main.cu) on this library.  Usage: zsph_deltasph [case.json] [--fused] [--simple]
 // The case file defaults to ../input/input.json, as the reference's does; the
 // initial particles are read from <input_path>/input.vtk and the outputs go to
 // <output_path>/zsph<step>.vtk.  --fused runs one fused step per step instead
-// of the reference's twelve launches.
+// of the reference's twelve launches; --simple runs the simple-SPH equations
+// (the reference's simplesph program).
 #include <cstdio>
 #include <cstring>
 
@@ -13,7 +14,8 @@ int main(int argc, char** argv) {
   const char* path = "../input/input.json";
   int mode = ZSPH_COMPAT_SEPARATE;
   for (int a = 1; a < argc; ++a) {
-    if (std::strcmp(argv[a], "--fused") == 0) mode = ZSPH_COMPAT_FUSED;
+    if (std::strcmp(argv[a], "--fused") == 0) mode |= ZSPH_COMPAT_FUSED;
+    else if (std::strcmp(argv[a], "--simple") == 0) mode |= ZSPH_COMPAT_SIMPLE;
     else path = argv[a];
   }
   int steps = 0;
