@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-corrector leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form leg")
     ap.add_argument("--learn-epochs", type=int, default=20)
+    ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of zsph_autotune's")
     return ap.parse_args()
 
 
@@ -383,6 +384,9 @@ def run_ours(args, dist: Dist):
     sptr = ctypes.c_void_p(stream.cuda_stream)
     K, W = args.steps, args.warmup
 
+    # launch shapes from the project's autotuner (untimed; it restores the state after every trial)
+    tune = None if args.no_tune else sol.autotune(3, sptr)
+
     # warm-up (captures the CUDA graph), then K steps timed with CUDA events
     with torch.cuda.stream(stream):
         sol.run(W, sptr)
@@ -483,6 +487,7 @@ def run_ours(args, dist: Dist):
                    "l2": "inputs larger than L2 (particle state 0.76 GB + scratch per step)",
                    "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
+        "tune": tune,
         "roofline": roofline, "dominant_kernel": dominant, "pair_kernels": pair, "kernels": kern, "cpu_baseline": cpu,
         "learned": learned, "batched": batched, "status_flags": flags,
     }
