@@ -120,7 +120,7 @@ int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
 
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
-                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.pr, s.sh.vp};
+                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.rec};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   std::memset(&s, 0, sizeof s);
@@ -297,8 +297,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.nb, (size_t)kMaxNb * ((n + 31) & ~(size_t)31));  // whole 32-particle list groups
   if (!e) e = dalloc(s.nb_cnt, n);
   if (!e) e = dalloc(s.flags, 1);
-  if (!e) e = dalloc(s.sh.pr, n);
-  if (!e) e = dalloc(s.sh.vp, n);
+  if (!e) e = dalloc(s.sh.rec, 2 * (size_t)n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
   if (!e) e = cudaMemset(s.misc, 0, 8 * sizeof(int));
   if (!e) e = cudaMemset(s.tile_state, 0, (size_t)h->tiles * sizeof(unsigned long long));

@@ -20,7 +20,12 @@
 //    stored blocked by 32-particle groups (nb_vec) and read 8 per 16-byte load.
 //  * k_boundary and k_governing walk their particle's list with one thread
 //    per particle, all lanes converged, loading the next four neighbours'
-//    packed data before doing their arithmetic.  k_boundary folds the
+//    packed data before doing their arithmetic: one 256-bit load of the
+//    neighbour's 32-byte shadow record (position, density, velocity,
+//    pressure), plus its grad(rho) in k_governing.  The walk is bound by the
+//    L1 data pipe (the 32 lanes' k-th neighbours spread over ~12 lines), so
+//    one wide request per neighbour costs fewer L1 wavefronts than two
+//    16-byte ones.  k_boundary folds the
 //    reference's second loop into its first walk.  The visit order is the
 //    reference's, so the order-dependent recurrence on grad(rho).x
 //    (delta_ns.cu:244-245) sees the same sequence.
@@ -29,9 +34,10 @@
 //    results agree with the reference to FP32 rounding, not bitwise.
 //
 // Neighbour test: the reference's q = sqrtf(r2)/h <= 2 (delta_ns.cu:67-68),
-// with r2 formed as fma(dz,dz,fma(dy,dy,dx*dx)).  Far from the threshold the
-// test is decided on r2 alone; within a relative 1e-5 of it the exact
-// IEEE sqrt and division decide, so the neighbour set is the reference's.
+// with r2 formed as fma(dz,dz,fma(dy,dy,dx*dx)).  IEEE sqrt and division
+// are monotone, so the test holds exactly for r2 <= r2max, the largest float
+// that passes it (found on the host with the same float operations): one
+// compare gives the reference's neighbour set.
 //
 // Particle type: only "fluid (type 1)" vs "not fluid" enters the equations,
 // so the packed shadow stores the density with the sign bit set for
@@ -161,7 +167,7 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
     const int a = rs[r * kPairBlock], b = re[r * kPairBlock];
     for (int j = a; j < b; ++j) {
       if (j == i) continue;
-      const float4 pj = s.sh.pr[j];
+      const float4 pj = s.sh.pr(j);
       if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) use(fetch(fb[r * kPairBlock] + (j - a)));
     }
   }
@@ -201,13 +207,14 @@ __device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, uint32_t p
 constexpr int kWaitPolls = 1 << 22;  // bounded wait on the window barrier (each poll suspends briefly)
 
 // Computes the window of the CTA's particles over the rows selected by ROWS
-// (ROWS(r) true), copies NARR packed float4 arrays into `win` (array a at
-// win + a*cap) and rewrites fb (per-thread row bases) to shared indices.
+// (ROWS(r) true), copies NARR packed arrays, whose elements are wid[a]
+// float4s wide, into `win` (array a at win + cap * (wid[0] + .. + wid[a-1]))
+// and rewrites fb (per-thread row bases) to shared indices.
 // Returns false (and leaves fb = rs) when the window does not fit `cap`
 // candidates or the copies did not complete in time.
 template <int NR, int NARR, class RowSel>
-__device__ bool stage_window(WinHdr& wh, float4* win, int cap, const float4* const (&src)[NARR], bool act,
-                             const int* rs, const int* re, int* fb, int* flags, RowSel rows) {
+__device__ bool stage_window(WinHdr& wh, float4* win, int cap, const float4* const (&src)[NARR],
+                             const int (&wid)[NARR], bool act, const int* rs, const int* re, int* fb, int* flags, RowSel rows) {
   const int tid = threadIdx.x;
   if (tid < NR) {
     wh.w0[tid] = 0x7fffffff;
@@ -243,14 +250,22 @@ __device__ bool stage_window(WinHdr& wh, float4* win, int cap, const float4* con
   __syncthreads();
   if (!wh.staged) return false;
   if (tid == 0) {
+    int wsum = 0;
+#pragma unroll
+    for (int a = 0; a < NARR; ++a) wsum += wid[a];
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&wh.bar)),
-                 "r"((uint32_t)(wh.total * NARR * 16))
+                 "r"((uint32_t)(wh.total * wsum * 16))
                  : "memory");
     for (int r = 0; r < NR; ++r)
-      if (wh.len[r] > 0)
+      if (wh.len[r] > 0) {
+        int base = 0;
 #pragma unroll
-        for (int a = 0; a < NARR; ++a)
-          bulk_copy(win + (size_t)a * cap + wh.woff[r], src[a] + wh.w0[r], (uint32_t)(wh.len[r] * 16), &wh.bar);
+        for (int a = 0; a < NARR; ++a) {
+          bulk_copy(win + (size_t)base * cap + (size_t)wh.woff[r] * wid[a], src[a] + (size_t)wh.w0[r] * wid[a],
+                    (uint32_t)(wh.len[r] * wid[a] * 16), &wh.bar);
+          base += wid[a];
+        }
+      }
   }
   if (act) {
 #pragma unroll
@@ -285,8 +300,15 @@ __device__ __forceinline__ float4 shifted(const KParams& kp, float4 pj, int cj, 
 }
 template <bool PRECISE>
 __device__ __forceinline__ float4 shadow_pr(const KParams& kp, const Scratch& s, int j, int3 ci) {
-  const float4 pj = s.sh.pr[j];
+  const float4 pj = s.sh.pr(j);
   return PRECISE ? shifted(kp, pj, kp.c3n[j], ci) : pj;
+}
+// Neighbour j's whole record (one 256-bit load), positions as shadow_pr.
+template <bool PRECISE>
+__device__ __forceinline__ ShadowRec shadow_rec(const KParams& kp, const Scratch& s, int j, int3 ci) {
+  ShadowRec r = s.sh.load(j);
+  if (PRECISE) r.pr = shifted(kp, r.pr, kp.c3n[j], ci);
+  return r;
 }
 
 // Wall pressure contribution of fluid neighbour j of wall particle i
@@ -303,7 +325,7 @@ __device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, f
   float w = aa * aa * aa;
   w = w * aa;
   w *= (2.0f * q + 1.0f) * p.adh;
-  const float p1 = s.sh.vp[j].w;
+  const float p1 = s.sh.vp(j).w;
   rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
   wsum += w;
 }
@@ -371,7 +393,7 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   const int c = act ? t.hash[i] : INT_MAX;  // sorted: non-decreasing over the lanes
   // batched form: the scene of the lane's cell (scenes own disjoint cell ranges)
   const int scn = BATCH && act ? scene_of(kp_arg.scene_cbase, kp_arg.nscenes, c) : 0;
-  const float4 pi = s.sh.pr[act ? i : p0];
+  const float4 pi = s.sh.pr(act ? i : p0);
   // precision form: the lane's own cell (its position is the offset from that cell's corner)
   const int3 ci = PRECISE && act ? unpack_cell(kp_arg.c3n[i]) : int3{0, 0, 0};
   u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
@@ -514,8 +536,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
     const zsph_gpu_param_t& p = kp.p;
     if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
     if (rsum < 0.0f) rsum = 0.0f;
-    s.sh.pr[i].w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-    s.sh.vp[i].w = rsum;
+    s.sh.pr(i).w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+    s.sh.vp(i).w = rsum;
   }
   if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
@@ -568,14 +590,14 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
   bool staged = false;
   if (GF == 1 && kp.stage_windows && !PRECISE) {
-    const float4* const src[2] = {s.sh.pr, s.sh.vp};
-    staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapB, src, act, sm.rs, sm.re, sm.fb, s.flags,
-                                             [](int r) { return Stencil<GF>::boundary_row(r); });
+    const float4* const src[1] = {s.sh.rec};  // 32-byte records: two float4s per candidate
+    staged = stage_window<Stencil<GF>::NR, 1>(*sm.wh, sm.win, kWinCapB, src, {2}, act, sm.rs, sm.re, sm.fb,
+                                              s.flags, [](int r) { return Stencil<GF>::boundary_row(r); });
   }
   if (!act) return;
   const zsph_gpu_param_t& p = kp.p;
-  const float4 pi = s.sh.pr[i];
-  const float4 vi = s.sh.vp[i];
+  const ShadowRec own = s.sh.load(i);
+  const float4 pi = own.pr, vi = own.vp;
   const bool fi = fluid_of(pi.w);
   const float rho_self = reinterpret_cast<const float2*>(ptc.rhop)[i].x;  // old own density
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
@@ -605,10 +627,13 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   const float4* win = sm.win;
   if (staged)
     walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
-                         [&](int q) { return NbB1{win[q], win[kWinCapB + q]}; }, use1);
+                         [&](int q) { return NbB1{win[2 * q], win[2 * q + 1]}; }, use1);
   else
     walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
-                         [&](int q) { return NbB1{shadow_pr<PRECISE>(kp, s, q, ci), s.sh.vp[q]}; }, use1);
+                         [&](int q) {
+                           const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+                           return NbB1{r.pr, r.vp};
+                         }, use1);
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
                     Lxy * Lxy * Lzz;
@@ -680,14 +705,14 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
   const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
   bool staged = false;
   if (GF == 1 && kp.stage_windows && !PRECISE) {
-    const float4* const src[3] = {s.sh.pr, s.sh.vp, dg};
-    staged = stage_window<Stencil<GF>::NR, 3>(*sm.wh, sm.win, kWinCapG, src, act, sm.rs, sm.re, sm.fb, s.flags,
-                                             [](int) { return true; });
+    const float4* const src[2] = {s.sh.rec, dg};  // 32-byte records, then grad(rho)
+    staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapG, src, {2, 1}, act, sm.rs, sm.re, sm.fb,
+                                              s.flags, [](int) { return true; });
   }
   if (!act) return;
   const zsph_gpu_param_t& p = kp.p;
-  const float4 pi = s.sh.pr[i];
-  const float4 vi = s.sh.vp[i];
+  const ShadowRec own = s.sh.load(i);
+  const float4 pi = own.pr, vi = own.vp;
   const bool fi = fluid_of(pi.w);
   const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
   const float inv_h = kp.inv_h, c_fr = kp.c_fr, m = p.m;
@@ -746,10 +771,13 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
   const float4* win = sm.win;
   if (staged)
     walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
-                         [&](int q) { return NbG{win[q], win[kWinCapG + q], win[2 * kWinCapG + q]}; }, use);
+                         [&](int q) { return NbG{win[2 * q], win[2 * q + 1], win[2 * kWinCapG + q]}; }, use);
   else
     walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
-                         [&](int q) { return NbG{shadow_pr<PRECISE>(kp, s, q, ci), s.sh.vp[q], dg[q]}; }, use);
+                         [&](int q) {
+                           const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+                           return NbG{r.pr, r.vp, dg[q]};
+                         }, use);
   if (rig) kp.rigid_f[i] = make_float4(rf.x, rf.y, rf.z, 0.f);
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
@@ -819,13 +847,16 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary_simple(KParams kp, Scra
   if (i >= kp.n) return;
   load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const zsph_gpu_param_t& p = kp.p;
-  const float4 pi = s.sh.pr[i];
-  const float4 vi = s.sh.vp[i];
+  const ShadowRec own = s.sh.load(i);
+  const float4 pi = own.pr, vi = own.vp;
   const bool fi = fluid_of(pi.w);
   float divv = 0.f;
   if (fi)
     walk<GF, true, NbB1>(
-        kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return NbB1{s.sh.pr[q], s.sh.vp[q]}; },
+        kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) {
+          const ShadowRec r = s.sh.load(q);
+          return NbB1{r.pr, r.vp};
+        },
         [&](const NbB1& nb) {
           if (!fluid_of(nb.pr.w)) return;
           const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
@@ -850,14 +881,17 @@ __global__ void __launch_bounds__(kPairBlock) k_governing_simple(KParams kp, Scr
   if (i >= kp.n) return;
   load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const zsph_gpu_param_t& p = kp.p;
-  const float4 pi = s.sh.pr[i];
-  const float4 vi = s.sh.vp[i];
+  const ShadowRec own = s.sh.load(i);
+  const float4 pi = own.pr, vi = own.vp;
   const bool fi = fluid_of(pi.w);
   const float r0 = fabsf(pi.w), p0 = vi.w, ir0 = rcp_fast(r0);
   const float d0 = t.dofv[i];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   walk<GF, false, NbS>(
-      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) { return NbS{s.sh.pr[q], s.sh.vp[q], t.dofv[q]}; },
+      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) {
+        const ShadowRec r = s.sh.load(q);
+        return NbS{r.pr, r.vp, t.dofv[q]};
+      },
       [&](const NbS& nb) {
         const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
         const float rr2 = dist2(dx, dy, dz);

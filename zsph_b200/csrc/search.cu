@@ -642,8 +642,7 @@ __device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t
   reinterpret_cast<float2*>(w.tmp_rhop)[dst] = trp;
   w.type[dst] = ty_;
   w.table[dst] = tb + src - dst;  // sort.cu:82
-  sh.pr[dst] = make_float4(x, y, z, packed_rho(rp.x, ty_));
-  sh.vp[dst] = make_float4(vx, vy, vz, rp.y);
+  st_rec(&sh.pr(dst), make_float4(x, y, z, packed_rho(rp.x, ty_)), make_float4(vx, vy, vz, rp.y));
 }
 
 // One particle's record of the eight reference arrays (72 bytes).
@@ -675,8 +674,8 @@ __device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const Shadow& sh,
   reinterpret_cast<float2*>(w.tmp_rhop)[dst] = r.trp;
   w.type[dst] = r.type;
   w.table[dst] = r.table + src - dst;  // sort.cu:82
-  sh.pr[dst] = make_float4(r.x, r.y, r.z, packed_rho(r.rp.x, r.type));
-  sh.vp[dst] = make_float4(r.vx, r.vy, r.vz, r.rp.y);
+  st_rec(&sh.pr(dst), make_float4(r.x, r.y, r.z, packed_rho(r.rp.x, r.type)),
+         make_float4(r.vx, r.vy, r.vz, r.rp.y));
 }
 
 // Fused search, last step: rank, write sorted hash/index, gather the eight
@@ -738,8 +737,8 @@ __global__ void __launch_bounds__(kSearchBlock) k_pack(KParams kp, Shadow sh, zs
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kp.n) return;
   const float2 rp = reinterpret_cast<const float2*>(s.rhop)[i];
-  sh.pr[i] = make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], packed_rho(rp.x, s.type[i]));
-  sh.vp[i] = make_float4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], rp.y);
+  st_rec(&sh.pr(i), make_float4(s.pos[3 * i], s.pos[3 * i + 1], s.pos[3 * i + 2], packed_rho(rp.x, s.type[i])),
+         make_float4(s.vel[3 * i], s.vel[3 * i + 1], s.vel[3 * i + 2], rp.y));
 }
 
 inline int blocks_for(int n, int b) { return (n + b - 1) / b; }

@@ -103,12 +103,38 @@ __host__ __device__ __forceinline__ int3 unpack_cell(int c) {
   return make_int3(c & kCellMask, (c >> kCellBits) & kCellMask, (c >> (2 * kCellBits)) & kCellMask);
 }
 
-// Packed per-particle shadows of the sorted state, written by the gather
-// (16-byte loads in the pair kernels).  pr = {x, y, z, +-rho} with the sign
-// bit set for non-fluid particles (type != 1), vp = {vx, vy, vz, p}.
+// 256-bit global load / store of one 32-byte record (sm_100 v8 vector
+// access; the address must be 32-byte aligned).
+__device__ __forceinline__ void ld_rec(const float4* p, float4& a, float4& b) {
+  asm("ld.global.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(a.x), "=f"(a.y), "=f"(a.z), "=f"(a.w), "=f"(b.x), "=f"(b.y), "=f"(b.z), "=f"(b.w)
+      : "l"(p));
+}
+__device__ __forceinline__ void st_rec(float4* p, float4 a, float4 b) {
+  asm volatile("st.global.v8.f32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(p), "f"(a.x), "f"(a.y), "f"(a.z),
+               "f"(a.w), "f"(b.x), "f"(b.y), "f"(b.z), "f"(b.w)
+               : "memory");
+}
+
+struct ShadowRec {
+  float4 pr, vp;
+};
+
+// Packed per-particle shadows of the sorted state, written by the gather:
+// one 32-byte record per particle, rec[2i] = pr = {x, y, z, +-rho} with the
+// sign bit set for non-fluid particles (type != 1) and rec[2i+1] = vp =
+// {vx, vy, vz, p}, so that a pair kernel fetches a neighbour's record with
+// one 256-bit load instead of two 16-byte loads.  rec comes from cudaMalloc
+// (256-byte aligned), so every record is 32-byte aligned.
 struct Shadow {
-  float4* pr;
-  float4* vp;
+  float4* rec;  // [2n]
+  __device__ __forceinline__ float4& pr(int i) const { return rec[2 * i]; }
+  __device__ __forceinline__ float4& vp(int i) const { return rec[2 * i + 1]; }
+  __device__ __forceinline__ ShadowRec load(int i) const {
+    ShadowRec r;
+    ld_rec(rec + 2 * i, r.pr, r.vp);
+    return r;
+  }
 };
 
 // Device scratch owned by a handle; allocated once in zsph_create.
