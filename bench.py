@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form leg")
     ap.add_argument("--learn-epochs", type=int, default=20)
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of zsph_autotune's")
+    ap.add_argument("--shapes", default=None, metavar="CW,MINB,SPG",
+                    help="apply these launch shapes (zsph_set_launch_shapes) instead of running zsph_autotune")
     return ap.parse_args()
 
 
@@ -385,7 +387,12 @@ def run_ours(args, dist: Dist):
     K, W = args.steps, args.warmup
 
     # launch shapes from the project's autotuner (untimed; it restores the state after every trial)
-    tune = None if args.no_tune else sol.autotune(3, sptr)
+    if args.shapes:
+        cw, mb, spg = (int(v) for v in args.shapes.split(","))
+        sol.set_launch_shapes(cw, mb, spg)
+        tune = {"list_cells_per_cta": cw, "governing_min_ctas": mb, "steps_per_graph": spg, "applied": True}
+    else:
+        tune = None if args.no_tune else sol.autotune(3, sptr)
 
     # warm-up (captures the CUDA graph), then K steps timed with CUDA events
     with torch.cuda.stream(stream):

@@ -422,6 +422,12 @@ typedef struct {
 } zsph_tune_t;
 int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
                   int trial_steps, zsph_tune_t* out, void* stream);
+/* Applies launch shapes chosen earlier (a zsph_autotune result kept by the
+ * caller, e.g. across restarts of the same case) without timing anything:
+ * list_cells_per_cta, governing_min_ctas and steps_per_graph from the
+ * candidate sets above, 0 for each one's default; the time fields are
+ * ignored.  ZSPH_EINVAL for any other value. */
+int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes);
 
 /* ---- Precision form (no reference counterpart) ----------------------------
  * zsph_set_precision(h, 1): a particle's position is held as its integer grid

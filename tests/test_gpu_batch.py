@@ -72,3 +72,23 @@ def test_autotune_batch(scenes):
     bt.run(5)
     assert bt.status() == 0
     bt.close()
+
+
+def test_set_launch_shapes_applies_every_candidate_bit_identically(scenes):
+    c = scenes[1]
+    ref = z.Solver.from_case(c)
+    ref.run(6)
+    want = ref.download("old")
+    ref.close()
+    for cw, mb, spg in ((2, 1, 4), (4, 8, 1), (2, 6, 4), (0, 0, 0)):
+        s = z.Solver.from_case(c)
+        s.set_launch_shapes(cw, mb, spg)
+        s.run(6)
+        got = s.download("old")
+        assert s.status() == 0
+        for k in ("pos", "vel", "rhop", "type", "table"):
+            assert np.array_equal(getattr(got, k), getattr(want, k)), (cw, mb, spg, k)
+        for bad in ((3, 0, 0), (0, 5, 0), (0, 0, 2), (-1, 0, 0)):
+            with pytest.raises(z.ZsphError):
+                s.set_launch_shapes(*bad)
+        s.close()

@@ -217,6 +217,7 @@ _sig = {
     "zsph_create_batch": (_I, [ctypes.POINTER(GpuParam), _IP, _I, ctypes.POINTER(_HP)]),
     "zsph_autotune": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I,
                            ctypes.POINTER(TuneResult), _VP]),
+    "zsph_set_launch_shapes": (_I, [_HP, ctypes.POINTER(TuneResult)]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -371,6 +372,13 @@ class Solver:
         self._call(lib.zsph_autotune, ctypes.byref(self.old), ctypes.byref(self.new), ctypes.byref(self.tmp),
                    int(trial_steps), ctypes.byref(r), stream)
         return _as_dict(r)
+
+    def set_launch_shapes(self, list_cells_per_cta: int = 0, governing_min_ctas: int = 0,
+                          steps_per_graph: int = 0) -> None:
+        """Applies launch shapes from an earlier autotune() result (0 = default) without timing."""
+        r = TuneResult(list_cells_per_cta=int(list_cells_per_cta), governing_min_ctas=int(governing_min_ctas),
+                       steps_per_graph=int(steps_per_graph))
+        self._call(lib.zsph_set_launch_shapes, ctypes.byref(r))
 
     def close(self) -> None:
         if getattr(self, "h", None):

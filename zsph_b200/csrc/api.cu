@@ -643,6 +643,26 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
   return ZSPH_OK;
 }
 
+int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes) {
+  if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle");
+  if (!shapes) return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: null shapes");
+  const int cw = shapes->list_cells_per_cta, mb = shapes->governing_min_ctas, spg = shapes->steps_per_graph;
+  if (cw != 0 && cw != 2 && cw != 4)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: list_cells_per_cta must be 0 (default), 2 or 4");
+  if (mb != 0 && mb != 1 && mb != 6 && mb != 8)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: governing_min_ctas must be 0 (default), 1, 6 or 8");
+  if (spg != 0 && spg != 1 && spg != 4)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: steps_per_graph must be 0 (default), 1 or 4");
+  if (h->graph) {  // captured with the previous shapes
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->kp.tune_cw = cw;
+  h->kp.tune_minb = mb;
+  h->graph_steps = spg ? spg : 1;
+  return ZSPH_OK;
+}
+
 int zsph_status(zsph_handle_t* h, int* flags, int clear) {
   if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle");
   if (int rc = check_device(h)) return rc;
