@@ -368,12 +368,16 @@ constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // short row is not padded to 64.  Each lane keeps only the hits inside its
 // own row range (delta_ns.cu:39-46), so its neighbour set and visit order are
 // those of the per-cell build, and list entries are offsets from the lane's
-// own row start.  Hits are emitted into a padded per-lane list buffer in
-// shared memory and written out with coalesced 16-byte stores.
+// own row start.  Each lane emits the hits of a 16-candidate half block into
+// its 32-entry ring in shared memory; after the half, the lanes write their
+// completed 8-entry blocks together (a nearly converged loop) with 16-byte
+// stores to the blocked list layout.  Flushing at a lane's 8th entry inside
+// the per-hit loop instead diverges: each flush then runs for 2-3 lanes.
 //
 // With WALL, every non-fluid particle then extrapolates its (rho, p) from
 // the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
 // summed in the reference's visit order, and publishes it in the shadows.
+constexpr int kRing = 32;  // list-build ring entries per lane (power of two)
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 
@@ -383,7 +387,9 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   __shared__ __align__(16) float s_x[CW][64];
   __shared__ __align__(16) float s_y[CW][64];
   __shared__ __align__(16) float s_z[CW][64];
-  __shared__ __align__(16) uint16_t s_ring[CW][32][16];  // per lane: the list's current and previous 8-entry block
+  // per lane: a 32-entry ring (a partial 8-entry block plus one half block's
+  // hits fit), padded to 80 bytes so that the lanes' rings spread over the banks
+  __shared__ __align__(16) uint16_t s_ring[CW][32][kRing + 8];
   __shared__ int s_rs[CW][NR][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int p0 = (blockIdx.x * CW + wid) * 32;
@@ -402,12 +408,14 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   float* sz = s_z[wid];
   uint16_t* ring = s_ring[wid][lane];
   uint4* nbv = reinterpret_cast<uint4*>(s.nb);
-  int cnt = 0;
+  int cnt = 0;   // entries emitted
+  int done = 0;  // entries written to global memory (a multiple of 8)
   bool ovf = false;
-  // stores entry number cnt (< kMaxNb); a completed 8-entry block goes to global memory
-  auto put = [&](unsigned e) {
-    ring[cnt & 15] = (uint16_t)e;
-    if ((cnt & 7) == 7) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & 8));
+  // writes the completed 8-entry blocks among the first min(cnt, kMaxNb) entries
+  auto flush = [&]() {
+    const int lim = min(cnt, kMaxNb);
+    for (; done + 8 <= lim; done += 8)
+      nbv[nb_vec(i, done >> 3)] = *reinterpret_cast<const uint4*>(ring + (done & (kRing - 1)));
   };
   unsigned todo = __ballot_sync(0xffffffffu, act);
   while (todo) {
@@ -486,23 +494,33 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
           if (!mh) continue;
           const int off0 = base - sl;  // >= -bit of the lowest kept hit, so every offset is >= 0
           if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
-            const unsigned ent0 = ((unsigned)r << kRowShift) + (unsigned)off0;
-            while (mh) {
-              const int bb = __ffs(mh) - 1;
-              mh &= mh - 1;
-              put(ent0 + bb);
-              ++cnt;
+#pragma unroll
+            for (int hb = 0; hb < 32; hb += 16) {  // one half block, then its flush
+              const unsigned ent0 = ((unsigned)r << kRowShift) + (unsigned)(off0 + hb);
+              unsigned part = (mh >> hb) & 0xffffu;
+              while (part) {
+                const int bb = __ffs(part) - 1;
+                part &= part - 1;
+                ring[cnt & (kRing - 1)] = (uint16_t)(ent0 + bb);
+                ++cnt;
+              }
+              flush();
             }
           } else {
-            while (mh) {
-              const int bb = __ffs(mh) - 1;
-              mh &= mh - 1;
-              const int off = off0 + bb;
-              if (cnt < kMaxNb && off <= kOffMask && !ovf)
-                put(((unsigned)r << kRowShift) | (unsigned)off);
-              else
-                ovf = true;
-              ++cnt;
+#pragma unroll
+            for (int hb = 0; hb < 32; hb += 16) {
+              unsigned part = (mh >> hb) & 0xffffu;
+              while (part) {
+                const int bb = __ffs(part) - 1;
+                part &= part - 1;
+                const int off = off0 + hb + bb;
+                if (cnt < kMaxNb && off <= kOffMask && !ovf)
+                  ring[cnt & (kRing - 1)] = (uint16_t)(((unsigned)r << kRowShift) | (unsigned)off);
+                else
+                  ovf = true;
+                ++cnt;
+              }
+              flush();
             }
           }
         }
@@ -510,7 +528,7 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
     }
   }
   if (cnt > 254) ovf = true;
-  if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & 8));
+  if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
   if (WALL && act && !fluid_of(pi.w)) {
     const KParams kp = BATCH ? scene_kp(kp_arg, scn) : kp_arg;
     float rsum = 0.0f, wsum = 0.0f;
