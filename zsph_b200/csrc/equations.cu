@@ -357,36 +357,46 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
 
 constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // Builds the neighbour lists of 32 consecutive sorted particles per warp,
-// one lane per particle (the plain form).  A cell holds about 18 particles,
-// so one warp per cell leaves about half the lanes idle; here every lane has
-// a particle.  The warp's lanes are split into segments whose cells lie
-// within three consecutive linear cell indices (usually one segment per
-// warp).  For each stencil row a segment tests the union of its lanes' row
-// ranges, which is contiguous in the sorted order because every lane's row
-// range is: 64 candidates at a time staged in shared memory as x/y/z arrays,
-// tested two per step with packed f32x2 arithmetic, in blocks of eight so a
-// short row is not padded to 64.  Each lane keeps only the hits inside its
-// own row range (delta_ns.cu:39-46), so its neighbour set and visit order are
-// those of the per-cell build, and list entries are offsets from the lane's
-// own row start.  Each lane emits the hits of a 16-candidate half block into
-// its 32-entry ring in shared memory; after the half, the lanes write their
-// completed 8-entry blocks together (a nearly converged loop) with 16-byte
-// stores to the blocked list layout.  Flushing at a lane's 8th entry inside
-// the per-hit loop instead diverges: each flush then runs for 2-3 lanes.
+// one lane per particle (the plain form).  A cell holds about 18-24
+// particles, so one warp per cell leaves lanes idle; here every lane has a
+// particle.  The lanes of one cell are contiguous; a round takes up to kSegs
+// cells (segments; usually all of the warp's two or three).  For each
+// stencil row every segment's row range (delta_ns.cu:39-46) is staged, 64
+// candidates at a time, in that segment's x/y/z arrays in shared memory, and
+// every lane tests its own cell's range, two candidates per step with packed
+// f32x2 arithmetic, in blocks of eight so a short row is not padded to 64.
+// Testing the union of the segments' ranges instead (one set of arrays)
+// costs 1.6x the candidate tests on the dam-break cases.  Hits come out in
+// candidate order, so a list is in the reference's visit order, and its
+// entries are offsets from the lane's row start.  Each lane emits the hits
+// of a 16-candidate half block into its 32-entry ring in shared memory;
+// after the half, the lanes write their completed 8-entry blocks together (a
+// nearly converged loop) with 16-byte stores to the blocked list layout.
+// Flushing at a lane's 8th entry inside the per-hit loop instead diverges:
+// each flush then runs for 2-3 lanes.
+//
+// Precision form: candidates are moved into the frame of the lane's own
+// cell (its position is the offset from that cell's corner, as in the pair
+// kernels); every candidate lies within GF cells of it, so each shift k * gs
+// is exact and one rounding forms every coordinate.
 //
 // With WALL, every non-fluid particle then extrapolates its (rho, p) from
 // the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
 // summed in the reference's visit order, and publishes it in the shadows.
 constexpr int kRing = 32;  // list-build ring entries per lane (power of two)
+constexpr int kSegs = 3;   // list build: cells whose lanes test their own rows concurrently
+constexpr int kStage = 66; // list build: staged candidates per segment (64) plus two floats of padding
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 
 template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
 __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
-  __shared__ __align__(16) float s_x[CW][64];
-  __shared__ __align__(16) float s_y[CW][64];
-  __shared__ __align__(16) float s_z[CW][64];
+  // per segment (cell) of a round: its 64 staged candidates; the two floats
+  // of padding put the segments' arrays in different banks
+  __shared__ __align__(16) float s_x[CW][kSegs][kStage];
+  __shared__ __align__(16) float s_y[CW][kSegs][kStage];
+  __shared__ __align__(16) float s_z[CW][kSegs][kStage];
   // per lane: a 32-entry ring (a partial 8-entry block plus one half block's
   // hits fit), padded to 80 bytes so that the lanes' rings spread over the banks
   __shared__ __align__(16) uint16_t s_ring[CW][32][kRing + 8];
@@ -402,10 +412,10 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   const float4 pi = s.sh.pr(act ? i : p0);
   // precision form: the lane's own cell (its position is the offset from that cell's corner)
   const int3 ci = PRECISE && act ? unpack_cell(kp_arg.c3n[i]) : int3{0, 0, 0};
-  u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
-  float* sx = s_x[wid];
-  float* sy = s_y[wid];
-  float* sz = s_z[wid];
+  // the lane's scene (batched form): its cell's neighbour threshold and grid
+  const KParams kp = BATCH ? scene_kp(kp_arg, scn) : kp_arg;
+  const float r2max = kp.r2max;
+  const u64 px = pk2(pi.x, pi.x), py = pk2(pi.y, pi.y), pz = pk2(pi.z, pi.z);
   uint16_t* ring = s_ring[wid][lane];
   uint4* nbv = reinterpret_cast<uint4*>(s.nb);
   int cnt = 0;   // entries emitted
@@ -417,57 +427,61 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
     for (; done + 8 <= lim; done += 8)
       nbv[nb_vec(i, done >> 3)] = *reinterpret_cast<const uint4*>(ring + (done & (kRing - 1)));
   };
+  // The lanes of one cell are contiguous (sorted particles).  A round takes
+  // the next kSegs cells (segments): per stencil row each segment's range is
+  // staged in its own arrays and every lane tests its own cell's range, so no
+  // lane tests candidates outside its range.
+  const int cprev = __shfl_up_sync(0xffffffffu, c, 1);
+  const unsigned starts = __ballot_sync(0xffffffffu, act && (lane == 0 || c != cprev));
   unsigned todo = __ballot_sync(0xffffffffu, act);
   while (todo) {
-    const int f = __ffs(todo) - 1;
-    const int cf = __shfl_sync(0xffffffffu, c, f);
-    const int sf = BATCH ? __shfl_sync(0xffffffffu, scn, f) : 0;
-    const int xd = kp_arg.p.grid_xdim;
-    const bool inseg = ((todo >> lane) & 1u) && c - cf <= 2 && (!BATCH || scn == sf) && (!PRECISE || c / xd == cf / xd);
+    const unsigned sm = starts & todo;  // todo is a run of whole cells
+    const int seg = ((todo >> lane) & 1u) ? __popc(sm & (0xffffffffu >> (31 - lane))) - 1 : kSegs;
+    const bool inseg = seg < kSegs;
     todo &= ~__ballot_sync(0xffffffffu, inseg);
-    const KParams kp = BATCH ? scene_kp(kp_arg, sf) : kp_arg;  // the segment's scene
-    const float r2max = kp.r2max;
-    // Precision form: positions are compared in the frame of the cell one
-    // step in x past the segment's first cell.  The segment's cells are that
-    // cell's x-neighbours (shift -1, 0 or +1 cell) and every candidate lies
-    // within two cells of it, so each shift k * gs is exact and one rounding
-    // forms every coordinate.
-    int3 mid{0, 0, 0};
-    if (PRECISE) {
-      const int cfx = __shfl_sync(0xffffffffu, ci.x, f);
-      mid = make_int3(cfx + 1, __shfl_sync(0xffffffffu, ci.y, f), __shfl_sync(0xffffffffu, ci.z, f));
-      const float sx0 = pi.x + (float)(ci.x - mid.x) * kp.p.grid_size;
-      px = pk2(sx0, sx0);
-    }
+    const int nseg = min(__popc(sm), kSegs);
+    const float* sx = s_x[wid][inseg ? seg : 0];
+    const float* sy = s_y[wid][inseg ? seg : 0];
+    const float* sz = s_z[wid][inseg ? seg : 0];
     for (int r = 0; r < NR; ++r) {
       int sl = 0, el = 0;
       if (inseg) {
         row_range<GF>(kp, t, c, r, sl, el);
         s_rs[wid][r][lane] = sl;
       }
-      const bool has = inseg && sl < el;
-      const int a = __reduce_min_sync(0xffffffffu, has ? sl : INT_MAX);
-      const int b = __reduce_max_sync(0xffffffffu, has ? el : INT_MIN);
-      for (int k0 = a; k0 < b; k0 += 64) {
+      const int len = inseg ? max(el - sl, 0) : 0;
+      const int L = __reduce_max_sync(0xffffffffu, len);
+      for (int k0 = 0; k0 < L; k0 += 64) {
         __syncwarp();
+        unsigned m = sm;
+        for (int g = 0; g < nseg; ++g) {  // uniform: stage segment g's candidates k0 .. k0+63
+          const int lead = __ffs(m) - 1;
+          m &= m - 1;
+          const int sg = __shfl_sync(0xffffffffu, sl, lead), lg = __shfl_sync(0xffffffffu, len, lead);
+          // precision form: candidates move into the frame of the segment's cell
+          int3 cg{0, 0, 0};
+          if (PRECISE)
+            cg = make_int3(__shfl_sync(0xffffffffu, ci.x, lead), __shfl_sync(0xffffffffu, ci.y, lead),
+                           __shfl_sync(0xffffffffu, ci.z, lead));
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int j = k0 + 32 * h + lane;
-          float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
-          if (j < b) q = shadow_pr<PRECISE>(kp, s, j, mid);
-          sx[32 * h + lane] = q.x;
-          sy[32 * h + lane] = q.y;
-          sz[32 * h + lane] = q.z;
+          for (int h = 0; h < 2; ++h) {
+            const int o = k0 + 32 * h + lane;
+            float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
+            if (o < lg) q = shadow_pr<PRECISE>(kp, s, sg + o, cg);
+            s_x[wid][g][32 * h + lane] = q.x;
+            s_y[wid][g][32 * h + lane] = q.y;
+            s_z[wid][g][32 * h + lane] = q.z;
+          }
         }
         __syncwarp();
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-          const int base = k0 + 32 * h;
-          if (base >= b) break;  // uniform
+          const int base = k0 + 32 * h;  // offset of the block in the lane's row range
+          if (base >= L) break;          // uniform
           unsigned mh = 0u;
 #pragma unroll
           for (int blk = 0; blk < 4; ++blk) {
-            if (base + 8 * blk >= b) break;  // uniform: the rest is padding
+            if (base + 8 * blk >= L) break;  // uniform: the rest is padding
 #pragma unroll
             for (int tt = 8 * blk; tt < 8 * blk + 8; tt += 2) {
               const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
@@ -481,18 +495,14 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
               if (r1 <= r2max) mh |= 2u << tt;
             }
           }
-          // keep the hits inside this lane's own row range [sl, el), not itself
-          const int lo = sl - base, hi = el - base;
-          unsigned keep = 0u;
-          if (has && hi > 0 && lo < 32) {
-            const unsigned up = hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u);
-            const unsigned dn = lo <= 0 ? 0xffffffffu : ~((1u << lo) - 1u);
-            keep = up & dn;
-          }
-          if (i >= base && i < base + 32) keep &= ~(1u << (i - base));
+          // keep the hits inside this lane's range (offsets < len), not itself
+          const int hi = len - base;
+          unsigned keep = hi <= 0 ? 0u : (hi >= 32 ? 0xffffffffu : ((1u << hi) - 1u));
+          const int self = i - sl - base;
+          if (self >= 0 && self < 32) keep &= ~(1u << self);
           mh &= keep;
           if (!mh) continue;
-          const int off0 = base - sl;  // >= -bit of the lowest kept hit, so every offset is >= 0
+          const int off0 = base;
           if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
 #pragma unroll
             for (int hb = 0; hb < 32; hb += 16) {  // one half block, then its flush
@@ -530,7 +540,6 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
   if (WALL && act && !fluid_of(pi.w)) {
-    const KParams kp = BATCH ? scene_kp(kp_arg, scn) : kp_arg;
     float rsum = 0.0f, wsum = 0.0f;
     if (!ovf) {
       for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
