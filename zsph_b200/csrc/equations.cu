@@ -389,18 +389,18 @@ constexpr int kStage = 66; // list build: staged candidates per segment (64) plu
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 
+// At least 42 warps per SM (a register budget of 40-48 without spills in the
+// plain form, 9.9 KB of shared memory per 2-warp CTA): the kernel is
+// issue-bound and hides its staging loads with more resident warps.
 template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
-__global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
+__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   constexpr int NR = Stencil<GF>::NR;
-  // per segment (cell) of a round: its 64 staged candidates; the two floats
-  // of padding put the segments' arrays in different banks
-  __shared__ __align__(16) float s_x[CW][kSegs][kStage];
-  __shared__ __align__(16) float s_y[CW][kSegs][kStage];
-  __shared__ __align__(16) float s_z[CW][kSegs][kStage];
+  // per segment (cell) of a round: its 64 staged candidates' x, y and z; the
+  // two floats of padding per array put the segments' arrays in different banks
+  __shared__ __align__(16) float s_c[CW][kSegs][3][kStage];
   // per lane: a 32-entry ring (a partial 8-entry block plus one half block's
   // hits fit), padded to 80 bytes so that the lanes' rings spread over the banks
   __shared__ __align__(16) uint16_t s_ring[CW][32][kRing + 8];
-  __shared__ int s_rs[CW][NR][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int p0 = (blockIdx.x * CW + wid) * 32;
   if (p0 >= kp_arg.n) return;  // uniform per warp
@@ -440,15 +440,10 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
     const bool inseg = seg < kSegs;
     todo &= ~__ballot_sync(0xffffffffu, inseg);
     const int nseg = min(__popc(sm), kSegs);
-    const float* sx = s_x[wid][inseg ? seg : 0];
-    const float* sy = s_y[wid][inseg ? seg : 0];
-    const float* sz = s_z[wid][inseg ? seg : 0];
+    const float* sx = s_c[wid][inseg ? seg : 0][0];  // y and z follow at kStage, 2 * kStage
     for (int r = 0; r < NR; ++r) {
       int sl = 0, el = 0;
-      if (inseg) {
-        row_range<GF>(kp, t, c, r, sl, el);
-        s_rs[wid][r][lane] = sl;
-      }
+      if (inseg) row_range<GF>(kp, t, c, r, sl, el);
       const int len = inseg ? max(el - sl, 0) : 0;
       const int L = __reduce_max_sync(0xffffffffu, len);
       for (int k0 = 0; k0 < L; k0 += 64) {
@@ -468,9 +463,9 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
             const int o = k0 + 32 * h + lane;
             float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
             if (o < lg) q = shadow_pr<PRECISE>(kp, s, sg + o, cg);
-            s_x[wid][g][32 * h + lane] = q.x;
-            s_y[wid][g][32 * h + lane] = q.y;
-            s_z[wid][g][32 * h + lane] = q.z;
+            s_c[wid][g][0][32 * h + lane] = q.x;
+            s_c[wid][g][1][32 * h + lane] = q.y;
+            s_c[wid][g][2][32 * h + lane] = q.z;
           }
         }
         __syncwarp();
@@ -485,8 +480,8 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
 #pragma unroll
             for (int tt = 8 * blk; tt < 8 * blk + 8; tt += 2) {
               const u64 x2 = *reinterpret_cast<const u64*>(&sx[32 * h + tt]);
-              const u64 y2 = *reinterpret_cast<const u64*>(&sy[32 * h + tt]);
-              const u64 z2 = *reinterpret_cast<const u64*>(&sz[32 * h + tt]);
+              const u64 y2 = *reinterpret_cast<const u64*>(&sx[kStage + 32 * h + tt]);
+              const u64 z2 = *reinterpret_cast<const u64*>(&sx[2 * kStage + 32 * h + tt]);
               const u64 dx = sub2(px, x2), dy = sub2(py, y2), dz = sub2(pz, z2);
               const u64 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
               float r0, r1;
@@ -545,8 +540,11 @@ __global__ void __launch_bounds__(CW * 32) k_nblist_seq(KParams kp_arg, Scratch 
       for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
         const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
         const int r = (int)(e >> kRowShift);
-        if (Stencil<GF>::boundary_row(r))
-          wall_term<PRECISE>(kp, s, pi, s_rs[wid][r][lane] + (int)(e & kOffMask), rsum, wsum, ci);
+        if (Stencil<GF>::boundary_row(r)) {
+          int a, b;  // the row's start (its cell bounds are L1-resident by now)
+          row_range<GF>(kp, t, c, r, a, b);
+          wall_term<PRECISE>(kp, s, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
+        }
       }
     } else {
       for (int r = 0; r < NR; ++r) {
