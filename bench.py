@@ -448,7 +448,11 @@ def run_ours(args, dist: Dist):
     gov_ms = kern.get("governing", {}).get("ms_per_step", 0) / 2
     pair = pair_kernel_rates(sol, kern, nb_b, nb_g, n, ck)
     dominant = {"kernel": dom[0], "ms_per_step": dom[1]["ms_per_step"], "share": dom[1]["share"],
-                "bound": "fp32 pair arithmetic / latency (not hbm, no tensor-core work on the pair path)",
+                "bound": {"nblist_wall": "instruction issue (candidate tests and per-lane hit emission)",
+                          "boundary": "L1 data pipe (scattered neighbour records)",
+                          "governing": "L1 data pipe (scattered neighbour records)"}.get(
+                              dom[0], "see profiles/kernels_medium.md") +
+                         "; not HBM-bound, no tensor-core work on the pair path",
                 "interacting_pairs_per_particle": pairs_gov,
                 "governing_pair_evals_per_s": pairs_gov * n / (gov_ms / 1e3) if gov_ms else None,
                 "traffic": ncu_traffic(dom[0])}
