@@ -425,7 +425,8 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* ne
 /* Applies launch shapes chosen earlier (a zsph_autotune result kept by the
  * caller, e.g. across restarts of the same case) without timing anything:
  * list_cells_per_cta, governing_min_ctas and steps_per_graph from the
- * candidate sets above, 0 for each one's default; the time fields are
+ * candidate sets above, 0 for each one's default (2 warps, 1 CTA, 1 step:
+ * the shapes the tuner picks on the dam-break cases); the time fields are
  * ignored.  ZSPH_EINVAL for any other value. */
 int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes);
 

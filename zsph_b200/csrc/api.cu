@@ -611,7 +611,7 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
         if (e) break;
         ms /= (float)(launches * spg);
         ++count;
-        if (cw == 4 && mb == (h->kp.scenes ? 1 : 6) && spg == 1) ms_default = ms;  // the untuned shapes
+        if (cw == 2 && mb == 1 && spg == 1) ms_default = ms;  // the untuned shapes
         if (ms < best.ms_per_step) {
           best.ms_per_step = ms;
           best.list_cells_per_cta = cw;

@@ -954,9 +954,10 @@ inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 template <bool WALL, bool BATCH>
 void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
+  // default (0): two warps per CTA, what zsph_autotune picks on the dam-break cases
   switch (kp.tune_cw) {
-    case 2: k_nblist_seq<1, WALL, 2, BATCH><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t); break;
-    default: k_nblist_seq<1, WALL, 4, BATCH><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t); break;
+    case 4: k_nblist_seq<1, WALL, 4, BATCH><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t); break;
+    default: k_nblist_seq<1, WALL, 2, BATCH><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t); break;
   }
 }
 
@@ -967,11 +968,12 @@ void launch_governing_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_
                             const zsph_ptc_t& out, cudaStream_t st) {
   const FeatOut none{};
   const int nb = thread_blocks(kp.n), sm = pair_smem<1>(0, 0);
+  // default (0): one resident CTA minimum (the largest register budget), what
+  // zsph_autotune picks on the dam-break cases
   switch (kp.tune_minb) {
-    case 1: k_governing<1, MODE, false, false, BATCH, false, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
     case 6: k_governing<1, MODE, false, false, BATCH, false, 6><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
     case 8: k_governing<1, MODE, false, false, BATCH, false, 8><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
-    default: k_governing<1, MODE, false, false, BATCH><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
+    default: k_governing<1, MODE, false, false, BATCH, false, 1><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, out, none); break;
   }
 }
 
