@@ -384,7 +384,7 @@ constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
 // summed in the reference's visit order, and publishes it in the shadows.
 constexpr int kRing = 32;  // list-build ring entries per lane (power of two)
-constexpr int kSegs = 3;   // list build: cells whose lanes test their own rows concurrently
+constexpr int kSegs = 4;   // list build: cells whose lanes test their own rows concurrently
 constexpr int kStage = 66; // list build: staged candidates per segment (64) plus two floats of padding
 // warps per CTA of k_nblist_seq (the 5x5 stencil's row starts need more shared memory)
 template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
