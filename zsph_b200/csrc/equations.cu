@@ -127,14 +127,19 @@ __device__ __forceinline__ void load_rows(const KParams& kp, const zsph_tmp_t& t
 }
 
 // Walks particle i's neighbours in visit order.  List entries (row r,
-// offset o) name the global particle rs[r] + o, checked against the row end
-// re[r]; what the arithmetic needs is fetched from index fb[r] + o (fb = rs
-// for the global arrays, or the row's base in a shared-memory window), four
-// neighbours ahead of their arithmetic; invalid slots fetch index fdummy.
-// Particles whose list overflowed re-filter their stencil rows directly.
+// offset o) name the global particle rs[r] + o; what the arithmetic needs is
+// fetched from index fb[r] + o (fb = rs for the global arrays, or the row's
+// base in a shared-memory window), four neighbours ahead of their
+// arithmetic; invalid slots fetch index fdummy.  Every caller builds the
+// lists from the same cell bounds just before the walk, so o is inside the
+// row; the fetch index is only clamped to fmax (the last particle, or the
+// window's last slot), which keeps every access in bounds without a
+// shared-memory load of the row end per entry.  Particles whose list
+// overflowed re-filter their stencil rows directly.
 template <int GF, bool BOUNDARY_ONLY, class Nb, class Fetch, class Use>
 __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i, float4 pi, const int* rs,
-                                     const int* re, const int* fb, int fdummy, Fetch&& fetch, Use&& use) {
+                                     const int* re, const int* fb, int fdummy, int fmax, Fetch&& fetch,
+                                     Use&& use) {
   const int cnt = s.nb_cnt[i];
   if (cnt != kOverflow) {
     const uint4* lst = reinterpret_cast<const uint4*>(s.nb);
@@ -146,9 +151,8 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
       for (int e = 0; e < 8; ++e) {
         const unsigned ent = (wv[e >> 1] >> ((e & 1) * 16)) & 0xffffu;
         const int r = (int)(ent >> kRowShift), off = (int)(ent & kOffMask);
-        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r)) &&
-                        rs[r * kPairBlock] + off < re[r * kPairBlock];
-        js[e] = ok ? fb[r * kPairBlock] + off : -1;
+        const bool ok = (k + e < cnt) && (!BOUNDARY_ONLY || Stencil<GF>::boundary_row(r));
+        js[e] = ok ? min(fb[r * kPairBlock] + off, fmax) : -1;
       }
 #pragma unroll
       for (int h = 0; h < 8; h += 4) {
@@ -651,10 +655,10 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   };
   const float4* win = sm.win;
   if (staged)
-    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
+    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapB - 1,
                          [&](int q) { return NbB1{win[2 * q], win[2 * q + 1]}; }, use1);
   else
-    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
+    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
                          [&](int q) {
                            const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
                            return NbB1{r.pr, r.vp};
@@ -795,10 +799,10 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
   };
   const float4* win = sm.win;
   if (staged)
-    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0,
+    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapG - 1,
                          [&](int q) { return NbG{win[2 * q], win[2 * q + 1], win[2 * kWinCapG + q]}; }, use);
   else
-    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i,
+    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
                          [&](int q) {
                            const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
                            return NbG{r.pr, r.vp, dg[q]};
@@ -878,7 +882,7 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary_simple(KParams kp, Scra
   float divv = 0.f;
   if (fi)
     walk<GF, true, NbB1>(
-        kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) {
+        kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1, [&](int q) {
           const ShadowRec r = s.sh.load(q);
           return NbB1{r.pr, r.vp};
         },
@@ -913,7 +917,7 @@ __global__ void __launch_bounds__(kPairBlock) k_governing_simple(KParams kp, Scr
   const float d0 = t.dofv[i];
   float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
   walk<GF, false, NbS>(
-      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, [&](int q) {
+      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1, [&](int q) {
         const ShadowRec r = s.sh.load(q);
         return NbS{r.pr, r.vp, t.dofv[q]};
       },
