@@ -162,3 +162,10 @@ def test_create_rejects_bad_grid_and_factor():
     gp.grid_factor = 3
     assert z.lib.zsph_create(ctypes.byref(gp), cp.grid_num, ctypes.byref(h)) == z.ZSPH_EINVAL
     assert "grid_factor" in z.last_error()
+
+
+def test_set_launch_shapes_rejects_a_null_handle_or_shapes():
+    # argument checks come before any CUDA call, so they run without a GPU
+    t = z.TuneResult(list_cells_per_cta=2, governing_min_ctas=1, steps_per_graph=1)
+    assert z.lib.zsph_set_launch_shapes(None, ctypes.byref(t)) == z.ZSPH_EINVAL
+    assert "null handle" in z.last_error()
