@@ -60,9 +60,20 @@ def parse():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-form leg")
     ap.add_argument("--learn-epochs", type=int, default=20)
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of zsph_autotune's")
+    ap.add_argument("--ref-cuda-child", choices=["plain", "profiled"], default=None,
+                    help=argparse.SUPPRESS)  # one reference-CUDA run in a fresh process (reference arm)
     ap.add_argument("--shapes", default=None, metavar="CW,MINB,SPG",
                     help="apply these launch shapes (zsph_set_launch_shapes) instead of running zsph_autotune")
     return ap.parse_args()
+
+
+def workload_config(args, case, grid_num, dt, world) -> dict:
+    """The `config` object of both arms' JSON lines (same keys and values)."""
+    return {"workload": WORKLOAD if args.workload == "config1" else f"{args.workload}: {case.name}",
+            "ptc_num": case.n, "fluid": case.n_fluid, "wall": case.n_wall, "grid_num": int(grid_num),
+            "dt": float(dt), "parallelism": f"replicas x{world}",
+            "l2": (f"inputs larger than L2 (particle state {case.n * 72 / 1e9:.2f} GB + scratch per step)"
+                   if case.n * 72 > 126e6 else "inputs smaller than L2 (profiling and parity-size case)")}
 
 
 def make_case(name):
@@ -493,10 +504,8 @@ def run_ours(args, dist: Dist):
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": dist.world,
         "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (lattice dam break, no randomness)",
-        "config": {"workload": WORKLOAD, "ptc_num": n, "fluid": case.n_fluid, "wall": case.n_wall,
-                   "grid_num": G, "dt": float(cp.dt), "parallelism": f"replicas x{dist.world}",
-                   "l2": "inputs larger than L2 (particle state 0.76 GB + scratch per step)",
-                   "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3)},
+        "config": workload_config(args, case, G, cp.dt, dist.world),
+        "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3),
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
         "tune": tune,
         "roofline": roofline, "dominant_kernel": dominant, "pair_kernels": pair, "kernels": kern, "cpu_baseline": cpu,
@@ -507,45 +516,114 @@ def run_ours(args, dist: Dist):
 
 
 # ---------------------------------------------------------------- reference arm
-def run_reference(args, dist: Dist):
-    """Reference's equations on the host cores (CPU oracle = the port: the
-    reference has no CPU implementation) plus the reference's own CUDA build."""
-    if dist.rank != 0:
-        return None
+REF_CUDA_RUNS = 3
+
+
+def ref_cuda_child(args):
+    """One reference-CUDA measurement in this (fresh) process: `plain` is the
+    step loop timed first event to last (oracle/ref_driver.cu ref_run);
+    `profiled` adds an event after each launch slot and the host time of the
+    Thrust sort calls (ref_run_profiled).  Prints one JSON line."""
     from oracle import pyoracle as po
     case = make_case(args.workload)
-    cpu = cpu_baseline(case, max(args.cpu_seconds, 30.0))
-    line = {"impl": "reference", "metric": "particle-steps/s", "value": cpu["value"], "unit": "particle-steps/s",
-            "n_gpus": 1, "steps": 0, "warmup": 0, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (lattice dam break, no randomness)",
-            "config": {"workload": WORKLOAD, "ptc_num": case.n},
-            "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "particle-steps/s",
-                                         "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    line["steps"] = int(cpu["sample"].split()[0])
-    if po.ref_available():
-        try:
-            import torch
-            if torch.cuda.is_available():
-                # two fresh runs from the case's initial state; the faster one is
-                # reported, both are listed (a transient slowdown shows as a spread)
-                runs = [po.ref_run(case.json, case.state, args.steps, warmup=args.warmup)[2] for _ in range(2)]
-                ms = min(runs)
-                line["reference_cuda"] = {"value": case.n / (ms / 1e3), "unit": "particle-steps/s",
-                                          "ms_per_step": ms, "ms_per_step_runs": runs, "steps": args.steps,
-                                          "warmup": args.warmup,
-                                          "what": "the reference's own hash/sort/boundary/governing/time "
-                                                  "integration kernels (unmodified sources, -maxrregcount 64, "
-                                                  "sm_100a), Thrust sort, launch order of main.cu:63-88, CUDA "
-                                                  "events; the faster of two runs"}
-        except Exception as e:  # keep the CPU line even if the GPU leg fails
-            line["reference_cuda"] = {"unavailable": str(e)[:200]}
+    t0 = time.perf_counter()
+    if args.ref_cuda_child == "plain":
+        ms = po.ref_run(case.json, case.state, args.steps, warmup=args.warmup)[2]
+        out = {"ms_per_step": ms}
     else:
-        line["reference_cuda"] = {"unavailable": "oracle/_ref/libzsph_ref.so not built"}
+        out = po.ref_run_profiled(case.json, case.state, args.steps, warmup=args.warmup)
+    out["process_seconds"] = time.perf_counter() - t0
+    print(json.dumps(out), flush=True)
+
+
+def reference_cuda_leg(args, case) -> dict:
+    """The reference's own CUDA kernels (oracle/_ref, built from its sources):
+    REF_CUDA_RUNS plain runs and one profiled run, each in a fresh process
+    started one after another, before any CPU work of this arm.  Reports the
+    median of the plain runs with their spread, and the per-slot split."""
+    from oracle import pyoracle as po
+    if not po.ref_available():
+        return {"unavailable": "oracle/_ref/libzsph_ref.so not built"}
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {"unavailable": "no CUDA device"}
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"torch: {e}"[:200]}
+
+    def child(mode):
+        cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--ref-cuda-child", mode,
+               "--workload", args.workload, "--steps", str(args.steps), "--warmup", str(args.warmup)]
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference CUDA run failed (rc {r.returncode}): {r.stderr[-300:]}")
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+    try:
+        plain = [child("plain") for _ in range(REF_CUDA_RUNS)]
+        prof = child("profiled")
+    except Exception as e:  # noqa: BLE001 - keep the CPU line even if the GPU leg fails
+        return {"unavailable": str(e)[:300]}
+    runs = [p["ms_per_step"] for p in plain]
+    ms = statistics.median(runs)
+    slots = prof["slot_ms"]
+    sort_slots = slots["sort_index"] + slots["sort_index_2"]
+    return {"value": case.n / (ms / 1e3), "unit": "particle-steps/s", "ms_per_step": ms,
+            "ms_per_step_runs": runs, "spread": (max(runs) - min(runs)) / ms, "steps": args.steps,
+            "warmup": args.warmup,
+            "profiled": {"ms_per_step": prof["ms_per_step"], "slot_ms": slots, "host_sort_ms": prof["host_sort_ms"],
+                         "sort_share": sort_slots / prof["ms_per_step"]},
+            "what": "the reference's own hash/sort/boundary/governing/time integration kernels (unmodified sources, "
+                    "-maxrregcount 64, sm_100a), Thrust sort, launch order of main.cu:63-88, CUDA events; median "
+                    f"of {REF_CUDA_RUNS} runs, each in a fresh process, run before the CPU leg; `profiled` is one "
+                    "more run with an event after each launch slot and the host time of each Thrust sort call"}
+
+
+def run_reference(args, dist: Dist):
+    """Reference arm.  `value`: the reference solver's equations on the host
+    cores; the reference has no CPU implementation of its own (its kernels
+    exist only as CUDA), so this is the CPU oracle, an OpenMP restatement of
+    those kernels (kind "port"), W untimed and K timed full steps of the
+    same case.  `reference_cuda`: the reference's own CUDA build on the GPU,
+    measured first, in separate processes."""
+    if dist.rank != 0:
+        return None
+    import numpy as np
+    from oracle import pyoracle as po
+    case = make_case(args.workload)
+    rc, op = po.params(case.json)
+    if rc:
+        raise SystemExit(f"case constants rejected by the oracle (rc {rc})")
+    ref_cuda = reference_cuda_leg(args, case)
+
+    K, W = args.steps, args.warmup
+    threads = os.cpu_count() or 1
+    po.set_threads(threads)
+    o = po.Oracle(case.json, case.state, np.float32)
+    if W:
+        o.step(W)
+    t0 = time.perf_counter()
+    o.step(K)
+    dt = time.perf_counter() - t0
+    value = case.n * K / dt
+    cpu = {"value": value, "unit": "particle-steps/s", "cores": po.max_threads(), "kind": "port",
+           "sample": f"{K} full steps (after {W} untimed) of the {case.n:,}-particle case: FP32 CPU oracle, OpenMP, "
+                     f"{dt:.1f} s"}
+    line = {"impl": "reference", "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
+            "n_gpus": 1, "steps": K, "warmup": W, "ms_per_step": dt / K * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (lattice dam break, no randomness)",
+            "config": workload_config(args, case, op.grid_num, op.dt, dist.world),
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_cuda": ref_cuda}
     return line
 
 
 def main():
     args = parse()
+    if args.ref_cuda_child:
+        ref_cuda_child(args)
+        return
     dist = Dist()
     try:
         line = run_reference(args, dist) if args.impl == "reference" else run_ours(args, dist)

@@ -166,9 +166,14 @@ int zsph_sort_index(zsph_handle_t* h, const zsph_tmp_t* tmp, void* stream);
  * library until the process exits, so it accepts at most 131072 particles
  * (gparam->ptc_num) and 131072 cells (grid_num) and returns ZSPH_EINVAL
  * beyond that.  The first call on a device looks up the array's address
- * (cudaGetSymbolAddress); make that call before any stream capture.  All
- * calls share the array: calls whose work overlaps on the GPU race.  Errors
- * are reported through zsph_last_error(NULL, ...). */
+ * (cudaGetSymbolAddress); make that call before any stream capture.  The
+ * address is kept per device and context: the first call in a new context of
+ * the device (after cudaDeviceReset, for example) looks it up again and must
+ * also come before any stream capture.  Keys must lie in [0, grid_num): a key
+ * outside it is sorted and written back clamped to 0 or grid_num - 1, without
+ * an error (zsph_sort_index reports it through zsph_status).  All calls share
+ * the array: calls whose work overlaps on the GPU race.  Errors are reported
+ * through zsph_last_error(NULL, ...). */
 int zsph_sort_index_noalloc(const zsph_gpu_param_t* gparam, int grid_num, const zsph_tmp_t* tmp, void* stream);
 /* cuda_sort_data (single_gpu_sph_src/lib/sort.cu:8-84): grid_start/grid_end
  * from the sorted keys (with the reference's end-of-array rules) and the

@@ -8,7 +8,8 @@
 # Output goes only to oracle/_ref/ (git-ignored).  Test infrastructure only.
 set -euo pipefail
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${ZSPH_REFERENCE:-/root/reference}
+# the reference checkout: ZSPH_REFERENCE, else a "reference" directory beside this repository
+REF=${ZSPH_REFERENCE:-$(cd "$HERE/../.." && pwd)/reference}
 SG="$REF/single_gpu_sph_src"
 OUT="$HERE/_ref"
 if [ ! -d "$SG" ]; then

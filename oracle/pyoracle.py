@@ -366,6 +366,7 @@ def ref_lib(simple: bool = False) -> ctypes.CDLL:
         lib_ = ctypes.CDLL(REF_SIMPLE_SO if simple else REF_SO)
         lib_.ref_substep.restype = _I
         lib_.ref_run.restype = _I
+        lib_.ref_run_profiled.restype = _I
         lib_.ref_params.restype = _I
         lib_.ref_last_error.restype = ctypes.c_char_p
         _ref[simple] = lib_
@@ -427,3 +428,25 @@ def ref_run(json, state, nsteps: int, warmup: int = 0, simple: bool = False):
     if rc:
         raise RuntimeError(lib_.ref_last_error().decode())
     return out, tmp, float(ms.value)
+
+
+REF_SLOTS = ("hash", "sort_index", "sort_data", "boundary", "governing", "prediction",
+             "hash_2", "sort_index_2", "sort_data_2", "boundary_2", "governing_2", "correction")
+
+
+def ref_run_profiled(json, state, nsteps: int, warmup: int = 0, simple: bool = False) -> dict:
+    """`warmup + nsteps` reference steps with a CUDA event after each of the
+    step's twelve launch slots (main.cu:63-88) and the host time of each
+    Thrust sort call; returns per-step means in ms."""
+    n = int(json.ptc_num)
+    arrs, rin = _rstate(state, n)
+    ms = ctypes.c_float(0.0)
+    slots = (ctypes.c_float * 12)()
+    host = (ctypes.c_float * 2)()
+    lib_ = ref_lib(simple)
+    rc = lib_.ref_run_profiled(ctypes.byref(case_of(json)), ctypes.byref(rin), _I(warmup), _I(nsteps),
+                               ctypes.byref(ms), slots, host)
+    if rc:
+        raise RuntimeError(lib_.ref_last_error().decode())
+    return {"ms_per_step": float(ms.value), "slot_ms": dict(zip(REF_SLOTS, (float(v) for v in slots))),
+            "host_sort_ms": [float(host[0]), float(host[1])]}

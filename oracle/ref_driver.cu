@@ -272,4 +272,96 @@ int ref_run(const rcase_t* c, const rstate_t* in, int warmup, int nsteps, rstate
   return rc;
 }
 
+// The loop of ref_run with a CUDA event after each of a step's twelve launch
+// slots (main.cu:63-88: hash, sort_index, sort_data, boundary, governing,
+// prediction, then the same five and correction), so that where the step's
+// time goes can be read per slot.  A slot's time is the interval between the
+// events around it; for the two cuda_sort_index slots it includes every gap
+// the host leaves on the device while Thrust allocates and frees its
+// temporary storage (lib/sort.cu:5 uses Thrust's default allocator, i.e. a
+// cudaMalloc and a cudaFree per call).  The host time of each
+// cuda_sort_index call is measured with a steady clock.
+//   slot_ms[12]      per-step mean of each slot (ms)
+//   host_sort_ms[2]  per-step mean host duration of the two sort calls (ms)
+//   ms_per_step      first event to last, per step
+// Events add a few microseconds per launch; ref_run gives the step time
+// without them.
+int ref_run_profiled(const rcase_t* c, const rstate_t* in, int warmup, int nsteps, float* ms_per_step,
+                     float* slot_ms, float* host_sort_ms) {
+  g_err = 0;
+  if (nsteps <= 0) return 0;
+  Session s;
+  if (open_session(c, in, s)) return 1;
+  const int kSlots = 12;
+  std::vector<cudaEvent_t> ev((size_t)nsteps * (kSlots + 1));
+  for (auto& e : ev) cudaEventCreate(&e);
+  double host_ms[2] = {0.0, 0.0};
+  for (int i = 0; i < warmup + nsteps; ++i) {
+    const bool timed = i >= warmup;
+    cudaEvent_t* e = timed ? &ev[(size_t)(i - warmup) * (kSlots + 1)] : nullptr;
+    auto mark = [&](int k) {
+      if (timed) cudaEventRecord(e[k]);
+    };
+    auto sort = [&](int which) {
+      auto t0 = std::chrono::steady_clock::now();
+      cuda_sort_index(s.tmp, s.cp);
+      auto t1 = std::chrono::steady_clock::now();
+      if (timed) host_ms[which] += std::chrono::duration<double, std::milli>(t1 - t0).count();
+    };
+    mark(0);
+    cuda_ptc_hash<<<s.grid, s.block>>>(s.d_old);
+    mark(1);
+    sort(0);
+    mark(2);
+    cuda_sort_data<<<s.grid, s.block>>>(s.d_old, s.d_new);
+    mark(3);
+    cuda_boundary_ns<<<s.grid, s.block>>>(s.d_new);
+    mark(4);
+    cuda_govering_ns<<<s.grid, s.block>>>(s.d_new);
+    mark(5);
+    cuda_prediction<<<s.grid, s.block>>>(s.d_new);
+    mark(6);
+    cuda_ptc_hash<<<s.grid, s.block>>>(s.d_new);
+    mark(7);
+    sort(1);
+    mark(8);
+    cuda_sort_data<<<s.grid, s.block>>>(s.d_new, s.d_old);
+    mark(9);
+    cuda_boundary_ns<<<s.grid, s.block>>>(s.d_old);
+    mark(10);
+    cuda_govering_ns<<<s.grid, s.block>>>(s.d_old);
+    mark(11);
+    cuda_correction<<<s.grid, s.block>>>(s.d_old);
+    mark(12);
+  }
+  cudaError_t err = cudaDeviceSynchronize();
+  if (!err) err = cudaGetLastError();
+  int rc = err ? fail("ref_run_profiled", err) : 0;
+  if (!rc) {
+    double slot[kSlots] = {0.0};
+    double total = 0.0;
+    for (int st = 0; st < nsteps; ++st) {
+      cudaEvent_t* e = &ev[(size_t)st * (kSlots + 1)];
+      for (int k = 0; k < kSlots; ++k) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e[k], e[k + 1]);
+        slot[k] += ms;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e[0], e[kSlots]);
+      total += ms;
+    }
+    for (int k = 0; k < kSlots; ++k)
+      if (slot_ms) slot_ms[k] = (float)(slot[k] / nsteps);
+    if (host_sort_ms) {
+      host_sort_ms[0] = (float)(host_ms[0] / nsteps);
+      host_sort_ms[1] = (float)(host_ms[1] / nsteps);
+    }
+    if (ms_per_step) *ms_per_step = (float)(total / nsteps);
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  close_session(s);
+  return rc;
+}
+
 }  // extern "C"

@@ -30,6 +30,18 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_case_generator_does_not_map_the_library():
+    # the reference arm of bench.py builds its case with zsph_b200.cases; that
+    # must leave libzsph_b200.so unmapped (a fresh process, so nothing earlier loaded it)
+    import subprocess
+    import sys
+    code = ("import zsph_b200 as z\nfrom zsph_b200 import cases\ncases.config0(); cases.batch_scenes(4, seed=1)\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "print(int(z.lib.loaded()), int('libzsph_b200' in maps))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, check=True)
+    assert out.stdout.split() == ["0", "0"], out.stdout + out.stderr
+
+
 def test_no_cpu_fallback_path():
     # the package binds only the CUDA library; no oracle import on the product path
     src = open(os.path.join(ROOT, "zsph_b200", "__init__.py")).read()

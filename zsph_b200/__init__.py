@@ -3,8 +3,10 @@
 The product is the CUDA library ``libzsph_b200.so`` built in this directory;
 this module only binds its C entry points with ctypes and offers a thin
 ``Solver`` that owns device buffers in the reference solver's particle layout
-(single_gpu_sph_src/header/data_structure.cuh:158-182).  Importing it loads the
-library and fails loudly if it has not been built: there is no fallback.
+(single_gpu_sph_src/header/data_structure.cuh:158-182).  The library is
+loaded on the first call that needs it (so that the case generator and the
+ctypes struct types can be used without mapping it); that first call fails
+loudly if the library has not been built: there is no fallback.
 """
 from __future__ import annotations
 
@@ -40,10 +42,34 @@ def _load() -> ctypes.CDLL:
         raise ImportError(
             f"{LIB_PATH} is missing: build it with `make -C zsph_b200` or __graft_entry__.build(); "
             "zsph_b200 has no CPU fallback")
-    return ctypes.CDLL(LIB_PATH)
+    cdll = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in _sig.items():
+        fn = getattr(cdll, name)
+        fn.restype = res
+        fn.argtypes = args
+    return cdll
 
 
-lib = _load()
+class _LazyLib:
+    """Stands for the ctypes handle of libzsph_b200.so: the first attribute
+    lookup loads the library (raising ImportError if it is missing) and
+    binds every entry point's signature; later lookups go straight to it."""
+
+    def __init__(self):
+        self._cdll = None
+
+    def loaded(self) -> bool:
+        return self._cdll is not None
+
+    def __getattr__(self, name):
+        if name.startswith("__"):
+            raise AttributeError(name)
+        if self._cdll is None:
+            self._cdll = _load()
+        return getattr(self._cdll, name)
+
+
+lib = _LazyLib()
 
 _F = ctypes.c_float
 _I = ctypes.c_int
@@ -241,12 +267,6 @@ def read_vtk(path: str, n: int, rho0: float = 1000.0, accept_float: bool = False
     check(lib.zsph_read_vtk(path.encode(), n, float(rho0), 1 if accept_float else 0, _ptr(st.pos), _ptr(st.vel),
                             _ptr(st.rhop), _ptr(acc), _ptr(st.type), _ptr(st.table)))
     return st, acc
-for _name, (_res, _args) in _sig.items():
-    _fn = getattr(lib, _name)
-    _fn.restype = _res
-    _fn.argtypes = _args
-
-
 def last_error(handle=None) -> str:
     buf = ctypes.create_string_buffer(1024)
     lib.zsph_last_error(handle, buf, len(buf))

@@ -16,12 +16,27 @@
 //
 // Set-up: the first call on each device looks up the array's device address
 // with cudaGetSymbolAddress (with that device current); make that first call
-// before any stream capture on the device.
+// before any stream capture on the device.  The address belongs to the
+// device's context: the lookup is kept together with the context's id
+// (cuCtxGetId, reached through the runtime's driver entry points, so the
+// library does not link libcuda), and a call made in a different context, for
+// example after cudaDeviceReset, looks the address up again.  The first call
+// after such a reset is then a set-up call too and must also come before any
+// stream capture.
+//
+// Keys: hash values must lie in [0, grid_num).  A key outside that range is
+// sorted as if it were 0 (negative keys) or grid_num - 1 (keys too large) and
+// is written back clamped; this entry point does not report it, since the
+// only place it could report it is the shared array, which the next call
+// clears.  zsph_sort_index on a handle reports the same condition as
+// ZSPH_EINVAL through zsph_status.
 //
 // Sharing: every call on a device uses the same array, which keeps the last
 // call's contents.  Each call clears the parts that must start at zero.  Calls
 // whose work overlaps on the GPU (different streams, or different host
 // threads) race on the array and must be serialised by the caller.
+#include <cuda.h>  // CUcontext / CUresult types only; the entry points come from the runtime
+
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -60,6 +75,37 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocBytes];
 
 std::mutex g_mu;
 unsigned char* g_base[kMaxDevices] = {};
+unsigned long long g_ctx[kMaxDevices] = {};  // id of the context g_base[dev] was looked up in
+
+using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
+using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+std::once_flag g_entry_once;
+
+// Unique id of the calling thread's current context (never reused within a
+// process), or 0 when there is none yet or the driver does not offer it; with
+// 0 the caller looks the symbol address up again on every call.
+unsigned long long current_context_id() {
+  std::call_once(g_entry_once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(p);
+    p = nullptr;
+    q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(p);
+  });
+  if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+  CUcontext c = nullptr;
+  if (g_ctx_get_current(&c) != CUDA_SUCCESS || !c) return 0;
+  unsigned long long id = 0;
+  if (g_ctx_get_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
 
 // errors are reported through zsph_last_error(NULL, ...)
 int fail(int code, const std::string& m) {
@@ -91,14 +137,17 @@ int zsph_sort_index_noalloc(const zsph_gpu_param_t* gparam, int grid_num, const 
   unsigned char* base = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_base[dev]) {  // once per device, with that device current
+    const unsigned long long ctx = current_context_id();
+    if (!g_base[dev] || ctx == 0 || ctx != g_ctx[dev]) {  // once per device and context, with that device current
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_sort_scratch);
       if (e != cudaSuccess) {
+        g_base[dev] = nullptr;
         record_library_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         return ZSPH_ECUDA;
       }
       g_base[dev] = static_cast<unsigned char*>(p);
+      g_ctx[dev] = current_context_id();  // the lookup made the device's context current if it was not
     }
     base = g_base[dev];
   }
