@@ -280,13 +280,22 @@ def cpu_baseline(case, target_s: float) -> dict:
 
 
 # ---------------------------------------------------------------- learned form
+GROWTH_STEPS = 2000
+
+
 def learned_leg(args, dist, sol, stream, sptr, n, ms_plain):
-    """Learned-corrector form on the bench's case: the network is trained on
-    the GPU (own tensor-core kernels) on 200 snapshots of plain dam-break
-    steps at dx = 0.02 (every 10th of 2000 steps after 100 settling steps),
-    then the learned form runs K steps of the bench's case with the plain
-    corrector judging every 10th step (tolerance 1e-2, fallback above it)
-    and, separately, K steps without judging (the network's speed alone)."""
+    """Learned-corrector form on the bench's case and its speed/error
+    frontier.  The network is trained on the GPU (own tensor-core kernels)
+    on 200 snapshots of plain dam-break steps at dx = 0.02 (every 10th of
+    2000 steps after 100 settling steps).  Three correctors then run from the
+    same state of the bench's case (zsph_run_learned_ex): the network
+    corrector, and two correctors that skip the second search and list build
+    by walking the predictor's neighbour lists at the predicted positions,
+    one with the predictor's boundary data (lagged) and one with a fresh
+    boundary pass.  Each is timed over K steps with the plain corrector
+    judging every 10th step (tolerance 1e-2, fallback above it) and over K
+    steps unjudged, and runs 2000 judged steps (every 10th) for its error
+    growth."""
     import torch
     import zsph_b200 as z
     from zsph_b200 import cases
@@ -311,19 +320,41 @@ def learned_leg(args, dist, sol, stream, sptr, n, ms_plain):
         torch.cuda.synchronize()
         return dist.max(a.elapsed_time(b)), r
 
-    ms_j, rj = timed(lambda: sol.run_learned(net, K, judge_every=10, tol=1e-2, stream=sptr))
-    ms_u, ru = timed(lambda: sol.run_learned(net, K, judge_every=0, tol=1e-2, stream=sptr))
+    start = sol.download("old")
+    forms = {}
+    for name, corr, nt in (("network", z.CORR_NETWORK, net), ("reuse_lagged", z.CORR_REUSE_LAGGED, None),
+                           ("reuse_fresh", z.CORR_REUSE_FRESH, None)):
+        sol.upload(start)
+        ms_j, rj = timed(lambda: sol.run_learned(nt, K, judge_every=10, tol=1e-2, stream=sptr, corrector=corr))
+        sol.upload(start)
+        ms_u, ru = timed(lambda: sol.run_learned(nt, K, judge_every=0, tol=1e-2, stream=sptr, corrector=corr))
+        sol.upload(start)
+        ms_g, rg = timed(lambda: sol.run_learned(nt, GROWTH_STEPS, judge_every=10, tol=1e-2, stream=sptr,
+                                                 corrector=corr, series=GROWTH_STEPS // 10))
+        errs = rg.pop("err_series")
+        forms[name] = {
+            "ms_per_step": ms_j / K, "speedup_vs_plain": ms_plain / (ms_j / K), "run": rj,
+            "unjudged": {"ms_per_step": ms_u / K, "speedup_vs_plain": ms_plain / (ms_u / K), "run": ru},
+            "growth": {"steps": GROWTH_STEPS, "judge_every": 10, "ms_per_step": ms_g / GROWTH_STEPS,
+                       "speedup_vs_plain": ms_plain / (ms_g / GROWTH_STEPS), "run": rg,
+                       "err_at_step": {str(10 * (k + 1)): errs[k] for k in (0, 9, 49, 99, 149, 199) if k < len(errs)},
+                       "err_series_every_100_steps": errs[9::10]}}
+    sol.upload(start)
     net.close()
-    v_j, v_u = dist.world * n * K / (ms_j / 1e3), dist.world * n * K / (ms_u / 1e3)
-    return {"value": v_j, "unit": "particle-steps/s", "ms_per_step": ms_j / K,
-            "speedup_vs_plain": ms_plain / (ms_j / K), "judge_every": 10, "tol": 1e-2, "run": rj,
-            "unjudged": {"value": v_u, "ms_per_step": ms_u / K, "speedup_vs_plain": ms_plain / (ms_u / K),
-                         "run": ru},
+    ok = [k for k, f in forms.items() if f["growth"]["run"]["fallbacks"] == 0 and f["growth"]["run"]["err_max"] <= 1e-2]
+    best = max(ok, key=lambda k: forms[k]["speedup_vs_plain"]) if ok else None
+    fn = forms["network"]
+    return {"value": dist.world * n / (fn["ms_per_step"] / 1e3), "unit": "particle-steps/s",
+            "ms_per_step": fn["ms_per_step"], "speedup_vs_plain": fn["speedup_vs_plain"], "judge_every": 10,
+            "tol": 1e-2, "run": fn["run"], "unjudged": fn["unjudged"],
+            "frontier": forms, "fastest_within_tol": best,
             "train": dict(train, snapshots=snaps, data="dam break dx=0.02 (105,048 particles), plain steps 100-2100, "
                                                        "every 10th step", prep_seconds=prep_s),
-            "what": "corrector stage = predictor-stage value + (value - previous corrector value) + network "
-                    "residual; judged steps run the plain corrector, compare accelerations (relative L2, fluid) "
-                    "and keep the plain result; above tol the plain corrector runs until a judged step passes"}
+            "what": "network: corrector stage = predictor-stage value + (value - previous corrector value) + network "
+                    "residual; reuse_lagged / reuse_fresh: governing walk on the predictor's neighbour lists at the "
+                    "predicted positions with lagged / fresh boundary data (no second search or list build). Judged "
+                    "steps run the plain corrector, compare accelerations (relative L2, fluid) and keep the plain "
+                    "result; above tol the plain corrector runs until a judged step passes"}
 
 
 # ---------------------------------------------------------------- batched form

@@ -401,6 +401,25 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old_, 
                      const zsph_tmp_t* tmp, int nsteps, int judge_every, float tol, zsph_learn_run_stats_t* stats,
                      void* stream);
 
+/* Corrector forms of zsph_run_learned_ex (no reference counterpart).  All
+ * run the plain predictor sub-step.
+ *   ZSPH_CORR_NETWORK       the network corrector of zsph_run_learned (net required);
+ *   ZSPH_CORR_REUSE_LAGGED  no second search and no list build: the corrector's
+ *                           governing walk runs on the predictor's neighbour lists
+ *                           at the predicted positions (every entry re-tested
+ *                           against the exact 2h threshold), with fresh wall
+ *                           pressures and the predictor's boundary data
+ *                           (renormalised grad rho, div v) (net ignored);
+ *   ZSPH_CORR_REUSE_FRESH   the same with a fresh boundary pass on those lists.
+ * The list-reuse forms need a single scene, grid factor 1, the delta
+ * equations, absolute positions and no rigid body.  Judging and fallback as
+ * in zsph_run_learned; err_series (may be null when series_cap is 0)
+ * receives the judged relative L2 errors in order, at most series_cap. */
+enum { ZSPH_CORR_NETWORK = 0, ZSPH_CORR_REUSE_LAGGED = 1, ZSPH_CORR_REUSE_FRESH = 2 };
+int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old_, const zsph_ptc_t* new_,
+                        const zsph_tmp_t* tmp, int nsteps, int judge_every, float tol, int corrector,
+                        float* err_series, int series_cap, zsph_learn_run_stats_t* stats, void* stream);
+
 /* ---- Batched form (no reference counterpart) ------------------------------
  * One handle over nscenes independent cases (grid_size_factor 1, delta-SPH
  * equations).  Scene s owns the particles [P_s, P_s + ptc_num_s) of the
@@ -485,12 +504,28 @@ typedef struct {
   double force[3], torque[3]; /* output: the last fluid force and torque */
   double inertia[9];        /* output: body-frame inertia about the centre of mass */
 } zsph_rigid_t;
-/* Attaches the body to the handle using the particles' current positions in
+/* Attaches a body to the handle using the particles' current positions in
  * old_ (the body frame is the given orientation); sets the body particles'
- * velocities from vel and omega. */
+ * velocities from vel and omega.  Up to 16 bodies with disjoint particle
+ * ranges: a body whose first index equals an attached body's replaces it,
+ * any other is added (ZSPH_EINVAL on an overlapping range or a 17th body). */
 int zsph_rigid_attach(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_rigid_t* body, void* stream);
-/* Current body state. */
+/* Current state of the first attached body. */
 int zsph_rigid_get(zsph_handle_t* h, zsph_rigid_t* body);
+/* Number of attached bodies, and the current state of body `index` (in
+ * attach order). */
+int zsph_rigid_count(zsph_handle_t* h, int* count);
+int zsph_rigid_get_body(zsph_handle_t* h, int index, zsph_rigid_t* body);
+/* Contact of the bodies with the walls and with each other (no counterpart
+ * in the reference, whose Test_6DOF bodies never touch anything): a body
+ * particle and a non-fluid particle of the walls or of another body closer
+ * than `distance` (m, at most the 2h support; dx makes bodies touch at their
+ * surfaces) push apart along the pair's normal with
+ * max(0, stiffness (distance - r) - damping v_n) newtons, v_n the normal
+ * relative velocity; the force enters the body's FP64 force and torque sums
+ * beside the fluid's.  stiffness 0 (the default) turns contact off.
+ * Grid factor 1 only. */
+int zsph_rigid_contact(zsph_handle_t* h, double stiffness, double damping, double distance);
 
 /* Plain device-memory helpers for callers without their own CUDA runtime
  * binding (the reference driver calls cudaMalloc/cudaMemcpy directly,

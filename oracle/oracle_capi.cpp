@@ -103,7 +103,11 @@ int oracle_max_threads(void) { return omp_get_max_threads(); }
                                int wall_mode) {                                                     \
     for (int k = 0; k < nsteps; ++k) step_rigid<T>(*p, *o, *w, *t, *b, wall_mode);                  \
   }                                                                                                 \
-  void oracle_rigid_place_##SUF(const Params* p, State<T>* s, const Rigid* b) { rigid_place<T>(*p, *s, *b); }
+  void oracle_rigid_place_##SUF(const Params* p, State<T>* s, const Rigid* b) { rigid_place<T>(*p, *s, *b); } \
+  void oracle_step_rigid_bodies_##SUF(const Params* p, State<T>* o, State<T>* w, Tmp<T>* t, Rigid* b, int nb,  \
+                                      const Contact* ct, int nsteps, int wall_mode) {                  \
+    for (int k = 0; k < nsteps; ++k) step_rigid_bodies<T>(*p, *o, *w, *t, b, nb, *ct, wall_mode);    \
+  }
 
 ORACLE_INSTANCE(f32, float)
 ORACLE_INSTANCE(f64, double)

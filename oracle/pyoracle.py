@@ -93,6 +93,11 @@ class ORigid(ctypes.Structure):
                 ("r0", ctypes.POINTER(ctypes.c_double))]
 
 
+class OContact(ctypes.Structure):
+    """zsph_oracle::Contact."""
+    _fields_ = [("kn", ctypes.c_double), ("cn", ctypes.c_double), ("dist", ctypes.c_double)]
+
+
 class Oracle:
     """One oracle run (FP32 or FP64) on host arrays in the reference layout."""
 
@@ -187,9 +192,31 @@ class Oracle:
         self._fn("step_rigid")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
                                ctypes.byref(self._t), ctypes.byref(self.rigid), _I(nsteps), _I(wall_mode))
 
-    def rigid_state(self) -> dict:
-        b = self.rigid
+    def rigid_state(self, body: int = 0) -> dict:
+        b = self.rigid if body == 0 and not hasattr(self, "_bodies") else self._bodies[body]
         return {k: np.array(getattr(b, k)[:]) for k in ("x", "v", "w", "q", "F", "T")}
+
+    def attach_bodies(self, bodies, contact=(0.0, 0.0, 0.0)):
+        """Several bodies (each a dict with first, count, mass and optionally
+        vel, omega, q) and the wall/body contact (kn N/m, cn N s/m, distance m;
+        kn = 0: off), for step_bodies."""
+        n = len(bodies)
+        self._bodies = (ORigid * n)()
+        self._r0s = []
+        for k, bd in enumerate(bodies):
+            b, r0 = rigid_from(self.p, self.old, bd["first"], bd["count"], bd["mass"], bd.get("vel", (0, 0, 0)),
+                               bd.get("omega", (0, 0, 0)), bd.get("q", (1, 0, 0, 0)))
+            self._r0s.append(r0)
+            self._bodies[k] = b
+            self._bodies[k].r0 = r0.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            self._fn("rigid_place")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._bodies[k]))
+        self._contact = OContact(*[float(v) for v in contact])
+        return self._bodies
+
+    def step_bodies(self, nsteps=1, wall_mode=WALLS_FIRST):
+        self._fn("step_rigid_bodies")(ctypes.byref(self.p), ctypes.byref(self._so), ctypes.byref(self._sn),
+                                      ctypes.byref(self._t), self._bodies, _I(len(self._bodies)),
+                                      ctypes.byref(self._contact), _I(nsteps), _I(wall_mode))
 
     # simple-SPH equations (the reference's simplesph target); div(v) is the
     # scalar array self.dofv

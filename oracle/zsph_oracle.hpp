@@ -626,12 +626,35 @@ inline void rig_quat(const double* q0, const double* w, const double* qr, double
   for (int k = 0; k < 4; ++k) out[k] = r[k] * inv;
 }
 
-template <class T> void rigid_force(const Params& p, const State<T>& s, const Tmp<T>& t, Rigid& b) {
+// Contact between a body particle and a non-fluid particle that is not of
+// its own body (a wall particle or another body's): within `dist`, a
+// linear spring-dashpot along the pair's normal, kn (dist - r) - cn v_n,
+// repulsive only (clamped at zero).  kn = 0 turns contact off.
+struct Contact {
+  double kn, cn, dist;
+};
+
+// the body owning particle i (type 2, original index table[i] + i inside a
+// body's range), or -1
+template <class T> int body_of(const State<T>& s, int i, const Rigid* bodies, int nb) {
+  if (s.type[i] != 2) return -1;
+  const int id = s.table[i] + i;
+  for (int b = 0; b < nb; ++b)
+    if (id >= bodies[b].first && id < bodies[b].first + bodies[b].count) return b;
+  return -1;
+}
+
+// Force and torque of every body: the fluid's pressure force on each body
+// particle (its acceleration per unit particle mass f, times m), plus the
+// contact force of the particle's non-fluid neighbours of other bodies or
+// walls; summed in FP64 over the body's particles in particle order.
+template <class T>
+void rigid_force_all(const Params& p, const State<T>& s, const Tmp<T>& t, Rigid* bodies, int nb, const Contact& ct) {
   const T h = (T)p.h, adh = (T)p.adh, h2 = (T)p.h2, m = (T)p.m;
-  double F[3] = {0, 0, 0}, Tq[3] = {0, 0, 0};
+  std::vector<double> F((size_t)3 * nb, 0.0), Tq((size_t)3 * nb, 0.0);
   for (int i = 0; i < p.ptc_num; ++i) {
-    const int k = s.table[i] + i - b.first;
-    if (s.type[i] != 2 || k < 0 || k >= b.count) continue;
+    const int bi = body_of(s, i, bodies, nb);
+    if (bi < 0) continue;
     const T px = s.pos[3 * i], py = s.pos[3 * i + 1], pz = s.pos[3 * i + 2];
     const T r0 = s.rhop[2 * i], p0 = s.rhop[2 * i + 1];
     T f[3] = {0, 0, 0};
@@ -648,19 +671,42 @@ template <class T> void rigid_force(const Params& p, const State<T>& s, const Tm
       f[1] += vt * dy;
       f[2] += vt * dz;
     });
+    if (ct.kn > 0) {
+      const T vx = s.vel[3 * i], vy = s.vel[3 * i + 1], vz = s.vel[3 * i + 2];
+      const T d0 = (T)ct.dist, kn = (T)ct.kn, cn = (T)ct.cn;
+      for_each_candidate(p, t, i, p.grid_factor, [&](int j) {
+        if (s.type[j] == 1 || body_of(s, j, bodies, nb) == bi) return;
+        const T dx = px - s.pos[3 * j], dy = py - s.pos[3 * j + 1], dz = pz - s.pos[3 * j + 2];
+        const T r = std::sqrt(rr2_of(dx, dy, dz));
+        if (!(r < d0) || !(r > (T)0)) return;
+        const T nx = dx / r, ny = dy / r, nz = dz / r;
+        const T vn = (vx - s.vel[3 * j]) * nx + (vy - s.vel[3 * j + 1]) * ny + (vz - s.vel[3 * j + 2]) * nz;
+        T fc = kn * (d0 - r) - cn * vn;
+        if (fc < (T)0) fc = (T)0;
+        f[0] += fc * nx / m;
+        f[1] += fc * ny / m;
+        f[2] += fc * nz / m;
+      });
+    }
+    const Rigid& b = bodies[bi];
     const double fv[3] = {(double)m * f[0], (double)m * f[1], (double)m * f[2]};
     const double r[3] = {(double)px - b.x[0], (double)py - b.x[1], (double)pz - b.x[2]};
     double tq[3];
     rig_cross(r, fv, tq);
     for (int a = 0; a < 3; ++a) {
-      F[a] += fv[a];
-      Tq[a] += tq[a];
+      F[3 * bi + a] += fv[a];
+      Tq[3 * bi + a] += tq[a];
     }
   }
-  for (int a = 0; a < 3; ++a) {
-    b.F[a] = F[a];
-    b.T[a] = Tq[a];
-  }
+  for (int b = 0; b < nb; ++b)
+    for (int a = 0; a < 3; ++a) {
+      bodies[b].F[a] = F[3 * b + a];
+      bodies[b].T[a] = Tq[3 * b + a];
+    }
+}
+
+template <class T> void rigid_force(const Params& p, const State<T>& s, const Tmp<T>& t, Rigid& b) {
+  rigid_force_all(p, s, t, &b, 1, Contact{0, 0, 0});
 }
 
 inline void rigid_advance(Rigid& b, int mode, double half_dt) {
@@ -715,27 +761,34 @@ template <class T> void rigid_place(const Params& p, State<T>& s, const Rigid& b
   }
 }
 
-// One step with the body: the plain step's call order, the body's force,
-// update and placement after each sub-step's governing / integration.
-template <class T> void step_rigid(const Params& p, State<T>& o, State<T>& w, Tmp<T>& t, Rigid& b, int wall_mode) {
+// One step with the bodies: the plain step's call order, the bodies'
+// forces, updates and placements after each sub-step's governing /
+// integration.
+template <class T>
+void step_rigid_bodies(const Params& p, State<T>& o, State<T>& w, Tmp<T>& t, Rigid* bodies, int nb,
+                       const Contact& ct, int wall_mode) {
   hash(p, o, t);
   sort_index(p, t);
   sort_data(p, o, w, t);
   boundary(p, w, t, wall_mode);
   governing(p, w, t);
-  rigid_force(p, w, t, b);
-  rigid_advance(b, 1, (double)p.half_dt);
+  rigid_force_all(p, w, t, bodies, nb, ct);
+  for (int b = 0; b < nb; ++b) rigid_advance(bodies[b], 1, (double)p.half_dt);
   prediction(p, w, t);
-  rigid_place(p, w, b);
+  for (int b = 0; b < nb; ++b) rigid_place(p, w, bodies[b]);
   hash(p, w, t);
   sort_index(p, t);
   sort_data(p, w, o, t);
   boundary(p, o, t, wall_mode);
   governing(p, o, t);
-  rigid_force(p, o, t, b);
-  rigid_advance(b, 2, (double)p.half_dt);
+  rigid_force_all(p, o, t, bodies, nb, ct);
+  for (int b = 0; b < nb; ++b) rigid_advance(bodies[b], 2, (double)p.half_dt);
   correction(p, o, t);
-  rigid_place(p, o, b);
+  for (int b = 0; b < nb; ++b) rigid_place(p, o, bodies[b]);
+}
+
+template <class T> void step_rigid(const Params& p, State<T>& o, State<T>& w, Tmp<T>& t, Rigid& b, int wall_mode) {
+  step_rigid_bodies(p, o, w, t, &b, 1, Contact{0, 0, 0}, wall_mode);
 }
 
 }  // namespace zsph_oracle

@@ -95,3 +95,58 @@ def test_untrained_network_falls_back():
     assert np.all(np.isfinite(st.pos))
     net.close()
     sol.close()
+
+
+def _by_id(st):
+    ids = st.table + np.arange(len(st.table), dtype=np.int32)
+    order = np.empty_like(ids)
+    order[ids] = np.arange(len(ids), dtype=np.int32)
+    return order
+
+
+def test_list_reuse_fresh_corrector_matches_the_plain_corrector():
+    """The corrector on the predictor's neighbour lists with a fresh boundary
+    pass evaluates the plain corrector's equations at the predicted state;
+    it differs only where a pair crossed the 2h radius during the half step
+    (the lists miss pairs that entered, whose kernel weight is near zero) and
+    in summation order.  Judged on every step, its accelerations agree with
+    the plain corrector's to well below the 1e-2 tolerance."""
+    c, sol = _moving_state(0.04, 60)
+    r = sol.run_learned(None, 20, judge_every=1, tol=1e-2, corrector=z.CORR_REUSE_FRESH, series=20)
+    print("fresh", r)
+    assert r["judged"] == 20 and r["fallbacks"] == 0 and len(r["err_series"]) == 20
+    assert 0 < r["err_max"] < 1e-3
+    assert sol.status() == 0
+    sol.close()
+
+
+def test_list_reuse_correctors_track_the_plain_run():
+    """Unjudged runs of both list-reuse correctors stay close to the plain
+    run by particle id (the lagged form further away than the fresh one), and
+    the lagged form's judged error is reported honestly (nonzero)."""
+    c, base = _moving_state(0.04, 60)
+    start = base.download("old")
+    base.run(30)
+    ref = base.download("old")
+    base.close()
+    errs = {}
+    for corr in (z.CORR_REUSE_FRESH, z.CORR_REUSE_LAGGED):
+        sol = z.Solver.from_case(c)
+        sol.upload(start)
+        r = sol.run_learned(None, 30, judge_every=0, tol=1e-2, corrector=corr)
+        assert r["learned"] == 30 and r["judged"] == 0
+        st = sol.download("old")
+        assert sol.status() == 0
+        a, b = _by_id(st), _by_id(ref)
+        fl = ref.type[b] == 1
+        errs[corr] = float(np.abs(st.pos[a][fl] - ref.pos[b][fl]).max())
+        sol.close()
+    print("max |x - x_plain| after 30 steps:", errs)
+    assert errs[z.CORR_REUSE_FRESH] < 1e-5
+    assert errs[z.CORR_REUSE_FRESH] <= errs[z.CORR_REUSE_LAGGED] < 1e-3
+    sol = z.Solver.from_case(c)
+    sol.upload(start)
+    r = sol.run_learned(None, 10, judge_every=2, tol=1.0, corrector=z.CORR_REUSE_LAGGED, series=5)
+    print("lagged", r)
+    assert r["judged"] == 5 and 0 < r["err_max"] < 1.0
+    sol.close()

@@ -213,3 +213,94 @@ def test_floating_body_against_fp64_checker():
     print("config2 comparison", json.dumps(r))
     assert r["precision"]["pos"]["rms"] <= r["plain"]["pos"]["rms"]
     assert r["precision"]["heave_max_diff"] < 2e-3 and r["plain"]["heave_max_diff"] < 2e-3
+
+
+# ---- several bodies and contact ---------------------------------------------
+
+def _contact_for(body, dx, n_bottom, sag=0.05, zeta=0.5, g=9.81):
+    """Spring-dashpot constants: the body's weight carried by n_bottom pairs at
+    a static penetration of sag * dx, damped at zeta of critical."""
+    kn = body["mass"] * g / (n_bottom * sag * dx)
+    cn = zeta * 2.0 * np.sqrt(kn * n_bottom * body["mass"]) / n_bottom
+    return kn, cn
+
+
+@pytest.mark.parametrize("precise", [False, True])
+def test_two_floating_bodies_match_fp64_oracle(precise):
+    """Two cubes of different densities dropped from different heights into
+    the same tank: each body's heave follows the FP64 oracle run of the same
+    equations (per-body FP64 force and torque sums, one update per body)."""
+    dx = 0.04
+    c = cases.floating_bodies(dx, cubes=[dict(x=1.0, size=0.2, rho=500.0, bottom=0.55),
+                                         dict(x=2.6, size=0.2, rho=800.0, bottom=0.62)], end_step=1000)
+    o = po.Oracle(c.json, _exact_state(c), dtype=np.float64)
+    o.attach_bodies(c.bodies)
+    s = _solver(c, precise)
+    for b in c.bodies:
+        s.attach_body(b["first"], b["count"], b["mass"])
+    assert s.body_count() == 2
+    got, want = [[], []], [[], []]
+    for _ in range(8):
+        o.step_bodies(50)
+        s.run(50)
+        for k in range(2):
+            got[k].append(s.body(k)["pos"][2])
+            want[k].append(o.rigid_state(k)["x"][2])
+    got, want = np.array(got), np.array(want)
+    print("heave", got.round(5), "oracle", want.round(5))
+    assert np.max(np.abs(got - want)) < 2e-3
+    assert s.body(1)["pos"][2] < s.body(0)["pos"][2] + 0.07  # the denser cube sits deeper
+    assert all(s.body(k)["force"][2] > 0 for k in range(2))
+    s.close()
+
+
+def test_stacked_bodies_rest_on_the_floor_with_contact():
+    """Empty tank, two cubes dropped one above the other, contact on: the
+    lower cube lands on the floor, the upper one on the lower, and both come
+    to rest; the trajectories follow the FP64 oracle and the resting heights
+    are those of the springs' static penetration (the lower contact carries
+    both weights)."""
+    dx = 0.04
+    c = cases.floating_bodies(dx, tank=(0.6, 0.6, 0.6), depth=0.0,
+                              cubes=[dict(x=0.3, size=0.2, rho=500.0, bottom=0.08),
+                                     dict(x=0.3, size=0.2, rho=500.0, bottom=0.36)], end_step=10)
+    kn, cn = _contact_for(c.bodies[0], dx, 25)
+    o = po.Oracle(c.json, c.state, dtype=np.float64)
+    o.attach_bodies(c.bodies, contact=(kn, cn, dx))
+    s = z.Solver.from_case(c)
+    for b in c.bodies:
+        s.attach_body(b["first"], b["count"], b["mass"])
+    s.set_contact(kn, cn, dx)
+    diff = 0.0
+    for _ in range(20):
+        o.step_bodies(100)
+        s.run(100)
+        for k in range(2):
+            diff = max(diff, abs(s.body(k)["pos"][2] - o.rigid_state(k)["x"][2]))
+    lo, hi = s.body(0), s.body(1)
+    print("resting", lo["pos"], hi["pos"], "max |gpu - oracle| heave", diff)
+    sag = dx * 0.05
+    want_lo = -dx / 2 + dx - 2 * sag + (0.2 - dx) / 2  # the floor contact carries both cubes
+    want_hi = want_lo + 0.2 - sag                        # one cube's weight on the contact between them
+    assert abs(lo["pos"][2] - want_lo) < 0.1 * dx and abs(hi["pos"][2] - want_hi) < 0.1 * dx
+    assert np.linalg.norm(lo["vel"]) < 0.02 and np.linalg.norm(hi["vel"]) < 0.02
+    assert diff < 2e-3
+    s.close()
+
+
+def test_body_api_rejects_overlap_and_bad_contact():
+    dx = 0.04
+    c = cases.floating_bodies(dx, tank=(0.6, 0.6, 0.6), depth=0.0,
+                              cubes=[dict(x=0.3, size=0.2, rho=500.0, bottom=0.1)], end_step=10)
+    s = z.Solver.from_case(c)
+    b = c.bodies[0]
+    with pytest.raises(z.ZsphError):
+        s.set_contact(1.0, 0.0, dx)  # no body yet
+    s.attach_body(b["first"], b["count"], b["mass"])
+    with pytest.raises(z.ZsphError):
+        s.attach_body(b["first"] + 3, 10, 1.0)  # overlaps the first body
+    with pytest.raises(z.ZsphError):
+        s.set_contact(1.0, 0.0, 3 * dx)  # beyond the 2h support
+    s.attach_body(b["first"], b["count"], 2 * b["mass"])  # same first index: replaces
+    assert s.body_count() == 1 and s.body(0)["mass"] == 2 * b["mass"]
+    s.close()

@@ -47,3 +47,37 @@ def test_torque_free_cube_spins_uniformly():
     assert np.allclose(r["w"], w, atol=1e-12)  # isotropic inertia: no gyroscopic term
     angle = 2 * np.arctan2(np.linalg.norm(r["q"][1:]), r["q"][0])
     assert abs(angle - np.linalg.norm(w) * t) < 1e-6
+
+
+def _contact_for(body, dx, n_bottom, sag=0.05, zeta=0.5, g=9.81):
+    """Spring-dashpot constants: the body's weight carried by n_bottom pairs at
+    a static penetration of sag * dx, damped at zeta of critical."""
+    kn = body["mass"] * g / (n_bottom * sag * dx)
+    cn = zeta * 2.0 * np.sqrt(kn * n_bottom * body["mass"]) / n_bottom
+    return kn, cn
+
+
+def test_cube_settles_on_the_floor_with_contact():
+    """Empty tank, one cube dropped 0.1 m: with contact it comes to rest on
+    the floor at the spring's static penetration (each of the 25 bottom
+    particles carries 1/25 of the weight against the wall particle right
+    below it); without contact it falls through."""
+    dx = 0.04
+    c = cases.floating_bodies(dx, tank=(0.6, 0.6, 0.6), depth=0.0,
+                              cubes=[dict(x=0.3, size=0.2, rho=500.0, bottom=0.1)], end_step=10)
+    b = c.bodies[0]
+    kn, cn = _contact_for(b, dx, 25)
+    o = po.Oracle(c.json, c.state, dtype=np.float64)
+    o.attach_bodies([b], contact=(kn, cn, dx))
+    o.step_bodies(1500)
+    r = o.rigid_state(0)
+    # bottom particles at z = -dx/2 + dx - sag*dx, centre (0.2 - dx)/2 above them
+    want = -dx / 2 + dx * (1 - 0.05) + (0.2 - dx) / 2
+    print("resting centre", r["x"], "expected z", want, "v", r["v"])
+    assert abs(r["x"][2] - want) < 0.1 * dx
+    assert np.linalg.norm(r["v"]) < 0.02
+    assert abs(r["F"][2] - b["mass"] * 9.81) < 0.05 * b["mass"] * 9.81  # the floor carries the weight
+    o2 = po.Oracle(c.json, c.state, dtype=np.float64)
+    o2.attach_bodies([b])
+    o2.step_bodies(700)
+    assert o2.rigid_state(0)["x"][2] < 0.0  # no contact: through the floor

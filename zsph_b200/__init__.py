@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libzsph_b200.so")
 
 ZSPH_OK, ZSPH_EINVAL, ZSPH_ECUDA, ZSPH_ENAN, ZSPH_ETIMEOUT, ZSPH_EIO, ZSPH_ENOMEM = range(7)
 EQ_DELTA, EQ_SIMPLE = 0, 1
+CORR_NETWORK, CORR_REUSE_LAGGED, CORR_REUSE_FRESH = 0, 1, 2
 FLAG_NAN, FLAG_KILLED, FLAG_NB_OVERFLOW, FLAG_BAD_KEY = 1, 2, 4, 8
 _CODES = {0: "ZSPH_OK", 1: "ZSPH_EINVAL", 2: "ZSPH_ECUDA", 3: "ZSPH_ENAN", 4: "ZSPH_ETIMEOUT", 5: "ZSPH_EIO",
           6: "ZSPH_ENOMEM"}
@@ -234,12 +235,17 @@ _sig = {
     "zsph_learn_train": (_I, [_HP, _VP, _I, _I, _F, ctypes.c_ulonglong, _F, ctypes.POINTER(LearnTrainStats), _VP]),
     "zsph_run_learned": (_I, [_HP, _VP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _F,
                               ctypes.POINTER(LearnRunStats), _VP]),
+    "zsph_run_learned_ex": (_I, [_HP, _VP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _F,
+                                 _I, _VP, _I, ctypes.POINTER(LearnRunStats), _VP]),
     "zsph_set_precision": (_I, [_HP, _I]),
     "zsph_precise_load": (_I, [_HP, ctypes.POINTER(Ptc), _VP, _VP]),
     "zsph_precise_positions": (_I, [_HP, ctypes.POINTER(Ptc), _VP, _VP]),
     "zsph_conservation": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Conservation), _VP]),
     "zsph_rigid_attach": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(RigidBody), _VP]),
     "zsph_rigid_get": (_I, [_HP, ctypes.POINTER(RigidBody)]),
+    "zsph_rigid_count": (_I, [_HP, _IP]),
+    "zsph_rigid_get_body": (_I, [_HP, _I, ctypes.POINTER(RigidBody)]),
+    "zsph_rigid_contact": (_I, [_HP, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     "zsph_create_batch": (_I, [ctypes.POINTER(GpuParam), _IP, _I, ctypes.POINTER(_HP)]),
     "zsph_autotune": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I,
                            ctypes.POINTER(TuneResult), _VP]),
@@ -571,12 +577,21 @@ class Solver:
         b.first, b.count, b.mass = int(first), int(count), float(mass)
         b.vel[:], b.omega[:], b.q[:] = list(map(float, vel)), list(map(float, omega)), list(map(float, q))
         self._call(lib.zsph_rigid_attach, ctypes.byref(self.old), ctypes.byref(b), None)
-        return self.body()
+        return self.body(self.body_count() - 1 if self.body_count() else 0)
 
-    def body(self) -> dict:
+    def body(self, index: int = 0) -> dict:
         b = RigidBody()
-        self._call(lib.zsph_rigid_get, ctypes.byref(b))
+        self._call(lib.zsph_rigid_get_body, int(index), ctypes.byref(b))
         return _as_dict(b)
+
+    def body_count(self) -> int:
+        n = ctypes.c_int(0)
+        self._call(lib.zsph_rigid_count, ctypes.byref(n))
+        return n.value
+
+    def set_contact(self, stiffness: float, damping: float, distance: float) -> None:
+        """zsph_rigid_contact: body-wall and body-body contact (stiffness 0: off)."""
+        self._call(lib.zsph_rigid_contact, float(stiffness), float(damping), float(distance))
 
     # ---- learned-corrector form (zsph_learn_*, zsph_run_learned) ----------
     def feature_scales(self) -> np.ndarray:
@@ -609,11 +624,25 @@ class Solver:
                    ctypes.byref(st), stream)
         return _as_dict(st)
 
-    def run_learned(self, net: "Mlp", nsteps: int, judge_every: int = 10, tol: float = 1e-2, stream=None) -> dict:
+    def run_learned(self, net: "Mlp | None", nsteps: int, judge_every: int = 10, tol: float = 1e-2, stream=None,
+                    corrector: int = None, series: int = 0) -> dict:
+        """zsph_run_learned (network corrector), or zsph_run_learned_ex with
+        `corrector` (CORR_*); with series > 0 the result also holds the first
+        `series` judged errors under "err_series"."""
         st = LearnRunStats()
-        self._call(lib.zsph_run_learned, net.h, ctypes.byref(self.old), ctypes.byref(self.new),
-                   ctypes.byref(self.tmp), int(nsteps), int(judge_every), float(tol), ctypes.byref(st), stream)
-        return _as_dict(st)
+        if corrector is None and not series:
+            self._call(lib.zsph_run_learned, net.h, ctypes.byref(self.old), ctypes.byref(self.new),
+                       ctypes.byref(self.tmp), int(nsteps), int(judge_every), float(tol), ctypes.byref(st), stream)
+            return _as_dict(st)
+        errs = np.zeros(max(int(series), 1), np.float32)
+        self._call(lib.zsph_run_learned_ex, net.h if net is not None else None, ctypes.byref(self.old),
+                   ctypes.byref(self.new), ctypes.byref(self.tmp), int(nsteps), int(judge_every), float(tol),
+                   CORR_NETWORK if corrector is None else int(corrector), _ptr(errs) if series else None,
+                   int(series), ctypes.byref(st), stream)
+        out = _as_dict(st)
+        if series:
+            out["err_series"] = errs[:min(out["judged"], int(series))].tolist()
+        return out
 
 
 # ---- device-memory helpers through the library's own C ABI ----------------

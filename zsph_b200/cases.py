@@ -34,6 +34,7 @@ class Case:
     name: str
     pos64: np.ndarray | None = None  # exact (FP64) positions, for the precision form
     body: dict | None = None         # rigid body: first, count, mass (floating-body case)
+    bodies: list | None = None       # every rigid body of the case (floating_bodies)
 
     @property
     def n(self) -> int:
@@ -114,6 +115,20 @@ def floating_body(dx: float = 0.01, tank=(4.0, 1.0, 1.0), depth: float = 0.5, cu
     (cube_x, tank_y/2) with its bottom `drop` above the surface.  dx = 0.01
     gives 2,000,000 fluid, 432,708 wall and 8,000 body particles.  Order:
     fluid, walls, body; case.body = {first, count, mass}."""
+    c = floating_bodies(dx, tank, depth, [dict(x=cube_x, size=cube, rho=body_rho, bottom=depth + drop)],
+                        layers, cfl, end_step, **phys)
+    c.name = f"floating_body_dx{dx:g}"
+    return c
+
+
+def floating_bodies(dx: float, tank=(4.0, 1.0, 1.0), depth: float = 0.5, cubes=(), layers: int = 3,
+                    cfl: float = 0.2, end_step: int = 5000, **phys) -> Case:
+    """Still water of the given depth (0: an empty tank) and several cubes of
+    type 2 particles on the fluid's lattice.  Each cube is a dict with its
+    centre x (and optionally y, default the tank's middle), side `size`,
+    density `rho` and the height of its bottom face `bottom`.  Order: fluid,
+    walls, then the cubes one after another; case.bodies lists each cube's
+    {first, count, mass} and case.body is the first one."""
     g = phys.get("g", -9.81)
     rho0 = phys.get("rho0", 1000.0)
     cs_factor = phys.get("cs_factor", 10.0)
@@ -128,10 +143,17 @@ def floating_body(dx: float = 0.01, tank=(4.0, 1.0, 1.0), depth: float = 0.5, cu
     ii, jj, kk = ii.ravel(), jj.ravel(), kk.ravel()
     outside = (ii < 0) | (ii >= tx) | (jj < 0) | (jj >= ty) | (kk < 0)
     pos_w = (np.stack([ii[outside], jj[outside], kk[outside]], axis=1).astype(np.float64) + 0.5) * dx
-    nc = int(round(cube / dx))
-    a, b, c = np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij")
-    corner = np.array([cube_x - cube / 2, ly / 2 - cube / 2, depth + drop])
-    pos_b = corner + (np.stack([a.ravel(), b.ravel(), c.ravel()], axis=1).astype(np.float64) + 0.5) * dx
+    blocks, bodies = [], []
+    first = len(pos_f) + len(pos_w)
+    for cb in cubes:
+        side = cb["size"]
+        nc = int(round(side / dx))
+        a, b, c = np.meshgrid(np.arange(nc), np.arange(nc), np.arange(nc), indexing="ij")
+        corner = np.array([cb["x"] - side / 2, cb.get("y", ly / 2) - side / 2, cb["bottom"]])
+        blocks.append(corner + (np.stack([a.ravel(), b.ravel(), c.ravel()], axis=1).astype(np.float64) + 0.5) * dx)
+        bodies.append({"first": first, "count": nc ** 3, "mass": cb["rho"] * side ** 3})
+        first += nc ** 3
+    pos_b = np.concatenate(blocks) if blocks else np.zeros((0, 3))
     c0 = cs_factor * math.sqrt(abs(g) * lz)
     H = nz * dx
 
@@ -156,8 +178,10 @@ def floating_body(dx: float = 0.01, tank=(4.0, 1.0, 1.0), depth: float = 0.5, cu
     dt = cfl * h / c0
     js = _json(dx, lx, ly, lz, dt, n, len(pos_f), len(pos_w), end_step, **phys)
     js.rigid_ptc_num = len(pos_b)
-    body = {"first": len(pos_f) + len(pos_w), "count": len(pos_b), "mass": body_rho * cube ** 3}
-    return Case(js, st, len(pos_f), len(pos_w), f"floating_body_dx{dx:g}", pos64=pos64, body=body)
+    c = Case(js, st, len(pos_f), len(pos_w), f"floating_bodies_dx{dx:g}", pos64=pos64,
+             body=bodies[0] if bodies else None)
+    c.bodies = bodies
+    return c
 
 
 def config2() -> Case:

@@ -137,7 +137,7 @@ cudaError_t substep(zsph_handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to
   cudaError_t e = launch_search(h->kp, h->s, h->tiles, from, to, t, st, pf);
   if (!e) e = launch_boundary(h->kp, h->s, to, t, st, pf);
   if (!e) e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf, feat);
-  if (!e && h->rigid && mode != 0) e = rigid_substep(h, from, to, mode, st);
+  if (!e && h->rigid && mode != 0) e = rigid_substep(h, from, to, t, mode, st);
   return e;
 }
 

@@ -606,7 +606,10 @@ template <int GF> struct PairSmem {
 
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
-template <int GF, bool PRECISE = false, bool BATCH = false>
+// REUSE (learned form's corrector variants): the lists were built at an
+// earlier state of the same sorted order, so every entry is tested again
+// against the exact threshold at the current positions and skipped beyond it.
+template <int GF, bool PRECISE = false, bool BATCH = false, bool REUSE = false>
 __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
   extern __shared__ __align__(16) unsigned char dsm[];
   PairSmem<GF> sm(dsm);
@@ -638,6 +641,9 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   float sx = 0.f, sy = 0.f, sz = 0.f;
   auto use1 = [&](const NbB1& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
+    if constexpr (REUSE) {
+      if (!interacts(kp, dist2(dx, dy, dz))) return;
+    }
     const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
     const float a = 1.0f - 0.5f * q;
     const float fr = c_fr * (a * a * a);
@@ -718,8 +724,9 @@ struct FeatAcc {
 // PRECISE: precision form (cell + offset positions).
 // MINB: minimum resident CTAs per SM (register budget); the default six
 // give 80 registers without spills for the plain variants.
+// REUSE: as k_boundary's (entries re-tested at the current positions).
 template <int GF, int MODE, bool FEAT = false, bool PRECISE = false, bool BATCH = false, bool RIGID = false,
-          int MINB = (FEAT || BATCH) ? 1 : 6>
+          int MINB = (FEAT || BATCH) ? 1 : 6, bool REUSE = false>
 __global__ void __launch_bounds__(kPairBlock, MINB)
     k_governing(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t, zsph_ptc_t out, FeatOut fo) {
   extern __shared__ __align__(16) unsigned char dsm[];
@@ -754,6 +761,9 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
   auto use = [&](const NbG& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
     const float rr2 = dist2(dx, dy, dz);
+    if constexpr (REUSE) {
+      if (!interacts(kp, rr2)) return;
+    }
     const float dvdx = (vi.x - nb.vp.x) * dx + (vi.y - nb.vp.y) * dy + (vi.z - nb.vp.z) * dz;
     const float q = sqrt_fast(rr2) * inv_h;
     const float a = 1.0f - 0.5f * q;
@@ -1091,6 +1101,117 @@ cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, 
   return cudaGetLastError();
 }
 
+// Learned form's corrector variants: wall (rho, p) of every non-fluid
+// particle at the current (predicted) positions, from the fluid neighbours of
+// its boundary rows in the lists the predictor built (delta_ns.cu:61-85,
+// :116-131), each entry tested again against the exact threshold; summed in
+// the lists' visit order and published in the packed shadows, and in
+// ptc.rhop when no boundary pass follows (which would otherwise write it).
+template <int GF>
+__global__ void __launch_bounds__(kPairBlock) k_walls_reuse(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
+                                                            int write_rhop) {
+  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  if (i >= kp.n) return;
+  const float4 pi = s.sh.pr(i);
+  if (fluid_of(pi.w)) return;
+  const int c = t.hash[i];
+  const int cnt = s.nb_cnt[i];
+  float rsum = 0.0f, wsum = 0.0f;
+  auto visit = [&](int j) {
+    const float4 pj = s.sh.pr(j);
+    if (!fluid_of(pj.w) || !interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) return;
+    wall_term(kp, s, pi, j, rsum, wsum);
+  };
+  if (cnt != kOverflow) {
+    for (int k = 0; k < cnt; ++k) {
+      const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
+      const int r = (int)(e >> kRowShift);
+      if (!Stencil<GF>::boundary_row(r)) continue;
+      int a, b;
+      row_range<GF>(kp, t, c, r, a, b);
+      const int j = a + (int)(e & kOffMask);
+      if (j < b) visit(j);
+    }
+  } else {
+    for (int r = 0; r < Stencil<GF>::NR; ++r) {
+      if (!Stencil<GF>::boundary_row(r)) continue;
+      int a, b;
+      row_range<GF>(kp, t, c, r, a, b);
+      for (int j = a; j < b; ++j)
+        if (j != i) visit(j);
+    }
+  }
+  const zsph_gpu_param_t& p = kp.p;
+  if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+  if (rsum < 0.0f) rsum = 0.0f;
+  const float rho = rsum / p.cs2 + p.rho0;
+  s.sh.pr(i).w = -rho;  // still non-fluid
+  s.sh.vp(i).w = rsum;
+  if (write_rhop) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(rho, rsum);
+}
+
+// Rigid-body contact (see launch_rigid_contact): one thread per particle,
+// body particles only; the neighbours come from the particle's list (all
+// stencil rows, visit order), the non-fluid ones of another body or of the
+// walls within `dist` push back along the pair's normal.
+__device__ __forceinline__ int body_range_of(const zsph_ptc_t& ptc, const BodyRange* br, int nb, int i) {
+  if (ptc.type[i] != 2) return -1;
+  const int id = ptc.table[i] + i;
+  for (int b = 0; b < nb; ++b)
+    if (id >= br[b].first && id < br[b].first + br[b].count) return b;
+  return -1;
+}
+
+template <int GF, bool PRECISE>
+__global__ void __launch_bounds__(kPairBlock) k_rigid_contact(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
+                                                              const BodyRange* br, int nb, float kn, float cn,
+                                                              float dist) {
+  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+  if (i >= kp.n) return;
+  const int bi = body_range_of(ptc, br, nb, i);
+  if (bi < 0) return;
+  const int3 ci = PRECISE ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
+  const ShadowRec own = s.sh.load(i);
+  const float inv_m = 1.0f / kp.p.m;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  auto visit = [&](int j) {
+    if (ptc.type[j] == 1 || body_range_of(ptc, br, nb, j) == bi) return;
+    const ShadowRec o = shadow_rec<PRECISE>(kp, s, j, ci);
+    const float dx = own.pr.x - o.pr.x, dy = own.pr.y - o.pr.y, dz = own.pr.z - o.pr.z;
+    const float r = __fsqrt_rn(dist2(dx, dy, dz));
+    if (!(r < dist) || !(r > 0.f)) return;
+    const float nx = dx / r, ny = dy / r, nz = dz / r;
+    const float vn = (own.vp.x - o.vp.x) * nx + (own.vp.y - o.vp.y) * ny + (own.vp.z - o.vp.z) * nz;
+    const float fc = fmaxf(kn * (dist - r) - cn * vn, 0.f) * inv_m;
+    fx += fc * nx;
+    fy += fc * ny;
+    fz += fc * nz;
+  };
+  const int c = t.hash[i];
+  const int cnt = s.nb_cnt[i];
+  if (cnt != kOverflow) {
+    for (int k = 0; k < cnt; ++k) {
+      const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
+      int a, b;
+      row_range<GF>(kp, t, c, (int)(e >> kRowShift), a, b);
+      const int j = a + (int)(e & kOffMask);
+      if (j < b) visit(j);
+    }
+  } else {
+    for (int r = 0; r < Stencil<GF>::NR; ++r) {
+      int a, b;
+      row_range<GF>(kp, t, c, r, a, b);
+      for (int j = a; j < b; ++j)
+        if (j != i) visit(j);
+    }
+  }
+  float4 f = kp.rigid_f[i];
+  f.x += fx;
+  f.y += fy;
+  f.z += fz;
+  kp.rigid_f[i] = f;
+}
+
 // Neighbour counts from the lists: governing stencil and boundary subset
 // (-1 for a particle whose list overflowed).
 template <int GF>
@@ -1171,6 +1292,33 @@ cudaError_t launch_integrate(const KParams& kp, const Scratch& s, const zsph_ptc
   const int nb = (kp.n + kSearchBlock - 1) / kSearchBlock;
   if (correction) k_integrate<2><<<nb, kSearchBlock, 0, st>>>(kp, ptc, t);
   else k_integrate<1><<<nb, kSearchBlock, 0, st>>>(kp, ptc, t);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_corrector_reuse(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                                  bool fresh_boundary, int mode, cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.rigid_f || kp.stage_windows ||
+      kp.equations != ZSPH_EQ_DELTA || (mode != 0 && mode != 2))
+    return cudaErrorInvalidValue;
+  cudaError_t e = launch_pack_shadows(kp, s, ptc, st);
+  if (e) return e;
+  const int nb = thread_blocks(kp.n), sm = pair_smem<1>(0, 0);
+  k_walls_reuse<1><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, fresh_boundary ? 0 : 1);
+  if (fresh_boundary) k_boundary<1, false, false, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t);
+  const FeatOut none{};
+  if (mode == 2) k_governing<1, 2, false, false, false, false, 1, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, ptc, none);
+  else k_governing<1, 0, false, false, false, false, 1, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t, ptc, none);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rigid_contact(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                                 const BodyRange* ranges, int nb, float kn, float cn, float dist, cudaStream_t st) {
+  if (kp.n == 0 || nb == 0) return cudaSuccess;
+  if (kp.p.grid_factor != 1 || kp.scenes || !kp.rigid_f) return cudaErrorInvalidValue;
+  const int blocks = thread_blocks(kp.n);
+  if (kp.c3o) k_rigid_contact<1, true><<<blocks, kPairBlock, 0, st>>>(kp, s, ptc, t, ranges, nb, kn, cn, dist);
+  else k_rigid_contact<1, false><<<blocks, kPairBlock, 0, st>>>(kp, s, ptc, t, ranges, nb, kn, cn, dist);
   return cudaGetLastError();
 }
 

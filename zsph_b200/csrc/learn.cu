@@ -198,6 +198,24 @@ __global__ void k_judge(int n, const int* index, const float4* acc_c, const floa
   block_sum_to(v, out);
 }
 
+// Judge of the list-reuse correctors: their corrector-stage accelerations
+// (predictor order) against the plain corrector's (corrector order t,
+// particle index[t]), fluid particles.
+__global__ void k_judge_acc(int n, const int* index, const float4* acc_c, const float4* acc_v, const int* type,
+                            double* out) {
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    if (type[t] != 1) continue;
+    const float4 c = acc_c[t], a = acc_v[index[t]];
+    const double ex = (double)a.x - c.x, ey = (double)a.y - c.y, ez = (double)a.z - c.z, ew = (double)a.w - c.w;
+    v[0] += ex * ex + ey * ey + ez * ez;
+    v[1] += (double)c.x * c.x + (double)c.y * c.y + (double)c.z * c.z;
+    v[4] += ew * ew;
+    v[5] += (double)c.w * c.w;
+  }
+  block_sum_to(v, out);
+}
+
 uint64_t mix64(uint64_t& s) {
   uint64_t z = (s += 0x9E3779B97F4A7C15ull);
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -576,31 +594,49 @@ int zsph_learn_train(zsph_handle_t* h, zsph_mlp_t* net, int epochs, int batch_ti
 int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, const zsph_ptc_t* w,
                      const zsph_tmp_t* t, int nsteps, int judge_every, float tol, zsph_learn_run_stats_t* out,
                      void* stream) {
+  return zsph_run_learned_ex(h, net, o, w, t, nsteps, judge_every, tol, ZSPH_CORR_NETWORK, nullptr, 0, out, stream);
+}
+
+int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, const zsph_ptc_t* w,
+                        const zsph_tmp_t* t, int nsteps, int judge_every, float tol, int corrector,
+                        float* err_series, int series_cap, zsph_learn_run_stats_t* out, void* stream) {
   if (int rc = check_buffers(h, o, w, t, "zsph_run_learned")) return rc;
-  if (!net || nsteps < 0 || judge_every < 0 || !(tol > 0.f))
-    return set_herr(h, ZSPH_EINVAL, "zsph_run_learned: bad network / nsteps / judge_every / tol");
+  const bool network = corrector == ZSPH_CORR_NETWORK;
+  if (corrector < ZSPH_CORR_NETWORK || corrector > ZSPH_CORR_REUSE_FRESH)
+    return set_herr(h, ZSPH_EINVAL, "zsph_run_learned: unknown corrector");
+  if ((network && !net) || nsteps < 0 || judge_every < 0 || !(tol > 0.f) || series_cap < 0 ||
+      (series_cap > 0 && !err_series))
+    return set_herr(h, ZSPH_EINVAL, "zsph_run_learned: bad network / nsteps / judge_every / tol / error series");
+  if (!network && (h->kp.p.grid_factor != 1 || h->kp.scenes || h->kp.c3o || h->rigid || h->kp.stage_windows ||
+                   h->kp.equations != ZSPH_EQ_DELTA))
+    return set_herr(h, ZSPH_EINVAL,
+                    "zsph_run_learned: the list-reuse correctors need a single scene, grid factor 1, the delta "
+                    "equations, absolute positions, no rigid body and no staged windows");
   if (int rc = ensure_state(h)) return rc;
   LearnState* L = h->learn;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   h->last_stream = st;
   const Units u = units_of(h->kp);
   const float4 un = u.target_unit();
-  const float4 oa = make_float4(net->out_std[0] * un.x, net->out_std[1] * un.y, net->out_std[2] * un.z,
-                                net->out_std[3] * un.w);
-  const float4 ob = make_float4(net->out_mean[0] * un.x, net->out_mean[1] * un.y, net->out_mean[2] * un.z,
-                                net->out_mean[3] * un.w);
+  float4 oa = make_float4(0.f, 0.f, 0.f, 0.f), ob = oa;
+  if (network) {
+    oa = make_float4(net->out_std[0] * un.x, net->out_std[1] * un.y, net->out_std[2] * un.z, net->out_std[3] * un.w);
+    ob = make_float4(net->out_mean[0] * un.x, net->out_mean[1] * un.y, net->out_mean[2] * un.z,
+                     net->out_mean[3] * un.w);
+  }
   FeatOut fo = make_feat(h, net);
   fo.tiles = L->tiles;
   FeatOut fj = fo;
   fj.acc_copy = L->acc_n;
+  const bool fresh = corrector == ZSPH_CORR_REUSE_FRESH;
   zsph_learn_run_stats_t rs{};
   double err_sum = 0;
   bool plain = false;
   const size_t acc_bytes = sizeof(float4) * h->kp.n;
   for (int s = 0; s < nsteps; ++s) {
     const bool judged = judge_every > 0 && (s + 1) % judge_every == 0;
-    // the first step has no previous corrector value of its own: plain
-    if (s == 0 && !judged) {
+    // the network's first step has no previous corrector value of its own: plain
+    if (network && s == 0 && !judged) {
       LCHECK(h, "zsph_run_learned plain", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
       LCHECK(h, "zsph_run_learned plain", run_substep(h, *o, *w, *t, 2, st, nullptr, nullptr));
       rs.plain += 1;
@@ -608,14 +644,28 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, con
       continue;
     }
     if (judged) {
-      LCHECK(h, "zsph_run_learned copy", cudaMemcpyAsync(L->acc_prev, t->acc_drhodt, acc_bytes,
-                                                         cudaMemcpyDeviceToDevice, st));
-      LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, &fj));
-      LCHECK(h, "zsph_run_learned network", launch_mlp_forward(*net, L->tiles, h->kp.n,
-                                                               reinterpret_cast<float*>(L->yhat), h->s.flags, st));
+      if (network) {
+        LCHECK(h, "zsph_run_learned copy", cudaMemcpyAsync(L->acc_prev, t->acc_drhodt, acc_bytes,
+                                                           cudaMemcpyDeviceToDevice, st));
+        LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, &fj));
+        LCHECK(h, "zsph_run_learned network", launch_mlp_forward(*net, L->tiles, h->kp.n,
+                                                                 reinterpret_cast<float*>(L->yhat), h->s.flags, st));
+      } else {
+        // the variant's corrector-stage values (not applied), in the predictor's order
+        LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
+        LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 0, st));
+        LCHECK(h, "zsph_run_learned copy", cudaMemcpyAsync(L->yhat, t->acc_drhodt, acc_bytes,
+                                                           cudaMemcpyDeviceToDevice, st));
+      }
       LCHECK(h, "zsph_run_learned corrector", run_substep(h, *o, *w, *t, 2, st, nullptr, nullptr));
-      k_judge<<<kRedBlocks, kRedThreads, 0, st>>>(h->kp.n, t->index, reinterpret_cast<const float4*>(t->acc_drhodt),
-                                                 L->acc_n, L->dprev, L->yhat, o->type, oa, ob, L->red);
+      if (network)
+        k_judge<<<kRedBlocks, kRedThreads, 0, st>>>(h->kp.n, t->index,
+                                                   reinterpret_cast<const float4*>(t->acc_drhodt), L->acc_n,
+                                                   L->dprev, L->yhat, o->type, oa, ob, L->red);
+      else
+        k_judge_acc<<<kRedBlocks, kRedThreads, 0, st>>>(h->kp.n, t->index,
+                                                       reinterpret_cast<const float4*>(t->acc_drhodt), L->yhat,
+                                                       o->type, L->red);
       LCHECK(h, "zsph_run_learned judge", cudaGetLastError());
       LCHECK(h, "zsph_run_learned judge", cudaMemcpyAsync(L->red_host, L->red, kRedBlocks * 8 * sizeof(double),
                                                           cudaMemcpyDeviceToHost, st));
@@ -623,6 +673,7 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, con
       double v[8];
       host_sums(L, v, 8);
       const float err = (float)std::sqrt(v[0] / std::max(v[1], 1e-300));
+      if (rs.judged < series_cap) err_series[rs.judged] = err;
       rs.judged += 1;
       rs.err_last = err;
       rs.err_max = std::max(rs.err_max, err);
@@ -634,13 +685,17 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, con
       LCHECK(h, "zsph_run_learned plain", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
       LCHECK(h, "zsph_run_learned plain", run_substep(h, *o, *w, *t, 2, st, nullptr, nullptr));
       rs.plain += 1;
-    } else {
+    } else if (network) {
       LCHECK(h, "zsph_run_learned copy", cudaMemcpyAsync(L->acc_prev, t->acc_drhodt, acc_bytes,
                                                          cudaMemcpyDeviceToDevice, st));
       LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, &fo));
       LCHECK(h, "zsph_run_learned corrector", launch_mlp_correct(*net, h->kp, L->tiles, *o,
                                                                  reinterpret_cast<float4*>(t->acc_drhodt), L->dprev,
                                                                  oa, ob, h->s.flags, st));
+      rs.learned += 1;
+    } else {
+      LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
+      LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 2, st));
       rs.learned += 1;
     }
     rs.steps += 1;

@@ -24,6 +24,13 @@
 // the particles' centroid, mass shared equally).  The reference moves body
 // particles by their velocity (time_int.cpp:7-12); here they are placed from
 // the body's pose, so the body stays rigid.
+//
+// Several bodies (up to kMaxBodies, disjoint ranges of original indices)
+// share these launches: k_rigid_sum runs one row of CTAs per body,
+// k_rigid_step one thread per body.  With contact switched on
+// (zsph_rigid_contact), k_rigid_contact (equations.cu) first adds to each
+// body particle's load the spring-dashpot force of its wall and other-body
+// neighbours.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -34,20 +41,28 @@
 
 namespace zsph {
 
+constexpr int kMaxBodies = 16;
+
 struct Body {
   double x[3], v[3], w[3], q[4];      // centre of mass, velocity, angular velocity (world), orientation (w,x,y,z)
   double xn[3], vn[3], wn[3], qn[4];  // the same at the start of the step
-  double F[3], T[3];                  // last fluid force and torque
+  double F[3], T[3];                  // last fluid (and contact) force and torque
   double I[9], Iinv[9];               // body-frame inertia about the centre of mass, and its inverse
   double M, g;
   int first, count;
+  long long r0_off;                   // first of this body's rows in RigidState::r0
 };
 
 struct RigidState {
-  Body* body = nullptr;      // device
-  double* r0 = nullptr;      // [count][3] body-frame offsets
-  double* partial = nullptr; // [kRigidBlocks][6]
-  float4* force = nullptr;   // [n] per-particle fluid pressure acceleration (kp.rigid_f)
+  Body* body = nullptr;         // device [kMaxBodies]
+  BodyRange* ranges = nullptr;  // device [kMaxBodies] (first, count), for the contact kernel
+  double* r0 = nullptr;         // [sum of counts][3] body-frame offsets, body after body
+  double* partial = nullptr;    // [kMaxBodies][kRigidBlocks][6]
+  float4* force = nullptr;      // [n] per-particle load per unit particle mass (kp.rigid_f)
+  int nb = 0;
+  std::vector<Body> host;       // the bodies as attached (device copies evolve)
+  std::vector<std::vector<double>> host_r0;
+  float kn = 0.f, cn = 0.f, dist = 0.f;  // contact (kn = 0: off)
 };
 
 namespace {
@@ -120,11 +135,26 @@ __device__ inline bool body_particle(const zsph_ptc_t& s, const Body& b, int i, 
   *k = s.table[i] + i - b.first;  // table[i] + i: the particle's original index (sort.cu:82)
   return *k >= 0 && *k < b.count;
 }
+// the body owning particle i (index into bodies) and its row k, or -1
+__device__ inline int body_of(const zsph_ptc_t& s, const Body* bodies, int nb, int i, int* k) {
+  if (s.type[i] != 2) return -1;
+  const int id = s.table[i] + i;
+  for (int b = 0; b < nb; ++b) {
+    const int kk = id - bodies[b].first;
+    if (kk >= 0 && kk < bodies[b].count) {
+      *k = kk;
+      return b;
+    }
+  }
+  return -1;
+}
 
-// FP64 force and torque of the fluid on the body, per-CTA partial sums
+// FP64 force and torque on each body, per-CTA partial sums: CTA row
+// blockIdx.y sums the particles of body blockIdx.y, in particle order
 __global__ void __launch_bounds__(kRigidThreads) k_rigid_sum(KParams kp, zsph_ptc_t s, const int* c3,
-                                                             const float4* f, const Body* body, double* partial) {
-  const Body& b = *body;
+                                                             const float4* f, const Body* bodies, double* partial) {
+  const Body& b = bodies[blockIdx.y];
+  partial += (size_t)blockIdx.y * gridDim.x * 6;
   double acc[6] = {0, 0, 0, 0, 0, 0};
   const double m = kp.p.m;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += gridDim.x * blockDim.x) {
@@ -154,10 +184,11 @@ __global__ void __launch_bounds__(kRigidThreads) k_rigid_sum(KParams kp, zsph_pt
   }
 }
 
-// FP64 predictor (mode 1) or corrector (mode 2) of the body, one thread
-__global__ void k_rigid_step(Body* body, const double* partial, int nparts, int mode, double half_dt) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  Body& b = *body;
+// FP64 predictor (mode 1) or corrector (mode 2) of each body, one thread per body
+__global__ void k_rigid_step(Body* bodies, int nb, const double* partial, int nparts, int mode, double half_dt) {
+  if (blockIdx.x != 0 || (int)threadIdx.x >= nb) return;
+  Body& b = bodies[threadIdx.x];
+  partial += (size_t)threadIdx.x * nparts * 6;
   double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
   for (int c = 0; c < nparts; ++c)
     for (int a = 0; a < 3; ++a) {
@@ -209,16 +240,17 @@ __global__ void k_rigid_step(Body* body, const double* partial, int nparts, int 
 }
 
 // body particles at the body's pose; precision form: cell + offset
-__global__ void __launch_bounds__(kRigidThreads) k_rigid_place(KParams kp, zsph_ptc_t s, int* c3, const Body* body,
-                                                               const double* r0) {
+__global__ void __launch_bounds__(kRigidThreads) k_rigid_place(KParams kp, zsph_ptc_t s, int* c3, const Body* bodies,
+                                                               int nb, const double* r0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kp.n) return;
-  const Body& b = *body;
   int k;
-  if (!body_particle(s, b, i, &k)) return;
+  const int bi = body_of(s, bodies, nb, i, &k);
+  if (bi < 0) return;
+  const Body& b = bodies[bi];
   double R[9], r[3], x[3], w[3];
   rot(b.q, R);
-  mat_vec(R, r0 + 3 * (size_t)k, r);
+  mat_vec(R, r0 + 3 * ((size_t)b.r0_off + (size_t)k), r);
   for (int a = 0; a < 3; ++a) x[a] = b.x[a] + r[a];
   cross(b.w, r, w);
   for (int a = 0; a < 3; ++a) s.vel[3 * i + a] = (float)(b.v[a] + w[a]);
@@ -339,6 +371,7 @@ void precise_destroy(Handle* h) {
   h->c3buf[0] = h->c3buf[1] = nullptr;
   if (h->rigid) {
     cudaFree(h->rigid->body);
+    cudaFree(h->rigid->ranges);
     cudaFree(h->rigid->r0);
     cudaFree(h->rigid->partial);
     cudaFree(h->rigid->force);
@@ -347,13 +380,18 @@ void precise_destroy(Handle* h) {
   }
 }
 
-cudaError_t rigid_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, int mode, cudaStream_t st) {
+cudaError_t rigid_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
+                          cudaStream_t st) {
   RigidState* R = h->rigid;
   const KParams& kp = h->kp;
-  k_rigid_sum<<<kRigidBlocks, kRigidThreads, 0, st>>>(kp, to, kp.c3n, R->force, R->body, R->partial);
-  k_rigid_step<<<1, 32, 0, st>>>(R->body, R->partial, kRigidBlocks, mode, (double)kp.p.half_dt);
+  if (R->kn > 0.f) {
+    cudaError_t e = launch_rigid_contact(kp, h->s, to, t, R->ranges, R->nb, R->kn, R->cn, R->dist, st);
+    if (e) return e;
+  }
+  k_rigid_sum<<<dim3(kRigidBlocks, R->nb), kRigidThreads, 0, st>>>(kp, to, kp.c3n, R->force, R->body, R->partial);
+  k_rigid_step<<<1, 32, 0, st>>>(R->body, R->nb, R->partial, kRigidBlocks, mode, (double)kp.p.half_dt);
   k_rigid_place<<<(kp.n + kRigidThreads - 1) / kRigidThreads, kRigidThreads, 0, st>>>(kp, from, kp.c3o, R->body,
-                                                                                      R->r0);
+                                                                                      R->nb, R->r0);
   return cudaGetLastError();
 }
 
@@ -453,16 +491,19 @@ int zsph_conservation(zsph_handle_t* h, const zsph_ptc_t* old_, zsph_conservatio
   c.potential = v[6];
   c.internal = v[7];
   if (h->rigid) {
-    Body b;
-    PCHECK(h, "zsph_conservation body", cudaMemcpy(&b, h->rigid->body, sizeof b, cudaMemcpyDeviceToHost));
-    double R[9], tmp[3], tmp2[3], Iw[3];
-    rot(b.q, R);
-    mat_tvec(R, b.w, tmp);
-    mat_vec(b.I, tmp, tmp2);
-    mat_vec(R, tmp2, Iw);
-    c.body_kinetic = 0.5 * b.M * (b.v[0] * b.v[0] + b.v[1] * b.v[1] + b.v[2] * b.v[2]) +
-                     0.5 * (b.w[0] * Iw[0] + b.w[1] * Iw[1] + b.w[2] * Iw[2]);
-    c.body_potential = -b.M * b.g * b.x[2];
+    std::vector<Body> bs(h->rigid->nb);
+    PCHECK(h, "zsph_conservation body",
+           cudaMemcpy(bs.data(), h->rigid->body, sizeof(Body) * bs.size(), cudaMemcpyDeviceToHost));
+    for (const Body& b : bs) {
+      double R[9], tmp[3], tmp2[3], Iw[3];
+      rot(b.q, R);
+      mat_tvec(R, b.w, tmp);
+      mat_vec(b.I, tmp, tmp2);
+      mat_vec(R, tmp2, Iw);
+      c.body_kinetic += 0.5 * b.M * (b.v[0] * b.v[0] + b.v[1] * b.v[1] + b.v[2] * b.v[2]) +
+                        0.5 * (b.w[0] * Iw[0] + b.w[1] * Iw[1] + b.w[2] * Iw[2]);
+      c.body_potential += -b.M * b.g * b.x[2];
+    }
   }
   *out = c;
   return ZSPH_OK;
@@ -551,12 +592,14 @@ int zsph_rigid_attach(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_rigid
   if (!h->rigid) {
     auto* R0 = new RigidState();
     const size_t n = (size_t)std::max(h->kp.n, 1);
-    cudaError_t e = cudaMalloc(&R0->body, sizeof(Body));
-    if (!e) e = cudaMalloc(&R0->partial, sizeof(double) * 6 * kRigidBlocks);
+    cudaError_t e = cudaMalloc(&R0->body, sizeof(Body) * kMaxBodies);
+    if (!e) e = cudaMalloc(&R0->ranges, sizeof(BodyRange) * kMaxBodies);
+    if (!e) e = cudaMalloc(&R0->partial, sizeof(double) * 6 * kRigidBlocks * kMaxBodies);
     if (!e) e = cudaMalloc(&R0->force, sizeof(float4) * n);
     if (!e) e = cudaMemset(R0->force, 0, sizeof(float4) * n);
     if (e) {
       cudaFree(R0->body);
+      cudaFree(R0->ranges);
       cudaFree(R0->partial);
       cudaFree(R0->force);
       delete R0;
@@ -564,26 +607,81 @@ int zsph_rigid_attach(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_rigid
     }
     h->rigid = R0;
   }
-  cudaFree(h->rigid->r0);
-  h->rigid->r0 = nullptr;
-  PCHECK(h, "zsph_rigid_attach", cudaMalloc(&h->rigid->r0, sizeof(double) * r.size()));
-  PCHECK(h, "zsph_rigid_attach", cudaMemcpy(h->rigid->r0, r.data(), sizeof(double) * r.size(), cudaMemcpyHostToDevice));
-  PCHECK(h, "zsph_rigid_attach", cudaMemcpy(h->rigid->body, &b, sizeof b, cudaMemcpyHostToDevice));
-  h->kp.rigid_f = h->rigid->force;
+  RigidState* RS = h->rigid;
+  // the bodies' current states (earlier bodies have moved since they were attached)
+  if (RS->nb > 0)
+    PCHECK(h, "zsph_rigid_attach", cudaMemcpy(RS->host.data(), RS->body, sizeof(Body) * RS->nb, cudaMemcpyDeviceToHost));
+  int slot = RS->nb;  // a body with the same first index is replaced, any other one added
+  for (int k = 0; k < RS->nb; ++k) {
+    if (RS->host[k].first == b.first) {
+      slot = k;
+      continue;
+    }
+    const Body& o = RS->host[k];
+    if (b.first < o.first + o.count && o.first < b.first + b.count)
+      return set_herr(h, ZSPH_EINVAL, "zsph_rigid_attach: the body's particle range overlaps another body's");
+  }
+  if (slot == kMaxBodies) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_attach: at most 16 bodies per handle");
+  if (slot == RS->nb) {
+    RS->host.push_back(b);
+    RS->host_r0.push_back(r);
+    RS->nb += 1;
+  } else {
+    RS->host[slot] = b;
+    RS->host_r0[slot] = r;
+  }
+  std::vector<double> all;
+  std::vector<BodyRange> ranges(RS->nb);
+  for (int k = 0; k < RS->nb; ++k) {
+    RS->host[k].r0_off = (long long)(all.size() / 3);
+    all.insert(all.end(), RS->host_r0[k].begin(), RS->host_r0[k].end());
+    ranges[k] = BodyRange{RS->host[k].first, RS->host[k].count};
+  }
+  cudaFree(RS->r0);
+  RS->r0 = nullptr;
+  PCHECK(h, "zsph_rigid_attach", cudaMalloc(&RS->r0, sizeof(double) * all.size()));
+  PCHECK(h, "zsph_rigid_attach", cudaMemcpy(RS->r0, all.data(), sizeof(double) * all.size(), cudaMemcpyHostToDevice));
+  PCHECK(h, "zsph_rigid_attach", cudaMemcpy(RS->body, RS->host.data(), sizeof(Body) * RS->nb, cudaMemcpyHostToDevice));
+  PCHECK(h, "zsph_rigid_attach", cudaMemcpy(RS->ranges, ranges.data(), sizeof(BodyRange) * RS->nb,
+                                            cudaMemcpyHostToDevice));
+  h->kp.rigid_f = RS->force;
   drop_graph(h);
-  // body particles' velocities (and precision cells) from the pose
-  k_rigid_place<<<(h->kp.n + kRigidThreads - 1) / kRigidThreads, kRigidThreads>>>(h->kp, *old_, h->kp.c3o,
-                                                                                 h->rigid->body, h->rigid->r0);
+  // body particles' velocities (and precision cells) from the poses
+  k_rigid_place<<<(h->kp.n + kRigidThreads - 1) / kRigidThreads, kRigidThreads>>>(h->kp, *old_, h->kp.c3o, RS->body,
+                                                                                 RS->nb, RS->r0);
   PCHECK(h, "zsph_rigid_attach place", cudaDeviceSynchronize());
   return ZSPH_OK;
 }
 
-int zsph_rigid_get(zsph_handle_t* h, zsph_rigid_t* body) {
-  if (!h || !body) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get: null argument");
-  if (!h->rigid) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get: no body attached");
-  PCHECK(h, "zsph_rigid_get", cudaStreamSynchronize(h->last_stream));
+int zsph_rigid_contact(zsph_handle_t* h, double stiffness, double damping, double distance) {
+  if (!h) return set_herr(nullptr, ZSPH_EINVAL, "zsph_rigid_contact: null handle");
+  if (!h->rigid) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_contact: attach a body first");
+  if (!(stiffness >= 0) || !(damping >= 0) || !(distance >= 0))
+    return set_herr(h, ZSPH_EINVAL, "zsph_rigid_contact: stiffness, damping and distance must be >= 0");
+  if (stiffness > 0 && !((float)distance * (float)distance <= h->kp.r2max))
+    return set_herr(h, ZSPH_EINVAL, "zsph_rigid_contact: the contact distance must not exceed the 2h support");
+  if (h->kp.p.grid_factor != 1)
+    return set_herr(h, ZSPH_EINVAL, "zsph_rigid_contact: needs grid_size_factor 1");
+  h->rigid->kn = (float)stiffness;
+  h->rigid->cn = (float)damping;
+  h->rigid->dist = (float)distance;
+  drop_graph(h);
+  return ZSPH_OK;
+}
+
+int zsph_rigid_count(zsph_handle_t* h, int* count) {
+  if (!h || !count) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_count: null argument");
+  *count = h->rigid ? h->rigid->nb : 0;
+  return ZSPH_OK;
+}
+
+int zsph_rigid_get_body(zsph_handle_t* h, int index, zsph_rigid_t* body) {
+  if (!h || !body) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get_body: null argument");
+  if (!h->rigid || index < 0 || index >= h->rigid->nb)
+    return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get_body: no such body");
+  PCHECK(h, "zsph_rigid_get_body", cudaStreamSynchronize(h->last_stream));
   Body b;
-  PCHECK(h, "zsph_rigid_get", cudaMemcpy(&b, h->rigid->body, sizeof b, cudaMemcpyDeviceToHost));
+  PCHECK(h, "zsph_rigid_get_body", cudaMemcpy(&b, h->rigid->body + index, sizeof b, cudaMemcpyDeviceToHost));
   body->first = b.first;
   body->count = b.count;
   body->mass = b.M;
@@ -595,6 +693,12 @@ int zsph_rigid_get(zsph_handle_t* h, zsph_rigid_t* body) {
   std::memcpy(body->torque, b.T, sizeof b.T);
   std::memcpy(body->inertia, b.I, sizeof b.I);
   return ZSPH_OK;
+}
+
+int zsph_rigid_get(zsph_handle_t* h, zsph_rigid_t* body) {
+  if (!h || !body) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get: null argument");
+  if (!h->rigid) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_get: no body attached");
+  return zsph_rigid_get_body(h, 0, body);
 }
 
 }  // extern "C"

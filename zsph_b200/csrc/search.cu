@@ -802,6 +802,12 @@ cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const 
   return cudaGetLastError();
 }
 
+cudaError_t launch_pack_shadows(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st) {
+  if (kp.n == 0) return cudaSuccess;
+  k_pack<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s.sh, ptc);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                         cudaStream_t st) {
   if (kp.n == 0) return cudaSuccess;

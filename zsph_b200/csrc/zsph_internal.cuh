@@ -55,6 +55,11 @@ struct KParams {
   int tune_minb;
 };
 
+// Original-index range [first, first + count) of one rigid body.
+struct BodyRange {
+  int first, count;
+};
+
 // One scene of the batched form: its case constants as KParams holds them.
 struct SceneDev {
   zsph_gpu_param_t p;  // grid_hash_min/max: the scene's cells in batch coordinates
@@ -228,7 +233,8 @@ void learn_destroy(Handle* h);
 void precise_destroy(Handle* h);
 // precise.cu: FP64 force/torque sum, body update and placement after a
 // fused sub-step's governing kernel (mode 1 predictor, 2 corrector)
-cudaError_t rigid_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, int mode, cudaStream_t st);
+cudaError_t rigid_substep(Handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
+                          cudaStream_t st);
 
 // api.cu: one sub-step of the fused path (search `from` into `to`, boundary
 // on `to`, governing of `to` with the integration written into `from`)
@@ -273,7 +279,17 @@ cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const 
 cudaError_t launch_pack(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                         cudaStream_t st);
 
+// packed shadows of a state in its current order (no cell ranges)
+cudaError_t launch_pack_shadows(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st);
+
 // equations.cu
+// Learned form's corrector variants on the lists of the predictor's search
+// (ptc: the predicted state in that sorted order): shadows repacked, wall
+// (rho, p) at the predicted positions, optionally a fresh boundary pass
+// (else tmp.dofv_grandrho keeps the predictor's values), then governing with
+// mode 0 (acc_drhodt only) or 2 (correction written in place into ptc).
+cudaError_t launch_corrector_reuse(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                                  bool fresh_boundary, int mode, cudaStream_t st);
 cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                             cudaStream_t st, Prof* pf = nullptr);
 // one-time kernel attributes (shared-memory windows above 48 KB); call before launches
@@ -284,6 +300,12 @@ cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc
                              int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr,
                              const FeatOut* feat = nullptr);
 cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& tmp, cudaStream_t st);
+// Rigid bodies: adds to kp.rigid_f of every body particle of ptc (the state
+// the lists were built for) the contact force per unit particle mass of its
+// non-fluid neighbours that are not of its own body, within `dist` (<= 2h):
+// max(0, kn (dist - r) - cn v_n) along the pair's normal.
+cudaError_t launch_rigid_contact(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                                 const BodyRange* ranges, int nb, float kn, float cn, float dist, cudaStream_t st);
 cudaError_t launch_nb_counts(const KParams& kp, const Scratch& s, int* nb_boundary, int* nb_governing,
                              cudaStream_t st);
 cudaError_t launch_integrate(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
