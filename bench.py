@@ -388,6 +388,14 @@ def batched_leg(args, dist, stream, sptr):
     ms_b = timed(lambda: bt.run(K, sptr))
     flags_b = bt.status()
     bt.close()
+    # the same scenes in one persistent launch per step (grid barriers between the stages)
+    bp = z.Solver.from_batch(scenes)
+    bp.set_persistent(True)
+    bp.run(W, sptr)
+    ms_p = timed(lambda: bp.run(K, sptr))
+    flags_p = bp.status()
+    pinfo = bp.persistent_info()
+    bp.close()
     solo = [z.Solver.from_case(c) for c in scenes]
     for s in solo:
         s.run(W, sptr)
@@ -404,6 +412,12 @@ def batched_leg(args, dist, stream, sptr):
     return {"value": dist.world * n * K / (ms_b / 1e3), "unit": "particle-steps/s", "ms_per_step": ms_b / K,
             "loop_value": dist.world * n * K / (ms_l / 1e3), "loop_ms_per_step": ms_l / K,
             "speedup_vs_loop": ms_l / ms_b, "scenes": len(scenes), "particles": n,
+            "persistent": {"value": dist.world * n * K / (ms_p / 1e3), "ms_per_step": ms_p / K,
+                           "vs_graph_of_launches": ms_b / ms_p, "ctas": pinfo["ctas"],
+                           "graph": {1: "replayed from a CUDA graph", -1: "one direct launch per zsph_run",
+                                     0: "not run"}[pinfo["graph"]], "status_flags": flags_p,
+                           "what": "every scene's whole step in one cooperative launch: the stages of the "
+                                   "graph-of-launches step behind bounded grid barriers"},
             "fluid_per_scene": {"min": min(nf), "max": max(nf), "sum": sum(nf)}, "tune": tune,
             "status_flags": flags_b,
             "what": "aggregate particle-steps/s of 256 scenes (widths U[0.2,0.6] m, aspect U[0.5,2], dx U[0.01,0.02] m, "

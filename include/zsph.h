@@ -430,6 +430,25 @@ int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* old
  * leaves its scene's grid is parked in that scene's first cell.  Per scene
  * the results are those of a handle created for that scene alone. */
 int zsph_create_batch(const zsph_gpu_param_t* scenes, const int* grid_num, int nscenes, zsph_handle_t** out);
+/* Batched handle in persistent mode (no reference counterpart): zsph_step
+ * and zsph_run advance every scene with one cooperative launch per step whose
+ * CTAs stay resident and pass each stage (search, list build, boundary,
+ * governing with the integration) through a grid barrier instead of a kernel
+ * boundary.  The stages run the same device code as the step's separate
+ * launches, so the results are bit-identical with them.  zsph_run captures
+ * the launch in its CUDA graph when the driver accepts a cooperative launch
+ * in a capture, and otherwise issues one launch for all its steps.  Every
+ * barrier wait is bounded (about a second); a wait that runs out sets
+ * ZSPH_FLAG_TIMEOUT, every CTA leaves the kernel, and zsph_status returns
+ * ZSPH_ETIMEOUT.  on = 0 returns to the separate launches. */
+int zsph_set_batch_persistent(zsph_handle_t* h, int on);
+/* CTAs of the persistent launch, and whether zsph_run replays it from a
+ * graph (1), issues it directly (-1) or has not run yet (0). */
+int zsph_persistent_info(zsph_handle_t* h, int* ctas, int* graph);
+/* Self-test of the bounded barrier: one persistent launch whose barrier
+ * waits for an arrival that never comes, each wait limited to spin_limit
+ * polls; returns ZSPH_ETIMEOUT (and clears the flag) when the bound works. */
+int zsph_persistent_barrier_test(zsph_handle_t* h, int spin_limit, void* stream);
 
 /* ---- Autotuner (no reference counterpart) ----------------------------------
  * Times every candidate launch shape of the grid-factor-1 step -- cells

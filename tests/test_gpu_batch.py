@@ -92,3 +92,51 @@ def test_set_launch_shapes_applies_every_candidate_bit_identically(scenes):
             with pytest.raises(z.ZsphError):
                 s.set_launch_shapes(*bad)
         s.close()
+
+
+# ---- persistent mode: the whole step in one cooperative launch --------------
+
+def test_persistent_step_matches_the_separate_launches(scenes):
+    """The persistent kernel runs the same stage code behind grid barriers:
+    zsph_step and zsph_run give the separate launches' results bit for bit
+    (hence each scene's result run alone), the tmp arrays included."""
+    nsteps = 7
+    ref = z.Solver.from_batch(scenes)
+    ref.run(nsteps)
+    want, want_t = ref.download("old"), ref.download_tmp()
+    ref.close()
+    for via_run in (True, False):
+        b = z.Solver.from_batch(scenes)
+        b.set_persistent(True)
+        info = b.persistent_info()
+        assert info["ctas"] >= 148
+        if via_run:
+            b.run(nsteps)
+        else:
+            for _ in range(nsteps):
+                b.step()
+        got, got_t = b.download("old"), b.download_tmp()
+        assert b.status() == 0
+        print("persistent", info, b.persistent_info())
+        for k in ("pos", "vel", "rhop", "tmp_pos", "tmp_vel", "tmp_rhop", "type", "table"):
+            assert np.array_equal(getattr(got, k), getattr(want, k)), (via_run, k)
+        for k in ("hash", "index", "grid_start", "grid_end", "acc_drhodt", "dofv_grandrho"):
+            assert np.array_equal(got_t[k], want_t[k]), (via_run, k)
+        b.close()
+
+
+def test_persistent_barrier_wait_is_bounded(scenes):
+    """A barrier whose last arrival never comes: every CTA gives up after its
+    bounded wait, the handle reports ZSPH_ETIMEOUT, and the context stays
+    usable (a persistent run afterwards still succeeds)."""
+    b = z.Solver.from_batch(scenes)
+    b.set_persistent(True)
+    rc = z.lib.zsph_persistent_barrier_test(b.h, 2000, None)
+    assert rc == z.ZSPH_ETIMEOUT, z.last_error(b.h)
+    assert b.status() == 0  # the self-test cleared the flag
+    b.run(2)
+    assert b.status() == 0
+    assert np.all(np.isfinite(b.download("old").pos))
+    with pytest.raises(z.ZsphError):
+        z.Solver.from_case(scenes[0]).set_persistent(True)  # single-scene handles have no persistent mode
+    b.close()

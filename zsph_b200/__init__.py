@@ -250,6 +250,9 @@ _sig = {
     "zsph_autotune": (_I, [_HP, ctypes.POINTER(Ptc), ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I,
                            ctypes.POINTER(TuneResult), _VP]),
     "zsph_set_launch_shapes": (_I, [_HP, ctypes.POINTER(TuneResult)]),
+    "zsph_set_batch_persistent": (_I, [_HP, _I]),
+    "zsph_persistent_info": (_I, [_HP, _IP, _IP]),
+    "zsph_persistent_barrier_test": (_I, [_HP, _I, _VP]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -583,6 +586,15 @@ class Solver:
         b = RigidBody()
         self._call(lib.zsph_rigid_get_body, int(index), ctypes.byref(b))
         return _as_dict(b)
+
+    def set_persistent(self, on: bool = True) -> None:
+        """zsph_set_batch_persistent (batched handles)."""
+        self._call(lib.zsph_set_batch_persistent, 1 if on else 0)
+
+    def persistent_info(self) -> dict:
+        c, g = ctypes.c_int(0), ctypes.c_int(0)
+        self._call(lib.zsph_persistent_info, ctypes.byref(c), ctypes.byref(g))
+        return {"ctas": c.value, "graph": g.value}
 
     def body_count(self) -> int:
         n = ctypes.c_int(0)

@@ -141,8 +141,17 @@ cudaError_t substep(zsph_handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to
   return e;
 }
 
+// the batched form's persistent kernel over nsteps steps (barrier words zeroed first)
+cudaError_t persistent_steps(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, const zsph_tmp_t& t,
+                             int nsteps, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(h->pbar, 0, 2 * sizeof(unsigned), st);
+  if (!e) e = launch_batch_persistent(h->kp, h->s, o, w, t, h->pbar, nsteps, h->spin_limit, 0, st);
+  return e;
+}
+
 cudaError_t step_launches(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, const zsph_tmp_t& t,
                           cudaStream_t st, Prof* pf = nullptr) {
+  if (h->persistent && !pf) return persistent_steps(h, o, w, t, 1, st);
   cudaError_t e = substep(h, o, w, t, 1, st, pf);
   if (!e) e = substep(h, o, w, t, 2, st, pf);
   return e;
@@ -380,6 +389,7 @@ void zsph_destroy(zsph_handle_t* h) {
   if (!h) return;
   if (h->graph) cudaGraphExecDestroy(h->graph);
   if (h->graph_stream) cudaStreamDestroy(h->graph_stream);
+  cudaFree(h->pbar);
   learn_destroy(h);
   precise_destroy(h);
   cudaFree(h->scene_tab);
@@ -517,6 +527,10 @@ int zsph_run(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const z
   if (int rc = check_tmp(h, tmp)) return rc;
   h->last_stream = as_stream(stream);
   if (nsteps == 0 || h->kp.n == 0) return ZSPH_OK;
+  if (h->persistent && h->persist_graph < 0) {  // graph capture refused: one launch for all steps
+    ZCHECK(h, "zsph_run persistent", persistent_steps(h, *o, *w, *tmp, nsteps, h->last_stream));
+    return ZSPH_OK;
+  }
   const bool same = h->graph && !std::memcmp(&h->graph_old, o, sizeof *o) &&
                     !std::memcmp(&h->graph_new, w, sizeof *w) && !std::memcmp(&h->graph_tmp, tmp, sizeof *tmp);
   if (!same) {
@@ -530,11 +544,26 @@ int zsph_run(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const z
     cudaError_t le = cudaSuccess;
     for (int k = 0; k < h->graph_steps && !le; ++k) le = step_launches(h, *o, *w, *tmp, h->graph_stream);
     cudaError_t ce = cudaStreamEndCapture(h->graph_stream, &g);
+    if (h->persistent && (le || ce)) {  // a cooperative launch the capture does not take: run it directly
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      h->persist_graph = -1;
+      ZCHECK(h, "zsph_run persistent", persistent_steps(h, *o, *w, *tmp, nsteps, h->last_stream));
+      return ZSPH_OK;
+    }
     if (le) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run launch", le); }
     if (ce) { if (g) cudaGraphDestroy(g); return cuda_fail(h, "zsph_run end capture", ce); }
     cudaError_t ie = cudaGraphInstantiate(&h->graph, g, 0);
     cudaGraphDestroy(g);
+    if (ie && h->persistent) {
+      cudaGetLastError();
+      h->graph = nullptr;
+      h->persist_graph = -1;
+      ZCHECK(h, "zsph_run persistent", persistent_steps(h, *o, *w, *tmp, nsteps, h->last_stream));
+      return ZSPH_OK;
+    }
     if (ie) { h->graph = nullptr; return cuda_fail(h, "zsph_run instantiate", ie); }
+    if (h->persistent) h->persist_graph = 1;
     h->graph_old = *o;
     h->graph_new = *w;
     h->graph_tmp = *tmp;
@@ -663,6 +692,48 @@ int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes) {
   return ZSPH_OK;
 }
 
+int zsph_set_batch_persistent(zsph_handle_t* h, int on) {
+  ENTRY_CHECKS(h);
+  if (on) {
+    if (!h->kp.scenes) return set_err(h, ZSPH_EINVAL, "zsph_set_batch_persistent: a batched handle is required");
+    int grid = 0;
+    ZCHECK(h, "zsph_set_batch_persistent", persistent_grid(&grid));
+    if (!h->pbar) ZCHECK(h, "zsph_set_batch_persistent", cudaMalloc(&h->pbar, 2 * sizeof(unsigned)));
+    ZCHECK(h, "zsph_set_batch_persistent", cudaMemset(h->pbar, 0, 2 * sizeof(unsigned)));
+  }
+  h->persistent = on ? 1 : 0;
+  h->persist_graph = 0;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  return ZSPH_OK;
+}
+
+int zsph_persistent_info(zsph_handle_t* h, int* ctas, int* graph) {
+  ENTRY_CHECKS(h);
+  int g = 0;
+  ZCHECK(h, "zsph_persistent_info", persistent_grid(&g));
+  if (ctas) *ctas = g;
+  if (graph) *graph = h->persist_graph;
+  return ZSPH_OK;
+}
+
+int zsph_persistent_barrier_test(zsph_handle_t* h, int spin_limit, void* stream) {
+  ENTRY_CHECKS(h);
+  if (!h->persistent) return set_err(h, ZSPH_EINVAL, "zsph_persistent_barrier_test: persistent mode is off");
+  if (spin_limit <= 0) return set_err(h, ZSPH_EINVAL, "zsph_persistent_barrier_test: spin_limit must be positive");
+  cudaStream_t st = as_stream(stream);
+  h->last_stream = st;
+  ZCHECK(h, "zsph_persistent_barrier_test", cudaMemsetAsync(h->pbar, 0, 2 * sizeof(unsigned), st));
+  ZCHECK(h, "zsph_persistent_barrier_test",
+         launch_batch_persistent(h->kp, h->s, zsph_ptc_t{}, zsph_ptc_t{}, zsph_tmp_t{}, h->pbar, 0,
+                                 (unsigned)spin_limit, 1, st));
+  ZCHECK(h, "zsph_persistent_barrier_test", cudaStreamSynchronize(st));
+  ZCHECK(h, "zsph_persistent_barrier_test", cudaMemsetAsync(h->pbar, 0, 2 * sizeof(unsigned), st));
+  return zsph_status(h, nullptr, 1);
+}
+
 int zsph_status(zsph_handle_t* h, int* flags, int clear) {
   if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle");
   if (int rc = check_device(h)) return rc;
@@ -673,6 +744,7 @@ int zsph_status(zsph_handle_t* h, int* flags, int clear) {
   if (clear) ZCHECK(h, "zsph_status clear", cudaMemset(h->s.flags, 0, sizeof(int)));
   if (flags) *flags = f;
   if (f & ZSPH_FLAG_NAN) return set_err(h, ZSPH_ENAN, "non-finite acceleration or density");
+  if (f & ZSPH_FLAG_TIMEOUT) return set_err(h, ZSPH_ETIMEOUT, "a bounded wait in a kernel ran out");
   if (f & ZSPH_FLAG_BAD_KEY) return set_err(h, ZSPH_EINVAL, "zsph_sort_index: key outside [0, grid_num)");
   return ZSPH_OK;
 }

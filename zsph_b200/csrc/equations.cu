@@ -54,6 +54,7 @@
 #include <climits>
 
 #include "integrate.cuh"
+#include "search_dev.cuh"
 #include "zsph_internal.cuh"
 
 namespace zsph {
@@ -396,8 +397,14 @@ template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 // At least 42 warps per SM (a register budget of 40-48 without spills in the
 // plain form, 9.9 KB of shared memory per 2-warp CTA): the kernel is
 // issue-bound and hides its staging loads with more resident warps.
-template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
-__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
+//
+// nblist_group is the work of one warp on group `group` (particles
+// 32*group .. 32*group+31); k_nblist_seq runs one group per warp, the
+// batched form's persistent kernel loops over groups.  The warp's staging
+// arrays are slot `wid` of the CTA's CW slots.
+template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE>
+__device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_tmp_t& t, int group,
+                                             int wid) {
   constexpr int NR = Stencil<GF>::NR;
   // per segment (cell) of a round: its 64 staged candidates' x, y and z; the
   // two floats of padding per array put the segments' arrays in different banks
@@ -405,8 +412,8 @@ __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg,
   // per lane: a 32-entry ring (a partial 8-entry block plus one half block's
   // hits fit), padded to 80 bytes so that the lanes' rings spread over the banks
   __shared__ __align__(16) uint16_t s_ring[CW][32][kRing + 8];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int p0 = (blockIdx.x * CW + wid) * 32;
+  const int lane = threadIdx.x & 31;
+  const int p0 = group * 32;
   if (p0 >= kp_arg.n) return;  // uniform per warp
   const int i = p0 + lane;
   const bool act = i < kp_arg.n;
@@ -571,6 +578,12 @@ __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg,
   if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
 
+template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
+__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
+  const int wid = threadIdx.x >> 5;
+  nblist_group<GF, WALL, CW, BATCH, PRECISE>(kp_arg, s, t, blockIdx.x * CW + wid, wid);
+}
+
 struct NbB1 {  // boundary loop 1
   float4 pr, vp;
 };
@@ -594,9 +607,9 @@ template <int GF> struct PairSmem {
   int *rs, *re, *fb;
   WinHdr* wh;
   float4* win;
-  __device__ explicit PairSmem(unsigned char* dsm) {
+  __device__ explicit PairSmem(unsigned char* dsm, int tid = threadIdx.x) {
     constexpr int NR = Stencil<GF>::NR;
-    rs = reinterpret_cast<int*>(dsm) + threadIdx.x;
+    rs = reinterpret_cast<int*>(dsm) + tid;
     re = rs + NR * kPairBlock;
     fb = re + NR * kPairBlock;
     wh = reinterpret_cast<WinHdr*>(dsm + 3 * NR * kPairBlock * 4);
@@ -609,11 +622,12 @@ template <int GF> struct PairSmem {
 // REUSE (learned form's corrector variants): the lists were built at an
 // earlier state of the same sorted order, so every entry is tested again
 // against the exact threshold at the current positions and skipped beyond it.
-template <int GF, bool PRECISE = false, bool BATCH = false, bool REUSE = false>
-__global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  PairSmem<GF> sm(dsm);
-  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+// boundary_one is the work of one thread on particle i (its row arrays in
+// sm); `windows` (the kernel: every thread of the CTA together) allows the
+// shared-memory windows when kp.stage_windows asks for them.
+template <int GF, bool PRECISE, bool BATCH, bool REUSE>
+__device__ __forceinline__ void boundary_one(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
+                                             const zsph_tmp_t& t, int i, const PairSmem<GF>& sm, bool windows) {
   KParams kp_scene;  // batched form: the parameters of the particle's scene
   if constexpr (BATCH) kp_scene = kp_of_particle(kp_arg, i);
   const KParams& kp = BATCH ? kp_scene : kp_arg;
@@ -621,7 +635,7 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   if (act) load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
   const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
   bool staged = false;
-  if (GF == 1 && kp.stage_windows && !PRECISE) {
+  if (windows && GF == 1 && kp.stage_windows && !PRECISE) {
     const float4* const src[1] = {s.sh.rec};  // 32-byte records: two float4s per candidate
     staged = stage_window<Stencil<GF>::NR, 1>(*sm.wh, sm.win, kWinCapB, src, {2}, act, sm.rs, sm.re, sm.fb,
                                               s.flags, [](int r) { return Stencil<GF>::boundary_row(r); });
@@ -696,6 +710,13 @@ __global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch
   if (!fi) reinterpret_cast<float2*>(ptc.rhop)[i] = make_float2(fabsf(pi.w), vi.w);
 }
 
+template <int GF, bool PRECISE = false, bool BATCH = false, bool REUSE = false>
+__global__ void __launch_bounds__(kPairBlock) k_boundary(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  boundary_one<GF, PRECISE, BATCH, REUSE>(kp_arg, s, ptc, t, blockIdx.x * kPairBlock + threadIdx.x,
+                                          PairSmem<GF>(dsm), true);
+}
+
 struct NbG {  // governing
   float4 pr, vp, dg;
 };
@@ -725,13 +746,11 @@ struct FeatAcc {
 // MINB: minimum resident CTAs per SM (register budget); the default six
 // give 80 registers without spills for the plain variants.
 // REUSE: as k_boundary's (entries re-tested at the current positions).
-template <int GF, int MODE, bool FEAT = false, bool PRECISE = false, bool BATCH = false, bool RIGID = false,
-          int MINB = (FEAT || BATCH) ? 1 : 6, bool REUSE = false>
-__global__ void __launch_bounds__(kPairBlock, MINB)
-    k_governing(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t, zsph_ptc_t out, FeatOut fo) {
-  extern __shared__ __align__(16) unsigned char dsm[];
-  PairSmem<GF> sm(dsm);
-  const int i = blockIdx.x * kPairBlock + threadIdx.x;
+// governing_one: one thread's particle i, as boundary_one.
+template <int GF, int MODE, bool FEAT, bool PRECISE, bool BATCH, bool RIGID, bool REUSE>
+__device__ __forceinline__ void governing_one(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
+                                              const zsph_tmp_t& t, const zsph_ptc_t& out, const FeatOut& fo, int i,
+                                              const PairSmem<GF>& sm, bool windows) {
   KParams kp_scene;  // batched form: the parameters of the particle's scene
   if constexpr (BATCH) kp_scene = kp_of_particle(kp_arg, i);
   const KParams& kp = BATCH ? kp_scene : kp_arg;
@@ -740,7 +759,7 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
   const int3 ci = PRECISE && act ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
   const float4* dg = reinterpret_cast<const float4*>(t.dofv_grandrho);
   bool staged = false;
-  if (GF == 1 && kp.stage_windows && !PRECISE) {
+  if (windows && GF == 1 && kp.stage_windows && !PRECISE) {
     const float4* const src[2] = {s.sh.rec, dg};  // 32-byte records, then grad(rho)
     staged = stage_window<Stencil<GF>::NR, 2>(*sm.wh, sm.win, kWinCapG, src, {2, 1}, act, sm.rs, sm.re, sm.fb,
                                               s.flags, [](int) { return true; });
@@ -864,6 +883,16 @@ __global__ void __launch_bounds__(kPairBlock, MINB)
     if (fo.acc_copy) fo.acc_copy[i] = acc;
   }
   if (MODE != 0) integrate_one<MODE, PRECISE>(kp, ptc, out, i, acc);
+}
+
+template <int GF, int MODE, bool FEAT = false, bool PRECISE = false, bool BATCH = false, bool RIGID = false,
+          int MINB = (FEAT || BATCH) ? 1 : 6, bool REUSE = false>
+__global__ void __launch_bounds__(kPairBlock, MINB)
+    k_governing(KParams kp_arg, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t, zsph_ptc_t out, FeatOut fo) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  governing_one<GF, MODE, FEAT, PRECISE, BATCH, RIGID, REUSE>(kp_arg, s, ptc, t, out, fo,
+                                                               blockIdx.x * kPairBlock + threadIdx.x,
+                                                               PairSmem<GF>(dsm), true);
 }
 
 // ---- simple-SPH equations (the reference's simplesph target) --------------
@@ -1212,6 +1241,156 @@ __global__ void __launch_bounds__(kPairBlock) k_rigid_contact(KParams kp, Scratc
   kp.rigid_f[i] = f;
 }
 
+// ---- batched form: the whole step in one persistent launch ----------------
+//
+// k_batch_persistent runs nsteps full steps of a batched handle (every scene)
+// in one cooperative launch: the grid is at most what the GPU holds at once,
+// every CTA stays resident, and the stages of a sub-step are separated by
+// grid barriers instead of kernel boundaries.  Each stage loops over its
+// work units with the same device code as the stage's own kernel
+// (search_dev.cuh bodies, nblist_group, boundary_one, governing_one), so the
+// arithmetic and the orders are those of the graph-of-launches step and each
+// scene's result is still that of the scene run alone.  A CTA has 256
+// threads: the search bodies' CTA, 8 list-build warps, or two 128-thread pair
+// blocks.  The stages of a sub-step (from = old_, to = new_, as the fused
+// step): hash and tickets | one-pass scan (tiles claimed in order) | scatter
+// | crowded cells sorted, if the scan listed any | rank and gather | list
+// build and wall pressure | boundary | governing with the prediction or
+// correction into old_.
+//
+// Grid barrier: a CTA's thread 0 arrives on a counter and waits for the
+// generation word to change; the last to arrive resets the counter and
+// advances the generation.  The wait is bounded (spin_limit polls with a
+// short sleep, about a second by default); a CTA that gives up raises
+// ZSPH_FLAG_TIMEOUT and leaves the kernel, and so, within the same bound,
+// does every other CTA.  `extra` adds arrivals that never come (self-test
+// of the bound: with extra > 0 no barrier can complete).
+constexpr int kPersistThreads = kSearchBlock;
+static_assert(kPersistThreads == 2 * kPairBlock, "two pair blocks per persistent CTA");
+constexpr int kPersistWarps = kPersistThreads / 32;
+
+struct PersistArgs {
+  KParams kp;
+  Scratch s;
+  zsph_ptc_t o, w;
+  zsph_tmp_t t;
+  unsigned* bar;  // [0] arrivals, [1] generation
+  int nsteps;
+  unsigned spin_limit;
+  int extra;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ bool grid_barrier(const PersistArgs& a) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = ld_acquire_u32(a.bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(a.bar, 1u) + 1u;
+    int ok = 1;
+    if (arrived == gridDim.x + (unsigned)a.extra) {
+      atomicExch(a.bar, 0u);
+      __threadfence();
+      atomicAdd(a.bar + 1, 1u);
+    } else {
+      unsigned spins = 0;
+      while (ld_acquire_u32(a.bar + 1) == g) {
+        if (++spins > a.spin_limit) {
+          ok = 0;
+          atomicOr(a.s.flags, ZSPH_FLAG_TIMEOUT);
+          break;
+        }
+        __nanosleep(200);
+      }
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int MODE>
+__device__ __forceinline__ void persistent_pairs(const PersistArgs& a, unsigned char* dsm) {
+  const KParams& kp = a.kp;
+  const int half = threadIdx.x / kPairBlock, tid = threadIdx.x % kPairBlock;
+  const PairSmem<1> sm(dsm + half * pair_smem<1>(0, 0), tid);
+  const int nvb = (kp.n + kPairBlock - 1) / kPairBlock;
+  const FeatOut none{};
+  if (MODE == 0) {  // boundary
+    for (int vb = 2 * blockIdx.x + half; vb < nvb; vb += 2 * gridDim.x)
+      boundary_one<1, false, true, false>(kp, a.s, a.w, a.t, vb * kPairBlock + tid, sm, false);
+  } else {          // governing, integrated into old_
+    for (int vb = 2 * blockIdx.x + half; vb < nvb; vb += 2 * gridDim.x)
+      governing_one<1, MODE, false, false, true, false, false>(kp, a.s, a.w, a.t, a.o, none, vb * kPairBlock + tid,
+                                                               sm, false);
+  }
+}
+
+__global__ void __launch_bounds__(kPersistThreads, 2) k_batch_persistent(PersistArgs a) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  __shared__ int s_tile;
+  const KParams& kp = a.kp;
+  const Scratch& s = a.s;
+  const int n = kp.n;
+  const int hash_chunks = (n + kSearchBlock * kHashItems - 1) / (kSearchBlock * kHashItems);
+  const int scan_tiles = (kp.G + kOneTile - 1) / kOneTile;
+  const int scat_chunks = (n + kSearchBlock * kScatterItems - 1) / (kSearchBlock * kScatterItems);
+  const int groups = (n + 31) / 32;
+  const int wid = threadIdx.x >> 5;
+  if (a.nsteps == 0 && !grid_barrier(a)) return;  // self-test: the barrier alone
+  for (int step = 0; step < a.nsteps; ++step) {
+    for (int sub = 1; sub <= 2; ++sub) {
+      for (int c = blockIdx.x; c < hash_chunks; c += gridDim.x) {
+        hash_count_body(kp, a.o, s, c);
+        __syncthreads();  // its block-maximum scratch is reused by the next chunk
+      }
+      if (!grid_barrier(a)) return;
+      for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(&s.misc[5], 1);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= scan_tiles) break;
+        scan_onepass_body(kp, s, a.t, tile);
+      }
+      if (!grid_barrier(a)) return;
+      for (int c = blockIdx.x; c < scat_chunks; c += gridDim.x) scatter_body(kp, s, c);
+      if (!grid_barrier(a)) return;
+      const int listed = s.misc[3];
+      if (listed > 0) {  // crowded cells: pre-sort their members (as the scatter's last CTA does)
+        if (listed <= kBigListCap) {
+          for (int e = blockIdx.x; e < listed; e += gridDim.x) {
+            const int c = s.big_list[e];
+            cta_sort_segment(s.perm + s.cell_lb[c], s.cell_lb[c + 1] - s.cell_lb[c]);
+          }
+        } else {
+          for (int c = blockIdx.x; c < kp.G; c += gridDim.x) {
+            const int lo = s.cell_lb[c], hi = s.cell_lb[c + 1];
+            if (hi - lo > kBigSegment) cta_sort_segment(s.perm + lo, hi - lo);
+          }
+        }
+      }
+      if (!grid_barrier(a)) return;
+      for (int t = blockIdx.x * kPersistThreads + threadIdx.x; t < n; t += gridDim.x * kPersistThreads)
+        rank_gather_one<false>(kp, s, a.o, a.w, a.t, t);
+      if (!grid_barrier(a)) return;
+      for (int g = blockIdx.x * kPersistWarps + wid; g < groups; g += gridDim.x * kPersistWarps)
+        nblist_group<1, true, kPersistWarps, true, false>(kp, s, a.t, g, wid);
+      if (!grid_barrier(a)) return;
+      persistent_pairs<0>(a, dsm);
+      if (!grid_barrier(a)) return;
+      if (sub == 1) persistent_pairs<1>(a, dsm);
+      else persistent_pairs<2>(a, dsm);
+      if (!grid_barrier(a)) return;
+    }
+  }
+}
+
 // Neighbour counts from the lists: governing stencil and boundary subset
 // (-1 for a particle whose list overflowed).
 template <int GF>
@@ -1320,6 +1499,32 @@ cudaError_t launch_rigid_contact(const KParams& kp, const Scratch& s, const zsph
   if (kp.c3o) k_rigid_contact<1, true><<<blocks, kPairBlock, 0, st>>>(kp, s, ptc, t, ranges, nb, kn, cn, dist);
   else k_rigid_contact<1, false><<<blocks, kPairBlock, 0, st>>>(kp, s, ptc, t, ranges, nb, kn, cn, dist);
   return cudaGetLastError();
+}
+
+cudaError_t persistent_grid(int* grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kPersistThreads,
+                                                            2 * pair_smem<1>(0, 0));
+  if (!e && per_sm < 1) e = cudaErrorInvalidConfiguration;
+  if (!e) *grid = per_sm * sms;
+  return e;
+}
+
+cudaError_t launch_batch_persistent(const KParams& kp, const Scratch& s, const zsph_ptc_t& o, const zsph_ptc_t& w,
+                                    const zsph_tmp_t& t, unsigned* bar, int nsteps, unsigned spin_limit, int extra,
+                                    cudaStream_t st) {
+  if (!kp.scenes || kp.p.grid_factor != 1 || kp.equations != ZSPH_EQ_DELTA || kp.c3o || kp.rigid_f ||
+      kp.stage_windows)
+    return cudaErrorInvalidValue;
+  int grid = 0;
+  cudaError_t e = persistent_grid(&grid);
+  if (e) return e;
+  PersistArgs a{kp, s, o, w, t, bar, nsteps, spin_limit, extra};
+  void* args[] = {&a};
+  return cudaLaunchCooperativeKernel((const void*)k_batch_persistent, dim3(grid), dim3(kPersistThreads), args,
+                                     2 * pair_smem<1>(0, 0), st);
 }
 
 cudaError_t launch_nb_counts(const KParams& kp, const Scratch& s, int* nb_boundary, int* nb_governing,

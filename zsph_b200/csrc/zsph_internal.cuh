@@ -225,6 +225,11 @@ struct Handle {
   SceneDev* scene_tab = nullptr;       // batched form: scene table and bases (device)
   int* scene_base = nullptr;           // [2][nscenes + 1]: particle bases, then cell bases
   int graph_steps = 1;                 // steps per replay of zsph_run's graph (zsph_autotune)
+  // batched form in one persistent launch per step (zsph_set_batch_persistent)
+  int persistent = 0;
+  unsigned* pbar = nullptr;            // the persistent kernel's grid-barrier words [2]
+  unsigned spin_limit = 1u << 22;      // polls per barrier wait (about a second)
+  int persist_graph = 0;               // 1: zsph_run replays a captured persistent launch; -1: capture refused
 };
 
 // learn.cu: frees the handle's learned-corrector state
@@ -300,6 +305,15 @@ cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc
                              int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr,
                              const FeatOut* feat = nullptr);
 cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& tmp, cudaStream_t st);
+// Batched form: nsteps full steps of every scene in one cooperative launch
+// (equations.cu, k_batch_persistent); bar: two zeroed device words of the
+// grid barrier, kept between launches.  spin_limit bounds each barrier wait;
+// extra > 0 (self-test) adds arrivals that never come.
+cudaError_t launch_batch_persistent(const KParams& kp, const Scratch& s, const zsph_ptc_t& o, const zsph_ptc_t& w,
+                                    const zsph_tmp_t& t, unsigned* bar, int nsteps, unsigned spin_limit, int extra,
+                                    cudaStream_t st);
+// CTAs of that launch (all resident at once)
+cudaError_t persistent_grid(int* grid);
 // Rigid bodies: adds to kp.rigid_f of every body particle of ptc (the state
 // the lists were built for) the contact force per unit particle mass of its
 // non-fluid neighbours that are not of its own body, within `dist` (<= 2h):
