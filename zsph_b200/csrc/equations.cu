@@ -587,6 +587,10 @@ __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg,
 struct NbB1 {  // boundary loop 1
   float4 pr, vp;
 };
+struct NbB1C {  // boundary loop 1 on reused lists: also the neighbour's current y cell
+  float4 pr, vp;
+  int cy;
+};
 
 constexpr int kWinCapB = 1536;  // boundary window capacity (candidates), 3x3 stencil
 constexpr int kWinCapG = 2048;  // governing window capacity (candidates), 3x3 stencil
@@ -653,10 +657,14 @@ __device__ __forceinline__ void boundary_one(const KParams& kp_arg, const Scratc
   // once afterwards (same value, summed in a different rounding order).
   float Lxx = 0.f, Lxy = 0.f, Lxz = 0.f, Lyy = 0.f, Lyz = 0.f, Lzz = 0.f, divv = 0.f;
   float sx = 0.f, sy = 0.f, sz = 0.f;
-  auto use1 = [&](const NbB1& nb) {
+  // reused lists: the boundary rows by the current cells (the lists' rows are the cells at build time)
+  const int cy_i = REUSE ? kp.cur_cy[i] : 0;
+  auto use1 = [&](const auto& nb) {
     const float dx = pi.x - nb.pr.x, dy = pi.y - nb.pr.y, dz = pi.z - nb.pr.z;
     if constexpr (REUSE) {
       if (!interacts(kp, dist2(dx, dy, dz))) return;
+      const int row = nb.cy - cy_i;
+      if (row < -GF || row >= GF) return;
     }
     const float q = sqrt_fast(dist2(dx, dy, dz)) * inv_h;
     const float a = 1.0f - 0.5f * q;
@@ -674,15 +682,23 @@ __device__ __forceinline__ void boundary_one(const KParams& kp_arg, const Scratc
     }
   };
   const float4* win = sm.win;
-  if (staged)
-    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapB - 1,
-                         [&](int q) { return NbB1{win[2 * q], win[2 * q + 1]}; }, use1);
-  else
-    walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
-                         [&](int q) {
-                           const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
-                           return NbB1{r.pr, r.vp};
-                         }, use1);
+  if constexpr (REUSE) {  // every list entry, classified by the current cells in use1
+    walk<GF, false, NbB1C>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
+                           [&](int q) {
+                             const ShadowRec r = s.sh.load(q);
+                             return NbB1C{r.pr, r.vp, kp.cur_cy[q]};
+                           }, use1);
+  } else {
+    if (staged)
+      walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapB - 1,
+                           [&](int q) { return NbB1{win[2 * q], win[2 * q + 1]}; }, use1);
+    else
+      walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
+                           [&](int q) {
+                             const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+                             return NbB1{r.pr, r.vp};
+                           }, use1);
+  }
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
                     Lxy * Lxy * Lzz;
@@ -1131,11 +1147,21 @@ cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, 
 }
 
 // Learned form's corrector variants: wall (rho, p) of every non-fluid
-// particle at the current (predicted) positions, from the fluid neighbours of
-// its boundary rows in the lists the predictor built (delta_ns.cu:61-85,
-// :116-131), each entry tested again against the exact threshold; summed in
-// the lists' visit order and published in the packed shadows, and in
-// ptc.rhop when no boundary pass follows (which would otherwise write it).
+// particle at the current (predicted) positions, from its fluid neighbours in
+// the lists the predictor built that lie in the boundary rows by the current
+// cells (delta_ns.cu:61-85, :116-131), each entry tested again against the
+// exact threshold; summed in the lists' visit order and published in the
+// packed shadows, and in ptc.rhop when no boundary pass follows (which would
+// otherwise write it).
+//
+// k_cur_cells: each particle's y cell index at its current position, with
+// the hash's arithmetic (hash.cu:13).
+__global__ void __launch_bounds__(kSearchBlock) k_cur_cells(KParams kp, zsph_ptc_t ptc, int* cy) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kp.n) return;
+  cy[i] = (int)floorf(__fdiv_rn(__fsub_rn(ptc.pos[3 * i + 1], kp.p.grid_ymin), kp.p.grid_size));
+}
+
 template <int GF>
 __global__ void __launch_bounds__(kPairBlock) k_walls_reuse(KParams kp, Scratch s, zsph_ptc_t ptc, zsph_tmp_t t,
                                                             int write_rhop) {
@@ -1145,17 +1171,19 @@ __global__ void __launch_bounds__(kPairBlock) k_walls_reuse(KParams kp, Scratch 
   if (fluid_of(pi.w)) return;
   const int c = t.hash[i];
   const int cnt = s.nb_cnt[i];
+  const int cy_i = kp.cur_cy[i];
   float rsum = 0.0f, wsum = 0.0f;
   auto visit = [&](int j) {
     const float4 pj = s.sh.pr(j);
     if (!fluid_of(pj.w) || !interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) return;
+    const int row = kp.cur_cy[j] - cy_i;  // the boundary rows by the current cells
+    if (row < -GF || row >= GF) return;
     wall_term(kp, s, pi, j, rsum, wsum);
   };
   if (cnt != kOverflow) {
     for (int k = 0; k < cnt; ++k) {
       const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
       const int r = (int)(e >> kRowShift);
-      if (!Stencil<GF>::boundary_row(r)) continue;
       int a, b;
       row_range<GF>(kp, t, c, r, a, b);
       const int j = a + (int)(e & kOffMask);
@@ -1163,7 +1191,6 @@ __global__ void __launch_bounds__(kPairBlock) k_walls_reuse(KParams kp, Scratch 
     }
   } else {
     for (int r = 0; r < Stencil<GF>::NR; ++r) {
-      if (!Stencil<GF>::boundary_row(r)) continue;
       int a, b;
       row_range<GF>(kp, t, c, r, a, b);
       for (int j = a; j < b; ++j)
@@ -1474,14 +1501,17 @@ cudaError_t launch_integrate(const KParams& kp, const Scratch& s, const zsph_ptc
   return cudaGetLastError();
 }
 
-cudaError_t launch_corrector_reuse(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
-                                  bool fresh_boundary, int mode, cudaStream_t st) {
-  if (kp.n == 0) return cudaSuccess;
-  if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.rigid_f || kp.stage_windows ||
-      kp.equations != ZSPH_EQ_DELTA || (mode != 0 && mode != 2))
+cudaError_t launch_corrector_reuse(const KParams& kp_in, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                                  bool fresh_boundary, int mode, int* cy, cudaStream_t st) {
+  if (kp_in.n == 0) return cudaSuccess;
+  if (kp_in.p.grid_factor != 1 || kp_in.scenes || kp_in.c3o || kp_in.rigid_f || kp_in.stage_windows ||
+      kp_in.equations != ZSPH_EQ_DELTA || (mode != 0 && mode != 2) || !cy)
     return cudaErrorInvalidValue;
+  KParams kp = kp_in;
+  kp.cur_cy = cy;
   cudaError_t e = launch_pack_shadows(kp, s, ptc, st);
   if (e) return e;
+  k_cur_cells<<<(kp.n + kSearchBlock - 1) / kSearchBlock, kSearchBlock, 0, st>>>(kp, ptc, cy);
   const int nb = thread_blocks(kp.n), sm = pair_smem<1>(0, 0);
   k_walls_reuse<1><<<nb, kPairBlock, 0, st>>>(kp, s, ptc, t, fresh_boundary ? 0 : 1);
   if (fresh_boundary) k_boundary<1, false, false, true><<<nb, kPairBlock, sm, st>>>(kp, s, ptc, t);

@@ -39,6 +39,7 @@ struct LearnState {
   float4* acc_prev = nullptr;      // [n] previous corrector-stage values (copied before a predictor)
   float4* dprev = nullptr;         // [n] D = predictor-stage value - previous corrector value
   float4* yhat = nullptr;          // [n] network outputs (judged steps)
+  int* cy = nullptr;               // [n] current y cells (list-reuse correctors)
   double* red = nullptr;           // [kRedBlocks][8] reduction partials
   double* red_host = nullptr;      // pinned copy
   bool targets_standardized = false;
@@ -233,6 +234,7 @@ void free_state(LearnState* L) {
   cudaFree(L->acc_prev);
   cudaFree(L->dprev);
   cudaFree(L->yhat);
+  cudaFree(L->cy);
   cudaFree(L->red);
   if (L->red_host) cudaFreeHost(L->red_host);
   delete L;
@@ -252,6 +254,7 @@ int ensure_state(Handle* h) {
   if (!e) e = cudaMalloc(&L->dprev, np * sizeof(float4));
   if (!e) e = cudaMemset(L->dprev, 0, np * sizeof(float4));
   if (!e) e = cudaMalloc(&L->yhat, np * sizeof(float4));
+  if (!e) e = cudaMalloc(&L->cy, np * sizeof(int));
   if (!e) e = cudaMalloc(&L->red, kRedBlocks * 8 * sizeof(double));
   if (!e) e = cudaMallocHost(&L->red_host, kRedBlocks * 8 * sizeof(double));
   if (e) {
@@ -653,7 +656,7 @@ int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, 
       } else {
         // the variant's corrector-stage values (not applied), in the predictor's order
         LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
-        LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 0, st));
+        LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 0, L->cy, st));
         LCHECK(h, "zsph_run_learned copy", cudaMemcpyAsync(L->yhat, t->acc_drhodt, acc_bytes,
                                                            cudaMemcpyDeviceToDevice, st));
       }
@@ -695,7 +698,7 @@ int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, 
       rs.learned += 1;
     } else {
       LCHECK(h, "zsph_run_learned predictor", run_substep(h, *o, *w, *t, 1, st, nullptr, nullptr));
-      LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 2, st));
+      LCHECK(h, "zsph_run_learned corrector", launch_corrector_reuse(h->kp, h->s, *o, *t, fresh, 2, L->cy, st));
       rs.learned += 1;
     }
     rs.steps += 1;

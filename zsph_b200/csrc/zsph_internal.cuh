@@ -53,6 +53,10 @@ struct KParams {
   // resident CTAs per SM (1, 6, 8), i.e. its register budget.
   int tune_cw;
   int tune_minb;
+  // Learned form's list-reuse correctors (null otherwise): each particle's
+  // grid row (y cell index) at the current positions, which decides the
+  // boundary stencil's asymmetric rows y in [-GF, GF) (delta_ns.cu:37).
+  const int* cur_cy;
 };
 
 // Original-index range [first, first + count) of one rigid body.
@@ -293,8 +297,9 @@ cudaError_t launch_pack_shadows(const KParams& kp, const Scratch& s, const zsph_
 // (rho, p) at the predicted positions, optionally a fresh boundary pass
 // (else tmp.dofv_grandrho keeps the predictor's values), then governing with
 // mode 0 (acc_drhodt only) or 2 (correction written in place into ptc).
+// cy: n ints of scratch for the particles' current y cell indices.
 cudaError_t launch_corrector_reuse(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
-                                  bool fresh_boundary, int mode, cudaStream_t st);
+                                  bool fresh_boundary, int mode, int* cy, cudaStream_t st);
 cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                             cudaStream_t st, Prof* pf = nullptr);
 // one-time kernel attributes (shared-memory windows above 48 KB); call before launches
