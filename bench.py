@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--no-tune", action="store_true", help="default launch shapes instead of zsph_autotune's")
     ap.add_argument("--ref-cuda-child", choices=["plain", "profiled"], default=None,
                     help=argparse.SUPPRESS)  # one reference-CUDA run in a fresh process (reference arm)
-    ap.add_argument("--shapes", default=None, metavar="CW,MINB,SPG",
+    ap.add_argument("--shapes", default=None, metavar="CW,MINB,SPG[,SEGS]",
                     help="apply these launch shapes (zsph_set_launch_shapes) instead of running zsph_autotune")
     return ap.parse_args()
 
@@ -444,9 +444,12 @@ def run_ours(args, dist: Dist):
 
     # launch shapes from the project's autotuner (untimed; it restores the state after every trial)
     if args.shapes:
-        cw, mb, spg = (int(v) for v in args.shapes.split(","))
-        sol.set_launch_shapes(cw, mb, spg)
-        tune = {"list_cells_per_cta": cw, "governing_min_ctas": mb, "steps_per_graph": spg, "applied": True}
+        vals = [int(v) for v in args.shapes.split(",")]
+        cw, mb, spg = vals[:3]
+        sg = vals[3] if len(vals) > 3 else 0
+        sol.set_launch_shapes(cw, mb, spg, sg)
+        tune = {"list_cells_per_cta": cw, "governing_min_ctas": mb, "steps_per_graph": spg, "list_segments": sg,
+                "applied": True}
     else:
         tune = None if args.no_tune else sol.autotune(3, sptr)
 

@@ -452,9 +452,10 @@ int zsph_persistent_barrier_test(zsph_handle_t* h, int spin_limit, void* stream)
 
 /* ---- Autotuner (no reference counterpart) ----------------------------------
  * Times every candidate launch shape of the grid-factor-1 step -- cells
- * (warps) per CTA of the neighbour-list build {2, 4}, minimum resident CTAs
- * per SM of the governing kernel {1, 6, 8} (its register budget), steps per
- * graph replay of zsph_run {1, 4} -- for trial_steps steps each on the
+ * (warps) per CTA of the neighbour-list build {2, 4}, cells (segments) a
+ * list-build warp handles together per round {2, 3, 4}, minimum resident
+ * CTAs per SM of the governing kernel {1, 6, 8} (its register budget), steps
+ * per graph replay of zsph_run {1, 4} (36 candidates) -- for trial_steps steps each on the
  * handle's buffers, restores old_ and the carried tmp arrays after every
  * trial, and keeps the fastest for the handle's later zsph_run calls. */
 typedef struct {
@@ -462,15 +463,16 @@ typedef struct {
   float ms_per_step;  /* of the chosen shapes */
   float ms_default;   /* of the untuned shapes */
   int candidates;
+  int list_segments;  /* list build: cells handled together per round {2, 3, 4} (0: the default, 4) */
 } zsph_tune_t;
 int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_ptc_t* new_, const zsph_tmp_t* tmp,
                   int trial_steps, zsph_tune_t* out, void* stream);
 /* Applies launch shapes chosen earlier (a zsph_autotune result kept by the
  * caller, e.g. across restarts of the same case) without timing anything:
- * list_cells_per_cta, governing_min_ctas and steps_per_graph from the
- * candidate sets above, 0 for each one's default (2 warps, 1 CTA, 1 step:
- * the shapes the tuner picks on the dam-break cases); the time fields are
- * ignored.  ZSPH_EINVAL for any other value. */
+ * list_cells_per_cta, list_segments, governing_min_ctas and steps_per_graph
+ * from the candidate sets above, 0 for each one's default (2 warps, 4
+ * segments, 1 CTA, 1 step); the time fields are ignored.  ZSPH_EINVAL for any
+ * other value. */
 int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes);
 
 /* ---- Precision form (no reference counterpart) ----------------------------

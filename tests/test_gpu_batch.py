@@ -51,7 +51,7 @@ def test_autotune_keeps_state_and_results(scenes):
     before = a.download("old")
     r = a.autotune(2)
     print("tune", r)
-    assert r["candidates"] == 12 and r["ms_per_step"] > 0 and r["ms_per_step"] <= r["ms_default"] * 1.0001
+    assert r["candidates"] == 36 and r["ms_per_step"] > 0 and r["ms_per_step"] <= r["ms_default"] * 1.0001
     after = a.download("old")
     for k in ("pos", "vel", "rhop", "type", "table"):
         assert np.array_equal(getattr(before, k), getattr(after, k)), k
@@ -68,7 +68,7 @@ def test_autotune_batch(scenes):
     bt = z.Solver.from_batch(scenes)
     r = bt.autotune(2)
     print("batch tune", r)
-    assert r["candidates"] == 12
+    assert r["candidates"] == 36
     bt.run(5)
     assert bt.status() == 0
     bt.close()
@@ -80,15 +80,15 @@ def test_set_launch_shapes_applies_every_candidate_bit_identically(scenes):
     ref.run(6)
     want = ref.download("old")
     ref.close()
-    for cw, mb, spg in ((2, 1, 4), (4, 8, 1), (2, 6, 4), (0, 0, 0)):
+    for cw, mb, spg, sg in ((2, 1, 4, 2), (4, 8, 1, 3), (2, 6, 4, 4), (0, 0, 0, 0), (4, 1, 1, 2)):
         s = z.Solver.from_case(c)
-        s.set_launch_shapes(cw, mb, spg)
+        s.set_launch_shapes(cw, mb, spg, sg)
         s.run(6)
         got = s.download("old")
         assert s.status() == 0
         for k in ("pos", "vel", "rhop", "type", "table"):
-            assert np.array_equal(getattr(got, k), getattr(want, k)), (cw, mb, spg, k)
-        for bad in ((3, 0, 0), (0, 5, 0), (0, 0, 2), (-1, 0, 0)):
+            assert np.array_equal(getattr(got, k), getattr(want, k)), (cw, mb, spg, sg, k)
+        for bad in ((3, 0, 0, 0), (0, 5, 0, 0), (0, 0, 2, 0), (-1, 0, 0, 0), (0, 0, 0, 1), (0, 0, 0, 5)):
             with pytest.raises(z.ZsphError):
                 s.set_launch_shapes(*bad)
         s.close()

@@ -158,7 +158,7 @@ class TuneResult(ctypes.Structure):
     """zsph_tune_t."""
     _fields_ = [("list_cells_per_cta", ctypes.c_int), ("governing_min_ctas", ctypes.c_int),
                 ("steps_per_graph", ctypes.c_int), ("ms_per_step", ctypes.c_float), ("ms_default", ctypes.c_float),
-                ("candidates", ctypes.c_int)]
+                ("candidates", ctypes.c_int), ("list_segments", ctypes.c_int)]
 
 
 def _as_dict(s: ctypes.Structure) -> dict:
@@ -403,10 +403,10 @@ class Solver:
         return _as_dict(r)
 
     def set_launch_shapes(self, list_cells_per_cta: int = 0, governing_min_ctas: int = 0,
-                          steps_per_graph: int = 0) -> None:
+                          steps_per_graph: int = 0, list_segments: int = 0) -> None:
         """Applies launch shapes from an earlier autotune() result (0 = default) without timing."""
         r = TuneResult(list_cells_per_cta=int(list_cells_per_cta), governing_min_ctas=int(governing_min_ctas),
-                       steps_per_graph=int(steps_per_graph))
+                       steps_per_graph=int(steps_per_graph), list_segments=int(list_segments))
         self._call(lib.zsph_set_launch_shapes, ctypes.byref(r))
 
     def close(self) -> None:

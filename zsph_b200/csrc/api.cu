@@ -606,7 +606,7 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
     }
     return cudaSuccess;
   };
-  const int cws[] = {2, 4}, minbs[] = {1, 6, 8}, spgs[] = {1, 4};
+  const int cws[] = {2, 4}, segss[] = {2, 3, 4}, minbs[] = {1, 6, 8}, spgs[] = {1, 4};
   zsph_tune_t best{};
   best.ms_per_step = 1e30f;
   float ms_default = 0.f;
@@ -618,10 +618,12 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
   if (!e) e = cudaEventCreate(&e0);
   if (!e) e = cudaEventCreate(&e1);
   for (int cw : cws)
+    for (int sg : segss)
     for (int mb : minbs)
       for (int spg : spgs) {
         if (e) break;
         h->kp.tune_cw = cw;
+        h->kp.tune_segs = sg;
         h->kp.tune_minb = mb;
         h->graph_steps = spg;
         if (h->graph) {
@@ -640,10 +642,11 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
         if (e) break;
         ms /= (float)(launches * spg);
         ++count;
-        if (cw == 2 && mb == 1 && spg == 1) ms_default = ms;  // the untuned shapes
+        if (cw == 2 && sg == 4 && mb == 1 && spg == 1) ms_default = ms;  // the untuned shapes
         if (ms < best.ms_per_step) {
           best.ms_per_step = ms;
           best.list_cells_per_cta = cw;
+          best.list_segments = sg;
           best.governing_min_ctas = mb;
           best.steps_per_graph = spg;
         }
@@ -664,6 +667,7 @@ int zsph_autotune(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, co
     return cuda_fail(h, "zsph_autotune", e ? e : re);
   }
   h->kp.tune_cw = best.list_cells_per_cta;
+  h->kp.tune_segs = best.list_segments;
   h->kp.tune_minb = best.governing_min_ctas;
   h->graph_steps = best.steps_per_graph;
   best.candidates = count;
@@ -682,11 +686,15 @@ int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes) {
     return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: governing_min_ctas must be 0 (default), 1, 6 or 8");
   if (spg != 0 && spg != 1 && spg != 4)
     return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: steps_per_graph must be 0 (default), 1 or 4");
+  const int sg = shapes->list_segments;
+  if (sg != 0 && sg != 2 && sg != 3 && sg != 4)
+    return set_err(h, ZSPH_EINVAL, "zsph_set_launch_shapes: list_segments must be 0 (default), 2, 3 or 4");
   if (h->graph) {  // captured with the previous shapes
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
   }
   h->kp.tune_cw = cw;
+  h->kp.tune_segs = sg;
   h->kp.tune_minb = mb;
   h->graph_steps = spg ? spg : 1;
   return ZSPH_OK;

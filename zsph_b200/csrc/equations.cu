@@ -402,13 +402,13 @@ template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 // 32*group .. 32*group+31); k_nblist_seq runs one group per warp, the
 // batched form's persistent kernel loops over groups.  The warp's staging
 // arrays are slot `wid` of the CTA's CW slots.
-template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE>
+template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs>
 __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_tmp_t& t, int group,
                                              int wid) {
   constexpr int NR = Stencil<GF>::NR;
   // per segment (cell) of a round: its 64 staged candidates' x, y and z; the
   // two floats of padding per array put the segments' arrays in different banks
-  __shared__ __align__(16) float s_c[CW][kSegs][3][kStage];
+  __shared__ __align__(16) float s_c[CW][SEGS][3][kStage];
   // per lane: a 32-entry ring (a partial 8-entry block plus one half block's
   // hits fit), padded to 80 bytes so that the lanes' rings spread over the banks
   __shared__ __align__(16) uint16_t s_ring[CW][32][kRing + 8];
@@ -447,10 +447,10 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   unsigned todo = __ballot_sync(0xffffffffu, act);
   while (todo) {
     const unsigned sm = starts & todo;  // todo is a run of whole cells
-    const int seg = ((todo >> lane) & 1u) ? __popc(sm & (0xffffffffu >> (31 - lane))) - 1 : kSegs;
-    const bool inseg = seg < kSegs;
+    const int seg = ((todo >> lane) & 1u) ? __popc(sm & (0xffffffffu >> (31 - lane))) - 1 : SEGS;
+    const bool inseg = seg < SEGS;
     todo &= ~__ballot_sync(0xffffffffu, inseg);
-    const int nseg = min(__popc(sm), kSegs);
+    const int nseg = min(__popc(sm), SEGS);
     const float* sx = s_c[wid][inseg ? seg : 0][0];  // y and z follow at kStage, 2 * kStage
     for (int r = 0; r < NR; ++r) {
       int sl = 0, el = 0;
@@ -578,10 +578,10 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
 }
 
-template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false>
+template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs>
 __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
   const int wid = threadIdx.x >> 5;
-  nblist_group<GF, WALL, CW, BATCH, PRECISE>(kp_arg, s, t, blockIdx.x * CW + wid, wid);
+  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS>(kp_arg, s, t, blockIdx.x * CW + wid, wid);
 }
 
 struct NbB1 {  // boundary loop 1
@@ -1014,9 +1014,17 @@ template <bool WALL, bool BATCH>
 void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
   // default (0): two warps per CTA, what zsph_autotune picks on the dam-break cases
-  switch (kp.tune_cw) {
-    case 4: k_nblist_seq<1, WALL, 4, BATCH><<<(kp.n + 127) / 128, 128, 0, st>>>(kp, s, t); break;
-    default: k_nblist_seq<1, WALL, 2, BATCH><<<(kp.n + 63) / 64, 64, 0, st>>>(kp, s, t); break;
+  // default segments per round (0): four
+  const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
+  const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
+  if (kp.tune_cw == 4) {
+    if (segs == 2) k_nblist_seq<1, WALL, 4, BATCH, false, 2><<<g4, 128, 0, st>>>(kp, s, t);
+    else if (segs == 3) k_nblist_seq<1, WALL, 4, BATCH, false, 3><<<g4, 128, 0, st>>>(kp, s, t);
+    else k_nblist_seq<1, WALL, 4, BATCH, false, 4><<<g4, 128, 0, st>>>(kp, s, t);
+  } else {
+    if (segs == 2) k_nblist_seq<1, WALL, 2, BATCH, false, 2><<<g2, 64, 0, st>>>(kp, s, t);
+    else if (segs == 3) k_nblist_seq<1, WALL, 2, BATCH, false, 3><<<g2, 64, 0, st>>>(kp, s, t);
+    else k_nblist_seq<1, WALL, 2, BATCH, false, 4><<<g2, 64, 0, st>>>(kp, s, t);
   }
 }
 

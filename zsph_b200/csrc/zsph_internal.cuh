@@ -53,6 +53,7 @@ struct KParams {
   // resident CTAs per SM (1, 6, 8), i.e. its register budget.
   int tune_cw;
   int tune_minb;
+  int tune_segs;         // list build: cells (segments) per round, 2, 3 or 4 (0 = 4)
   // Learned form's list-reuse correctors (null otherwise): each particle's
   // grid row (y cell index) at the current positions, which decides the
   // boundary stencil's asymmetric rows y in [-GF, GF) (delta_ns.cu:37).
