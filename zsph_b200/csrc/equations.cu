@@ -1541,7 +1541,11 @@ cudaError_t launch_rigid_contact(const KParams& kp, const Scratch& s, const zsph
 
 cudaError_t persistent_grid(int* grid) {
   int dev = 0, sms = 0, per_sm = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  // 46 KB of static shared memory (the list build's staging) plus the two
+  // pair blocks' row arrays: above the 48 KB a launch gets without opting in
+  cudaError_t e = cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       2 * pair_smem<1>(0, 0));
+  if (!e) e = cudaGetDevice(&dev);
   if (!e) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (!e) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kPersistThreads,
                                                             2 * pair_smem<1>(0, 0));
