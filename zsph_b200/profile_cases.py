@@ -5,7 +5,7 @@ kernel family at a time (python -m zsph_b200.profile_cases CASE).
                full-size dam break): pack, then three forward passes
   mlp_train    k_mlp training mode (forward + backward, one partial row per
                CTA) over the same rows, then k_adam, three iterations
-  rigid        the floating cube (dx = 0.02 m, 321,708 particles) with
+  rigid        the floating cube (dx = 0.02 m, 362,408 particles) with
                contact on: two steps (k_rigid_contact, k_rigid_sum,
                k_rigid_step, k_rigid_place) and the FP64 sums (k_conserve)
 
