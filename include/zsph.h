@@ -45,7 +45,8 @@ enum {
   ZSPH_FLAG_KILLED = 2,      /* a particle left the grid and became type 100 */
   ZSPH_FLAG_NB_OVERFLOW = 4, /* a neighbour list overflowed (handled, slower path) */
   ZSPH_FLAG_BAD_KEY = 8,     /* zsph_sort_index got a hash outside [0, grid_num) */
-  ZSPH_FLAG_TIMEOUT = 16     /* a bounded wait for a shared-memory staging copy gave up (slower path taken) */
+  ZSPH_FLAG_TIMEOUT = 16     /* a bounded device-side wait gave up: a staging copy (slower path taken), the
+                                search's scan look-back, or a persistent kernel's grid barrier */
 };
 
 /* cpu_json_t (single_gpu_sph_src/header/data_structure.cuh:6-51); the three
@@ -228,7 +229,8 @@ int zsph_launches_per_step(zsph_handle_t* h);
 
 /* Synchronises the handle's last stream and returns the accumulated device
  * status bits (ZSPH_FLAG_*), clearing them when clear != 0.  Returns
- * ZSPH_ENAN if the NAN bit is set, else ZSPH_OK (or ZSPH_ECUDA). */
+ * ZSPH_ENAN if the NAN bit is set, ZSPH_ETIMEOUT if the TIMEOUT bit is set,
+ * ZSPH_EINVAL if the BAD_KEY bit is set, else ZSPH_OK (or ZSPH_ECUDA). */
 int zsph_status(zsph_handle_t* h, int* flags, int clear);
 /* Copies the last error message of the handle (or of the library when h is
  * NULL) into buf; returns its length. */
