@@ -11,8 +11,32 @@ from zsph_b200 import cases
 pytestmark = pytest.mark.gpu
 
 
+def _on_cell_faces(n, seed):
+    """Random cloud with most coordinates on a cell face (including the grid's
+    far faces, which kill the particle) or a few ulps to either side of it:
+    the inputs where the hash's quotient is within rounding of an integer."""
+    c = cases.random_cloud(n, seed)
+    p = po.Oracle(c.json, c.state, np.float32).p
+    rng = np.random.default_rng(seed)
+    pos = c.state.pos
+    size = np.float32(p.grid_size)
+    for ax, (lo, dim) in enumerate(((p.grid_xmin, p.grid_xdim), (p.grid_ymin, p.grid_ydim),
+                                    (p.grid_zmin, p.grid_zdim))):
+        pick = rng.uniform(size=n) < 0.8
+        m = rng.integers(0, dim + 1, size=n).astype(np.float32)
+        v = (np.float32(lo) + m * size).astype(np.float32)
+        ulps = rng.choice([-64, -16, -3, -2, -1, 0, 0, 0, 1, 2, 3, 16, 64], size=n)
+        for k in range(64):
+            more = np.abs(ulps) > k
+            v[more] = np.nextafter(v[more], np.where(ulps[more] > 0, np.float32(np.inf), np.float32(-np.inf)))
+        pos[pick, ax] = v[pick]
+    c.state.tmp_pos[:] = pos
+    return c
+
+
 def _cases():
     return {
+        "cloud_on_cell_faces": lambda: _on_cell_faces(6000, 31),
         "small_dam": lambda: cases.small(0.04),
         "config0_dam": cases.config0,
         "cloud_killed": lambda: cases.random_cloud(5000, 1, kill_frac=0.02),
@@ -51,7 +75,7 @@ def test_fused_search_bit_exact(name):
     sol.close()
 
 
-@pytest.mark.parametrize("name", ["small_dam", "cloud_killed", "cloud_crowded_cell0", "cloud_1"])
+@pytest.mark.parametrize("name", ["small_dam", "cloud_killed", "cloud_crowded_cell0", "cloud_1", "cloud_on_cell_faces"])
 def test_dropin_hash_sort_index_sort_data_bit_exact(name):
     c = _cases()[name]()
     sol = z.Solver.from_case(c)

@@ -485,7 +485,7 @@ int zsph_governing(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp_t* tm
   if (int rc = check_tmp(h, tmp)) return rc;
   h->last_stream = as_stream(stream);
   ZCHECK(h, "zsph_governing pack", launch_pack(h->kp, h->s, *ptc, *tmp, h->last_stream));
-  ZCHECK(h, "zsph_governing list", launch_nblist(h->kp, h->s, *tmp, h->last_stream));
+  ZCHECK(h, "zsph_governing list", launch_nblist(h->kp, h->s, *ptc, *tmp, h->last_stream));
   ZCHECK(h, "zsph_governing", launch_governing(h->kp, h->s, *ptc, *tmp, 0, *ptc, h->last_stream));
   return ZSPH_OK;
 }
@@ -764,7 +764,7 @@ int zsph_neighbor_counts(zsph_handle_t* h, const zsph_ptc_t* ptc, const zsph_tmp
   if (int rc = check_tmp(h, tmp)) return rc;
   h->last_stream = as_stream(stream);
   ZCHECK(h, "zsph_neighbor_counts pack", launch_pack(h->kp, h->s, *ptc, *tmp, h->last_stream));
-  ZCHECK(h, "zsph_neighbor_counts list", launch_nblist(h->kp, h->s, *tmp, h->last_stream));
+  ZCHECK(h, "zsph_neighbor_counts list", launch_nblist(h->kp, h->s, *ptc, *tmp, h->last_stream));
   ZCHECK(h, "zsph_neighbor_counts", launch_nb_counts(h->kp, h->s, nb_boundary, nb_governing, h->last_stream));
   return ZSPH_OK;
 }

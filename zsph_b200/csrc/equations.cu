@@ -335,6 +335,33 @@ __device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, f
   wsum += w;
 }
 
+// Particle j's position from the sorted arrays, in the precision form moved
+// into the frame of cell ci (the list build reads the arrays: it writes the
+// packed records itself).
+template <bool PRECISE>
+__device__ __forceinline__ float4 ptc_xyz(const KParams& kp, const zsph_ptc_t& ptc, int j, int3 ci) {
+  const float4 p = make_float4(ptc.pos[3 * j], ptc.pos[3 * j + 1], ptc.pos[3 * j + 2], 0.0f);
+  return PRECISE ? shifted(kp, p, kp.c3n[j], ci) : p;
+}
+
+// wall_term with the fluid neighbour's data from the sorted arrays
+template <bool PRECISE = false>
+__device__ __forceinline__ void wall_term_ptc(const KParams& kp, const zsph_ptc_t& ptc, float4 pi, int j,
+                                              float& rsum, float& wsum, int3 ci = int3{0, 0, 0}) {
+  if (ptc.type[j] != 1) return;
+  const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
+  const float2 rp = reinterpret_cast<const float2*>(ptc.rhop)[j];
+  const zsph_gpu_param_t& p = kp.p;
+  const float dz = pi.z - pj.z;
+  const float q = __fsqrt_rn(dist2(pi.x - pj.x, pi.y - pj.y, dz)) / p.h;
+  const float aa = 1.0f - q / 2.0f;
+  float w = aa * aa * aa;
+  w = w * aa;
+  w *= (2.0f * q + 1.0f) * p.adh;
+  rsum += (rp.y - fabsf(rp.x) * ((0.0f - p.g) * dz)) * w;
+  wsum += w;
+}
+
 using u64 = unsigned long long;
 // Packed FP32 pairs (sm_100 f32x2 instructions): each half is rounded
 // exactly as the scalar operation, so r^2 keeps the reference's rounding.
@@ -403,8 +430,8 @@ template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 // batched form's persistent kernel loops over groups.  The warp's staging
 // arrays are slot `wid` of the CTA's CW slots.
 template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs>
-__device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_tmp_t& t, int group,
-                                             int wid) {
+__device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
+                                             const zsph_tmp_t& t, int group, int wid) {
   constexpr int NR = Stencil<GF>::NR;
   // per segment (cell) of a round: its 64 staged candidates' x, y and z; the
   // two floats of padding per array put the segments' arrays in different banks
@@ -420,7 +447,11 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   const int c = act ? t.hash[i] : INT_MAX;  // sorted: non-decreasing over the lanes
   // batched form: the scene of the lane's cell (scenes own disjoint cell ranges)
   const int scn = BATCH && act ? scene_of(kp_arg.scene_cbase, kp_arg.nscenes, c) : 0;
-  const float4 pi = s.sh.pr(act ? i : p0);
+  // the lane's own position and packed density (its record is written at the end)
+  const int iself = act ? i : p0;
+  const float2 rp_self = reinterpret_cast<const float2*>(ptc.rhop)[iself];
+  const float4 pi = make_float4(ptc.pos[3 * iself], ptc.pos[3 * iself + 1], ptc.pos[3 * iself + 2],
+                                packed_rho(rp_self.x, ptc.type[iself]));
   // precision form: the lane's own cell (its position is the offset from that cell's corner)
   const int3 ci = PRECISE && act ? unpack_cell(kp_arg.c3n[i]) : int3{0, 0, 0};
   // the lane's scene (batched form): its cell's neighbour threshold and grid
@@ -473,7 +504,7 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
           for (int h = 0; h < 2; ++h) {
             const int o = k0 + 32 * h + lane;
             float4 q = make_float4(3e37f, 3e37f, 3e37f, 0.f);  // padding never passes the test
-            if (o < lg) q = shadow_pr<PRECISE>(kp, s, sg + o, cg);
+            if (o < lg) q = ptc_xyz<PRECISE>(kp, ptc, sg + o, cg);
             s_c[wid][g][0][32 * h + lane] = q.x;
             s_c[wid][g][1][32 * h + lane] = q.y;
             s_c[wid][g][2][32 * h + lane] = q.z;
@@ -545,6 +576,8 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   }
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
+  float rho_w = 0.0f, p_w = 0.0f;
+  bool wall_new = false;
   if (WALL && act && !fluid_of(pi.w)) {
     float rsum = 0.0f, wsum = 0.0f;
     if (!ovf) {
@@ -554,7 +587,7 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
         if (Stencil<GF>::boundary_row(r)) {
           int a, b;  // the row's start (its cell bounds are L1-resident by now)
           row_range<GF>(kp, t, c, r, a, b);
-          wall_term<PRECISE>(kp, s, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
+          wall_term_ptc<PRECISE>(kp, ptc, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
         }
       }
     } else {
@@ -564,24 +597,36 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
         row_range<GF>(kp, t, c, r, a, b);
         for (int j = a; j < b; ++j) {
           if (j == i) continue;
-          const float4 pj = shadow_pr<PRECISE>(kp, s, j, ci);
-          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term<PRECISE>(kp, s, pi, j, rsum, wsum, ci);
+          const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
+          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term_ptc<PRECISE>(kp, ptc, pi, j, rsum, wsum, ci);
         }
       }
     }
     const zsph_gpu_param_t& p = kp.p;
     if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
     if (rsum < 0.0f) rsum = 0.0f;
-    s.sh.pr(i).w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-    s.sh.vp(i).w = rsum;
+    rho_w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+    p_w = rsum;
+    wall_new = true;
   }
-  if (act) s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+  if (act) {
+    // the lane's packed record, with a wall's new (rho, p)
+    float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
+    float4 pr = pi;
+    if (wall_new) {
+      pr.w = rho_w;
+      vp.w = p_w;
+    }
+    st_rec(&s.sh.pr(i), pr, vp);
+    s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+  }
 }
 
 template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs>
-__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_tmp_t t) {
+__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_ptc_t ptc,
+                                                                   zsph_tmp_t t) {
   const int wid = threadIdx.x >> 5;
-  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS>(kp_arg, s, t, blockIdx.x * CW + wid, wid);
+  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS>(kp_arg, s, ptc, t, blockIdx.x * CW + wid, wid);
 }
 
 struct NbB1 {  // boundary loop 1
@@ -1011,20 +1056,21 @@ inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 
 // list build (grid factor 1) with the tuned number of cells per CTA
 template <bool WALL, bool BATCH>
-void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
+void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                         cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
   // default (0): two warps per CTA, what zsph_autotune picks on the dam-break cases
   // default segments per round (0): four
   const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
   const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
   if (kp.tune_cw == 4) {
-    if (segs == 2) k_nblist_seq<1, WALL, 4, BATCH, false, 2><<<g4, 128, 0, st>>>(kp, s, t);
-    else if (segs == 3) k_nblist_seq<1, WALL, 4, BATCH, false, 3><<<g4, 128, 0, st>>>(kp, s, t);
-    else k_nblist_seq<1, WALL, 4, BATCH, false, 4><<<g4, 128, 0, st>>>(kp, s, t);
+    if (segs == 2) k_nblist_seq<1, WALL, 4, BATCH, false, 2><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, WALL, 4, BATCH, false, 3><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, WALL, 4, BATCH, false, 4><<<g4, 128, 0, st>>>(kp, s, ptc, t);
   } else {
-    if (segs == 2) k_nblist_seq<1, WALL, 2, BATCH, false, 2><<<g2, 64, 0, st>>>(kp, s, t);
-    else if (segs == 3) k_nblist_seq<1, WALL, 2, BATCH, false, 3><<<g2, 64, 0, st>>>(kp, s, t);
-    else k_nblist_seq<1, WALL, 2, BATCH, false, 4><<<g2, 64, 0, st>>>(kp, s, t);
+    if (segs == 2) k_nblist_seq<1, WALL, 2, BATCH, false, 2><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, WALL, 2, BATCH, false, 3><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, WALL, 2, BATCH, false, 4><<<g2, 64, 0, st>>>(kp, s, ptc, t);
   }
 }
 
@@ -1049,7 +1095,7 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
                         cudaStream_t st, Prof* pf) {
   if (kp.scenes) {  // batched form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA || kp.c3o) return cudaErrorInvalidValue;
-    launch_nblist_tuned<true, true>(kp, s, t, st);
+    launch_nblist_tuned<true, true>(kp, s, ptc, t, st);
     mark(pf, "nblist_wall", st);
     k_boundary<1, false, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
     mark(pf, "boundary", st);
@@ -1057,14 +1103,14 @@ cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& p
   }
   if (kp.c3o) {  // precision form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
-    k_nblist_seq<1, true, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<1, true, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
     mark(pf, "nblist_wall", st);
     k_boundary<1, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
     mark(pf, "boundary", st);
     return cudaGetLastError();
   }
-  if (GF == 1) launch_nblist_tuned<true, false>(kp, s, t, st);
-  else k_nblist_seq<GF, true, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, t);
+  if (GF == 1) launch_nblist_tuned<true, false>(kp, s, ptc, t, st);
+  else k_nblist_seq<GF, true, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
   mark(pf, "nblist_wall", st);
   if (kp.equations == ZSPH_EQ_SIMPLE)
     k_boundary_simple<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, ptc, t);
@@ -1141,15 +1187,16 @@ cudaError_t governing_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
 }
 
 template <int GF>
-cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
+cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                      cudaStream_t st) {
   if (kp.scenes) {
     if (GF != 1) return cudaErrorInvalidValue;
-    launch_nblist_tuned<false, true>(kp, s, t, st);
+    launch_nblist_tuned<false, true>(kp, s, ptc, t, st);
   } else if (kp.c3o) {
     if (GF != 1) return cudaErrorInvalidValue;
-    k_nblist_seq<1, false, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<1, false, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
   } else {
-    k_nblist_seq<GF, false, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, t);
+    k_nblist_seq<GF, false, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
   }
   return cudaGetLastError();
 }
@@ -1415,7 +1462,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_batch_persistent(Persist
         rank_gather_one<false>(kp, s, a.o, a.w, a.t, t);
       if (!grid_barrier(a)) return;
       for (int g = blockIdx.x * kPersistWarps + wid; g < groups; g += gridDim.x * kPersistWarps)
-        nblist_group<1, true, kPersistWarps, true, false>(kp, s, a.t, g, wid);
+        nblist_group<1, true, kPersistWarps, true, false>(kp, s, a.w, a.t, g, wid);
       if (!grid_barrier(a)) return;
       persistent_pairs<0>(a, dsm);
       if (!grid_barrier(a)) return;
@@ -1484,10 +1531,11 @@ cudaError_t launch_boundary(const KParams& kp, const Scratch& s, const zsph_ptc_
   return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
+cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                          cudaStream_t st) {
   if (kp.n == 0) return cudaSuccess;
-  if (kp.p.grid_factor == 1) return nblist_gf<1>(kp, s, t, st);
-  if (kp.p.grid_factor == 2) return nblist_gf<2>(kp, s, t, st);
+  if (kp.p.grid_factor == 1) return nblist_gf<1>(kp, s, ptc, t, st);
+  if (kp.p.grid_factor == 2) return nblist_gf<2>(kp, s, ptc, t, st);
   return cudaErrorInvalidValue;
 }
 

@@ -239,7 +239,9 @@ __global__ void __launch_bounds__(1024) k_sort_big_cells(KParams kp, Scratch sc)
 }
 
 // Fused search, last step: rank, write sorted hash/index, gather the eight
-// particle arrays (sort.cu:62-82) and the packed shadows (rank_gather_one).
+// particle arrays (sort.cu:62-82) (rank_gather_one).  The packed records of
+// the sorted state are written by the list build, which reads each
+// particle's arrays anyway.
 __global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
                                                               zsph_tmp_t t) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,7 +265,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_gather_by_index(KParams kp, Sc
                                                                   zsph_ptc_t w, zsph_tmp_t t) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= kp.n) return;
-  gather_one(o, w, sc.sh, t.index[slot], slot);
+  gather_one(o, w, t.index[slot], slot);
 }
 
 // Exact per-cell particle ranges [cell_lb[c], cell_lb[c+1]) of an already

@@ -22,12 +22,30 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Cell hash of one position, exactly as hash.cu:12-15 computes it (IEEE
-// subtract and divide, floorf, float->int conversion, int multiply-add).
-__device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, float y, float z) {
-  const int hx = (int)floorf(__fdiv_rn(__fsub_rn(x, p.grid_xmin), p.grid_size));
-  const int hy = (int)floorf(__fdiv_rn(__fsub_rn(y, p.grid_ymin), p.grid_size));
-  const int hz = (int)floorf(__fdiv_rn(__fsub_rn(z, p.grid_zmin), p.grid_size));
+// floorf(a / c) with a correctly rounded division, for c > 0 and rc the
+// correctly rounded 1 / c, without the division in the common case.
+// q = a * rc is within 2^-23 |a / c| (relative) of a / c, and the rounded
+// quotient within 2^-24: both lie within 2^-22 |q| of q.  When q is farther
+// than 2^-20 |q| from every integer (and not tiny, where the bound would be
+// absolute), q, a / c and its rounding share one floor.  Otherwise (q near a
+// cell face, NaN, infinite) the division is taken as written.  The distance
+// d is exact: q - floor(q) and floor(q) + 1 - q subtract numbers within a
+// factor two of each other (or from zero).
+__device__ __forceinline__ int floor_quot(float a, float c, float rc) {
+  const float q = __fmul_rn(a, rc);
+  const float f = floorf(q);
+  const float d = fminf(__fsub_rn(q, f), __fsub_rn(__fadd_rn(f, 1.0f), q));
+  if (d > fmaxf(fabsf(q) * 0x1p-20f, 0x1p-100f)) return (int)f;
+  return (int)floorf(__fdiv_rn(a, c));
+}
+
+// Cell hash of one position, as hash.cu:12-15 computes it (IEEE subtract and
+// divide, floorf, float->int conversion, int multiply-add); rc is
+// __frcp_rn(p.grid_size) and the divisions go through floor_quot.
+__device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, float y, float z, float rc) {
+  const int hx = floor_quot(__fsub_rn(x, p.grid_xmin), p.grid_size, rc);
+  const int hy = floor_quot(__fsub_rn(y, p.grid_ymin), p.grid_size, rc);
+  const int hz = floor_quot(__fsub_rn(z, p.grid_zmin), p.grid_size, rc);
   return hz * p.grid_xdim * p.grid_ydim + hy * p.grid_xdim + hx;
 }
 
@@ -36,7 +54,7 @@ __device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, flo
 // particle's position (x, y, z) or, in the precision form, its packed cell
 // (cpk), already loaded.
 __device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_ptc_t& s, int i, float x, float y,
-                                                float z, int cpk, int* flags) {
+                                                float z, int cpk, int* flags, float rc) {
   const zsph_gpu_param_t& p = kp.p;
   int h;
   bool out;
@@ -46,7 +64,7 @@ __device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_pt
     h = (c.z * p.grid_ydim + c.y) * p.grid_xdim + c.x;
   } else {
     // batched form: the scene's cells start at grid_hash_min (0 for one scene)
-    h = cell_hash(p, x, y, z);
+    h = cell_hash(p, x, y, z, rc);
     out = h < 0 || h > p.grid_hash_max - p.grid_hash_min;
     h += p.grid_hash_min;
   }
@@ -83,7 +101,7 @@ __device__ __forceinline__ int hash_and_kill(const KParams& kp, const zsph_ptc_t
     y = s.pos[3 * i + 1];
     z = s.pos[3 * i + 2];
   }
-  return hash_and_kill_at(kp, s, i, x, y, z, cpk, flags);
+  return hash_and_kill_at(kp, s, i, x, y, z, cpk, flags, __frcp_rn(kp.p.grid_size));
 }
 
 // One atomic per distinct key per warp; returns this lane's ticket (its
@@ -139,13 +157,15 @@ __device__ __forceinline__ void hash_count_body(const KParams& kp_in, const zsph
   }
   int h[kHashItems];
   int kmax = -1;
+  const float rc0 = __frcp_rn(kp_in.p.grid_size);
 #pragma unroll
   for (int k = 0; k < kHashItems; ++k) {
     const int i = base + k * kSearchBlock;
     h[k] = 0;
     if (i < n) {
       const KParams kp = kp_of_particle(kp_in, i);
-      h[k] = hash_and_kill_at(kp, s, i, x[k], y[k], z[k], cpk[k], sc.flags);
+      const float rc = kp_in.scenes ? __frcp_rn(kp.p.grid_size) : rc0;  // a scene's own cell size
+      h[k] = hash_and_kill_at(kp, s, i, x[k], y[k], z[k], cpk[k], sc.flags, rc);
       sc.key[i] = h[k];
       kmax = max(kmax, h[k]);
     }
@@ -425,7 +445,7 @@ __device__ __forceinline__ float packed_rho(float rho, int type) {
   return type == 1 ? fabsf(rho) : -fabsf(rho);
 }
 
-__device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t& w, const Shadow& sh, int src,
+__device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t& w, int src,
                                            int dst) {
   const float x = o.pos[3 * src], y = o.pos[3 * src + 1], z = o.pos[3 * src + 2];
   const float vx = o.vel[3 * src], vy = o.vel[3 * src + 1], vz = o.vel[3 * src + 2];
@@ -443,7 +463,6 @@ __device__ __forceinline__ void gather_one(const zsph_ptc_t& o, const zsph_ptc_t
   reinterpret_cast<float2*>(w.tmp_rhop)[dst] = trp;
   w.type[dst] = ty_;
   w.table[dst] = tb + src - dst;  // sort.cu:82
-  st_rec(&sh.pr(dst), make_float4(x, y, z, packed_rho(rp.x, ty_)), make_float4(vx, vy, vz, rp.y));
 }
 
 // One particle's record of the eight reference arrays (72 bytes).
@@ -466,7 +485,7 @@ __device__ __forceinline__ void load_rec(const zsph_ptc_t& o, int src, PtcRec& r
   r.table = o.table[src];
 }
 
-__device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const Shadow& sh, const PtcRec& r, int src, int dst) {
+__device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const PtcRec& r, int src, int dst) {
   w.pos[3 * dst] = r.x; w.pos[3 * dst + 1] = r.y; w.pos[3 * dst + 2] = r.z;
   w.vel[3 * dst] = r.vx; w.vel[3 * dst + 1] = r.vy; w.vel[3 * dst + 2] = r.vz;
   reinterpret_cast<float2*>(w.rhop)[dst] = r.rp;
@@ -475,13 +494,11 @@ __device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const Shadow& sh,
   reinterpret_cast<float2*>(w.tmp_rhop)[dst] = r.trp;
   w.type[dst] = r.type;
   w.table[dst] = r.table + src - dst;  // sort.cu:82
-  st_rec(&sh.pr(dst), make_float4(r.x, r.y, r.z, packed_rho(r.rp.x, r.type)),
-         make_float4(r.vx, r.vy, r.vz, r.rp.y));
 }
 
 
 // Fused search, last step: rank, write sorted hash/index, gather the eight
-// particle arrays (sort.cu:62-82) and the packed shadows.  The source record's
+// particle arrays (sort.cu:62-82).  The source record's
 // loads are issued as soon as the source is known, before the rank (which
 // needs the key, the cell's range and its members) is counted, so they
 // overlap that dependent chain.
@@ -498,7 +515,7 @@ __device__ __forceinline__ void rank_gather_one(const KParams& kp, const Scratch
   const int dst = ranked_slot<NC>(sc, slot, i, c);
   t.index[dst] = i;
   t.hash[dst] = c;
-  store_rec(w, sc.sh, r, i, dst);
+  store_rec(w, r, i, dst);
   if (kp.c3o) kp.c3n[dst] = cpk;
 }
 

@@ -130,7 +130,9 @@ struct ShadowRec {
   float4 pr, vp;
 };
 
-// Packed per-particle shadows of the sorted state, written by the gather:
+// Packed per-particle shadows of the sorted state, written by the list build
+// (each particle's own record, with a wall's new density and pressure), or by
+// k_pack where no list build runs:
 // one 32-byte record per particle, rec[2i] = pr = {x, y, z, +-rho} with the
 // sign bit set for non-fluid particles (type != 1) and rec[2i+1] = vp =
 // {vx, vy, vz, p}, so that a pair kernel fetches a neighbour's record with
@@ -310,7 +312,8 @@ cudaError_t init_pair_kernels();
 cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                              int mode, const zsph_ptc_t& out, cudaStream_t st, Prof* pf = nullptr,
                              const FeatOut* feat = nullptr);
-cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_tmp_t& tmp, cudaStream_t st);
+cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                          cudaStream_t st);
 // Batched form: nsteps full steps of every scene in one cooperative launch
 // (equations.cu, k_batch_persistent); bar: two zeroed device words of the
 // grid barrier, kept between launches.  spin_limit bounds each barrier wait;
