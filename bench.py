@@ -235,14 +235,18 @@ def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks):
     fp32_peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
     cand = stencil_candidates(sol, n)
     out = {"fp32_peak_tflops_nominal": fp32_peak}
-    t_nb = kern.get("nblist_wall", {}).get("ms_per_step", 0) / 2e3
+    per_launch = lambda k: (kern[k]["ms_per_step"] / max(kern[k]["launches_per_step"], 1) / 1e3) if k in kern else 0
+    t_nb = per_launch("nblist_wall")
     if t_nb:
         tr = ncu_traffic("nblist_wall")
         out["nblist_wall"] = {"ms_per_substep": t_nb * 1e3, "stencil_candidates_per_particle": cand,
                               "candidate_tests_per_s": cand * n / t_nb,
                               "dram_gbs": tr / t_nb / 1e9 if tr else None}
+    for name in ("xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback"):
+        if per_launch(name):
+            out[name] = {"ms_per_substep": per_launch(name) * 1e3}
     for name, nb in (("boundary", nb_b), ("governing", nb_g)):
-        t = kern.get(name, {}).get("ms_per_step", 0) / 2e3
+        t = per_launch(name)
         if not t:
             continue
         pairs = float(np.mean(nb[nb >= 0]))
@@ -462,11 +466,14 @@ def run_ours(args, dist: Dist):
     clocks = Clocks(dev)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    xf0 = sol.list_transfer_info()
     e0.record(stream)
     sol.run(K, sptr)
     e1.record(stream)
     torch.cuda.synchronize()
     ck = clocks.stop()
+    xf1 = sol.list_transfer_info()
+    xfer = {k: xf1[k] - xf0[k] for k in xf1}
     dist.barrier()
     ms_local = e0.elapsed_time(e1)
     ms = dist.max(ms_local)
@@ -555,7 +562,7 @@ def run_ours(args, dist: Dist):
         "config": workload_config(args, case, G, cp.dt, dist.world),
         "fluid_particle_steps_per_s": dist.world * case.n_fluid * K / (ms / 1e3),
         "clocks": ck, "e2e": e2e, "gpu_launches": sol.launches_per_step() * K, "launches_per_step": launches,
-        "tune": tune,
+        "tune": tune, "list_transfer": xfer,
         "roofline": roofline, "dominant_kernel": dominant, "pair_kernels": pair, "kernels": kern, "cpu_baseline": cpu,
         "learned": learned, "batched": batched, "status_flags": flags,
     }

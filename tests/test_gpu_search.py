@@ -201,9 +201,17 @@ def test_profiled_steps_report_every_launch_and_group():
     b = z.Solver.from_case(c)
     per = a.step_profiled()
     names = [k for k, _ in per]
-    sub = ["hash_count", "scan", "scatter", "rank_gather", "nblist_wall", "boundary", "governing"]
+    search = ["hash_count", "scan", "scatter", "rank_gather"]
+    sub = search + ["nblist_wall", "boundary", "governing"]
     assert names == sub + sub
-    assert len(names) == a.launches_per_step()
+    assert len(names) == a.launches_per_step() == 14
+    # the corrector's lists by the list transfer (opt-in)
+    a.set_list_transfer(True)
+    corr = search + ["xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback", "boundary", "governing"]
+    assert [k for k, _ in a.step_profiled()] == sub + corr
+    assert a.launches_per_step() == 17
+    a.set_list_transfer(False)
+    b.step()
     grp = a.step_profiled(groups=True)
     assert [k for k, _ in grp] == ["search", "pair", "search", "pair"]
     assert all(t > 0 for _, t in per + grp)

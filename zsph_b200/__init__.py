@@ -251,6 +251,9 @@ _sig = {
                            ctypes.POINTER(TuneResult), _VP]),
     "zsph_set_launch_shapes": (_I, [_HP, ctypes.POINTER(TuneResult)]),
     "zsph_set_batch_persistent": (_I, [_HP, _I]),
+    "zsph_set_list_transfer": (_I, [_HP, _I, _F]),
+    "zsph_list_transfer_info": (_I, [_HP, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                                     ctypes.POINTER(ctypes.c_longlong)]),
     "zsph_persistent_info": (_I, [_HP, _IP, _IP]),
     "zsph_persistent_barrier_test": (_I, [_HP, _I, _VP]),
 }
@@ -586,6 +589,18 @@ class Solver:
         b = RigidBody()
         self._call(lib.zsph_rigid_get_body, int(index), ctypes.byref(b))
         return _as_dict(b)
+
+    def set_list_transfer(self, on: bool = True, skin: float = 0.05) -> None:
+        """zsph_set_list_transfer: the corrector's lists made from the predictor's
+        (bit-identical results; skin is a multiple of h, 0 = always build in full)."""
+        self._call(lib.zsph_set_list_transfer, 1 if on else 0, float(skin))
+
+    def list_transfer_info(self) -> dict:
+        """zsph_list_transfer_info: steps that transferred, steps that built in full,
+        particles that got a full search in the transferred steps."""
+        a, b, c = ctypes.c_longlong(0), ctypes.c_longlong(0), ctypes.c_longlong(0)
+        self._call(lib.zsph_list_transfer_info, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        return {"transferred": a.value, "full_builds": b.value, "full_searches": c.value}
 
     def set_persistent(self, on: bool = True) -> None:
         """zsph_set_batch_persistent (batched handles)."""

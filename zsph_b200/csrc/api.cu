@@ -118,16 +118,106 @@ int check_tmp(zsph_handle* h, const zsph_tmp_t* t) {
   return ZSPH_OK;
 }
 
+void free_xfer(Xfer& x) {
+  void* ptrs[] = {x.nb2,   x.nb_cnt2, x.sk,  x.sk_cnt, x.pos4,  x.xl,     x.xcnt,
+                  x.hashP, x.gsP,     x.geP, x.flag,   x.fullb, x.alist, x.acount, x.stats};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  std::memset(&x, 0, sizeof x);
+}
+
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
                   s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.rec};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  free_xfer(s.xf);
   std::memset(&s, 0, sizeof s);
 }
 
 template <class T> cudaError_t dalloc(T*& p, size_t count) {
   return cudaMalloc(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T));
+}
+
+// List transfer constants for a skin of xfer_skin * h: the skin lists'
+// outer radius, and the largest half-step displacement for which every pair
+// within 2h at the predicted positions lies within that radius at the old
+// ones (with margins for the FP32 rounding of both distance tests).  A
+// negative bound makes every step build in full.
+void xfer_params(zsph_handle* h) {
+  KParams& kp = h->kp;
+  const double R = (2.0 + (double)h->xfer_skin) * (double)kp.p.h;
+  kp.r2skin = (float)(R * R);
+  const double d = 0.5 * (std::sqrt((double)kp.r2skin) * (1.0 - 1e-6) - std::sqrt((double)kp.r2max) * (1.0 + 1e-6));
+  kp.disp2max = d > 0.0 ? (float)(d * d * (1.0 - 1e-6)) : -1.0f;
+}
+
+cudaError_t xfer_alloc(zsph_handle* h) {
+  Xfer& x = h->s.xf;
+  if (x.nb2) return cudaSuccess;
+  const size_t n = (size_t)h->kp.n, G = (size_t)h->kp.G, n32 = (n + 31) & ~(size_t)31;
+  cudaError_t e = dalloc(x.nb2, (size_t)kMaxNb * n32);
+  if (!e) e = dalloc(x.nb_cnt2, n);
+  if (!e) e = dalloc(x.sk, (size_t)kSkinCap * n32);
+  if (!e) e = dalloc(x.sk_cnt, n);
+  if (!e) e = dalloc(x.pos4, n);
+  if (!e) e = dalloc(x.xl, (size_t)kXtra * n);
+  if (!e) e = dalloc(x.xcnt, n);
+  if (!e) e = dalloc(x.hashP, n);
+  if (!e) e = dalloc(x.gsP, G);
+  if (!e) e = dalloc(x.geP, G);
+  if (!e) e = dalloc(x.flag, 1);
+  if (!e) e = dalloc(x.fullb, n);
+  if (!e) e = dalloc(x.alist, n);
+  if (!e) e = dalloc(x.acount, 1);
+  if (!e) e = dalloc(x.stats, 3);
+  if (!e) e = cudaMemset(x.nb_cnt2, 0, n ? n : 1);
+  if (!e) e = cudaMemset(x.sk_cnt, 0, n ? n : 1);
+  if (!e) e = cudaMemset(x.xcnt, 0, (n ? n : 1) * sizeof(int));
+  if (!e) e = cudaMemset(x.flag, 0, sizeof(int));
+  if (!e) e = cudaMemset(x.stats, 0, 3 * sizeof(unsigned long long));
+  if (!e) e = cudaDeviceSynchronize();
+  if (e) free_xfer(x);
+  return e;
+}
+
+// The plain step's corrector can take the list transfer: one scene, grid
+// factor 1, delta equations, absolute positions, no rigid body, global loads.
+bool xfer_eligible(const zsph_handle* h) {
+  const KParams& kp = h->kp;
+  return h->xfer_on && h->s.xf.nb2 && kp.n >= 64 && !kp.scenes && !kp.c3o && !kp.rigid_f && !h->rigid &&
+         kp.equations == ZSPH_EQ_DELTA && kp.p.grid_factor == 1 && !kp.stage_windows;
+}
+
+// One step with the list transfer: the predictor sub-step also makes skin
+// lists and records the predicted positions; the corrector's lists come from
+// the predictor's (or a full build, when the device flag says so).  The
+// user's tmp receives both searches' outputs as in the plain step, so cell
+// bounds keep the reference's stale-value behaviour; the predictor's hash and
+// bounds are copied aside for the transfer.
+cudaError_t xfer_step(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, const zsph_tmp_t& t, cudaStream_t st,
+                      Prof* pf) {
+  const Xfer& x = h->s.xf;
+  const size_t n = (size_t)h->kp.n, G = (size_t)h->kp.G;
+  cudaError_t e = launch_search(h->kp, h->s, h->tiles, o, w, t, st, pf);
+  if (!e) e = cudaMemsetAsync(x.flag, 0, sizeof(int), st);
+  if (!e) e = cudaMemsetAsync(x.xcnt, 0, n * sizeof(int), st);
+  if (!e) e = cudaMemsetAsync(x.acount, 0, sizeof(int), st);
+  if (!e) e = cudaMemcpyAsync(x.hashP, t.hash, n * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (!e) e = cudaMemcpyAsync(x.gsP, t.grid_start, G * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (!e) e = cudaMemcpyAsync(x.geP, t.grid_end, G * sizeof(int), cudaMemcpyDeviceToDevice, st);
+  if (!e) e = launch_xfer_pred_lists(h->kp, h->s, w, t, st, pf);
+  KParams kp1 = h->kp;
+  kp1.xfer_pos4 = x.pos4;
+  kp1.xfer_flag = x.flag;
+  if (!e) e = launch_governing(kp1, h->s, w, t, 1, o, st, pf);
+  if (!e) e = launch_search(h->kp, h->s, h->tiles, o, w, t, st, pf);
+  if (!e) e = launch_xfer_corr_lists(h->kp, h->s, w, t, st, pf);
+  Scratch s2 = h->s;
+  s2.nb = x.nb2;
+  s2.nb_cnt = x.nb_cnt2;
+  if (!e) e = launch_governing(h->kp, s2, w, t, 2, o, st, pf);
+  return e;
 }
 
 // One sub-step of the fused path: search `from` into `to`, boundary on `to`,
@@ -152,6 +242,7 @@ cudaError_t persistent_steps(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc
 cudaError_t step_launches(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, const zsph_tmp_t& t,
                           cudaStream_t st, Prof* pf = nullptr) {
   if (h->persistent && !pf) return persistent_steps(h, o, w, t, 1, st);
+  if (xfer_eligible(h)) return xfer_step(h, o, w, t, st, pf);
   cudaError_t e = substep(h, o, w, t, 1, st, pf);
   if (!e) e = substep(h, o, w, t, 2, st, pf);
   return e;
@@ -313,6 +404,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = cudaMemset(s.flags, 0, sizeof(int));
   if (!e) e = cudaMemset(s.nb_cnt, 0, n ? n : 1);
   if (!e) e = cudaDeviceSynchronize();
+  if (!e) xfer_params(h);  // the list transfer stays off (and unallocated) until zsph_set_list_transfer
   if (e) {
     const int code = cuda_fail(nullptr, "zsph_create", e);
     free_scratch(h->s);
@@ -408,6 +500,7 @@ int zsph_set_params(zsph_handle_t* h, const zsph_gpu_param_t* gp) {
   const int eq = h->kp.equations;
   fill_kparams(h->kp, *gp, h->kp.G);
   h->kp.equations = eq;
+  xfer_params(h);
   if (h->graph) {  // kernel arguments changed: re-capture on the next zsph_run
     cudaGraphExecDestroy(h->graph);
     h->graph = nullptr;
@@ -700,6 +793,33 @@ int zsph_set_launch_shapes(zsph_handle_t* h, const zsph_tune_t* shapes) {
   return ZSPH_OK;
 }
 
+int zsph_set_list_transfer(zsph_handle_t* h, int on, float skin) {
+  ENTRY_CHECKS(h);
+  if (!(skin >= 0.0f && skin <= 1.0f))
+    return set_err(h, ZSPH_EINVAL, "zsph_set_list_transfer: skin must be in [0, 1] (a multiple of h)");
+  if (on) ZCHECK(h, "zsph_set_list_transfer", xfer_alloc(h));
+  if (h->graph) {  // captured with the other step form
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->xfer_on = on ? 1 : 0;
+  h->xfer_skin = skin;
+  xfer_params(h);
+  return ZSPH_OK;
+}
+
+int zsph_list_transfer_info(zsph_handle_t* h, long long* transferred, long long* full_builds,
+                            long long* full_searches) {
+  ENTRY_CHECKS(h);
+  unsigned long long v[3] = {0, 0, 0};
+  if (h->s.xf.stats)
+    ZCHECK(h, "zsph_list_transfer_info", cudaMemcpy(v, h->s.xf.stats, sizeof v, cudaMemcpyDeviceToHost));
+  if (transferred) *transferred = (long long)v[0];
+  if (full_builds) *full_builds = (long long)v[1];
+  if (full_searches) *full_searches = (long long)v[2];
+  return ZSPH_OK;
+}
+
 int zsph_set_batch_persistent(zsph_handle_t* h, int on) {
   ENTRY_CHECKS(h);
   if (on) {
@@ -872,8 +992,11 @@ int zsph_step_profiled_groups(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_
 }
 
 int zsph_launches_per_step(zsph_handle_t* h) {
-  (void)h;
-  // per sub-step: hash_count, scan, scatter, rank_gather, nblist, boundary, governing
+  // per sub-step: hash_count, scan, scatter, rank_gather, nblist, boundary,
+  // governing; with the list transfer the corrector's nblist is
+  // xfer_classify, xfer_search, nblist_xfer and nblist_fallback (one of the
+  // last two returns at once)
+  if (h && xfer_eligible(h)) return 7 + 10;
   return 2 * 7;
 }
 

@@ -78,6 +78,10 @@ constexpr int kListVec = kMaxNb / 8;  // uint4 per particle list
 __device__ __forceinline__ size_t nb_vec(int i, int b) {
   return ((size_t)(i >> 5) * kListVec + (size_t)b) * 32 + (size_t)(i & 31);
 }
+// entry k of particle i's skin list (list transfer), blocked the same way
+__device__ __forceinline__ size_t sk_idx(int i, int k) {
+  return ((size_t)(i >> 5) * kSkinCap + (size_t)k) * 32 + (size_t)(i & 31);
+}
 
 __device__ __forceinline__ float rcp_fast(float x) {
   float r;
@@ -387,6 +391,59 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
   return r;
 }
 
+// The end of particle i's list build, once s.nb holds its finished list
+// (cnt entries, or ovf): with WALL a non-fluid particle extrapolates its
+// (rho, p) from the fluid neighbours of its boundary rows
+// (delta_ns.cu:61-85, :116-131), summed in list order; then the particle's
+// packed shadow record (with a wall's new values) and its list count.
+template <int GF, bool WALL, bool PRECISE>
+__device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc,
+                                          const zsph_tmp_t& t, int i, int c, int cnt, bool ovf, float4 pi,
+                                          float2 rp_self, int3 ci) {
+  constexpr int NR = Stencil<GF>::NR;
+  float rho_w = 0.0f, p_w = 0.0f;
+  bool wall_new = false;
+  if (WALL && !fluid_of(pi.w)) {
+    float rsum = 0.0f, wsum = 0.0f;
+    if (!ovf) {
+      for (int k = 0; k < cnt; ++k) {  // this particle's own list, just written
+        const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
+        const int r = (int)(e >> kRowShift);
+        if (Stencil<GF>::boundary_row(r)) {
+          int a, b;  // the row's start (its cell bounds are L1-resident by now)
+          row_range<GF>(kp, t, c, r, a, b);
+          wall_term_ptc<PRECISE>(kp, ptc, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
+        }
+      }
+    } else {
+      for (int r = 0; r < NR; ++r) {
+        if (!Stencil<GF>::boundary_row(r)) continue;
+        int a, b;
+        row_range<GF>(kp, t, c, r, a, b);
+        for (int j = a; j < b; ++j) {
+          if (j == i) continue;
+          const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
+          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term_ptc<PRECISE>(kp, ptc, pi, j, rsum, wsum, ci);
+        }
+      }
+    }
+    const zsph_gpu_param_t& p = kp.p;
+    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+    if (rsum < 0.0f) rsum = 0.0f;
+    rho_w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+    p_w = rsum;
+    wall_new = true;
+  }
+  float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
+  float4 pr = pi;
+  if (wall_new) {
+    pr.w = rho_w;
+    vp.w = p_w;
+  }
+  st_rec(&s.sh.pr(i), pr, vp);
+  s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+}
+
 constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // Builds the neighbour lists of 32 consecutive sorted particles per warp,
 // one lane per particle (the plain form).  A cell holds about 18-24
@@ -429,7 +486,7 @@ template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 // 32*group .. 32*group+31); k_nblist_seq runs one group per warp, the
 // batched form's persistent kernel loops over groups.  The warp's staging
 // arrays are slot `wid` of the CTA's CW slots.
-template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs>
+template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs, bool SKIN = false>
 __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
                                              const zsph_tmp_t& t, int group, int wid) {
   constexpr int NR = Stencil<GF>::NR;
@@ -463,6 +520,11 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   int cnt = 0;   // entries emitted
   int done = 0;  // entries written to global memory (a multiple of 8)
   bool ovf = false;
+  // SKIN (the list transfer's predictor): the candidates with
+  // r2max < r^2 <= r2skin, in candidate order, into the skin list
+  const float r2skin = kp.r2skin;
+  int kc = 0;
+  bool skovf = false;
   // writes the completed 8-entry blocks among the first min(cnt, kMaxNb) entries
   auto flush = [&]() {
     const int lim = min(cnt, kMaxNb);
@@ -515,7 +577,7 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
         for (int h = 0; h < 2; ++h) {
           const int base = k0 + 32 * h;  // offset of the block in the lane's row range
           if (base >= L) break;          // uniform
-          unsigned mh = 0u;
+          unsigned mh = 0u, mk = 0u;
 #pragma unroll
           for (int blk = 0; blk < 4; ++blk) {
             if (base + 8 * blk >= L) break;  // uniform: the rest is padding
@@ -530,6 +592,10 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
               upk2(d2, r0, r1);
               if (r0 <= r2max) mh |= 1u << tt;
               if (r1 <= r2max) mh |= 2u << tt;
+              if constexpr (SKIN) {
+                if (r0 <= r2skin) mk |= 1u << tt;
+                if (r1 <= r2skin) mk |= 2u << tt;
+              }
             }
           }
           // keep the hits inside this lane's range (offsets < len), not itself
@@ -538,6 +604,19 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
           const int self = i - sl - base;
           if (self >= 0 && self < 32) keep &= ~(1u << self);
           mh &= keep;
+          if constexpr (SKIN) {
+            mk &= keep & ~mh;
+            while (mk) {
+              const int bb = __ffs(mk) - 1;
+              mk &= mk - 1;
+              const int off = base + bb;
+              if (kc < kSkinCap && off <= kOffMask)
+                s.xf.sk[sk_idx(i, kc)] = (uint16_t)(((unsigned)r << kRowShift) | (unsigned)off);
+              else
+                skovf = true;
+              ++kc;
+            }
+          }
           if (!mh) continue;
           const int off0 = base;
           if (cnt + __popc(mh) <= kMaxNb && off0 + 31 <= kOffMask) {
@@ -576,57 +655,28 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   }
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
-  float rho_w = 0.0f, p_w = 0.0f;
-  bool wall_new = false;
-  if (WALL && act && !fluid_of(pi.w)) {
-    float rsum = 0.0f, wsum = 0.0f;
-    if (!ovf) {
-      for (int k = 0; k < cnt; ++k) {  // this thread's own list, written above
-        const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
-        const int r = (int)(e >> kRowShift);
-        if (Stencil<GF>::boundary_row(r)) {
-          int a, b;  // the row's start (its cell bounds are L1-resident by now)
-          row_range<GF>(kp, t, c, r, a, b);
-          wall_term_ptc<PRECISE>(kp, ptc, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
-        }
-      }
-    } else {
-      for (int r = 0; r < NR; ++r) {
-        if (!Stencil<GF>::boundary_row(r)) continue;
-        int a, b;
-        row_range<GF>(kp, t, c, r, a, b);
-        for (int j = a; j < b; ++j) {
-          if (j == i) continue;
-          const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
-          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term_ptc<PRECISE>(kp, ptc, pi, j, rsum, wsum, ci);
-        }
-      }
-    }
-    const zsph_gpu_param_t& p = kp.p;
-    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-    if (rsum < 0.0f) rsum = 0.0f;
-    rho_w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-    p_w = rsum;
-    wall_new = true;
-  }
-  if (act) {
-    // the lane's packed record, with a wall's new (rho, p)
-    float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
-    float4 pr = pi;
-    if (wall_new) {
-      pr.w = rho_w;
-      vp.w = p_w;
-    }
-    st_rec(&s.sh.pr(i), pr, vp);
-    s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
-  }
+  if (SKIN && act) s.xf.sk_cnt[i] = skovf ? kOverflow : (uint8_t)kc;
+  if (act) list_tail<GF, WALL, PRECISE>(kp, s, ptc, t, i, c, cnt, ovf, pi, rp_self, ci);
 }
 
-template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs>
+template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs,
+          bool SKIN = false>
 __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_ptc_t ptc,
                                                                    zsph_tmp_t t) {
   const int wid = threadIdx.x >> 5;
-  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS>(kp_arg, s, ptc, t, blockIdx.x * CW + wid, wid);
+  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS, SKIN>(kp_arg, s, ptc, t, blockIdx.x * CW + wid, wid);
+}
+
+// The list transfer's fallback: the full list build of the corrector, run
+// only when the transfer's conditions failed this step (*s.xf.flag set);
+// otherwise every CTA returns at once.
+template <int CW, int SEGS>
+__global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_fallback(KParams kp, Scratch s, zsph_ptc_t ptc,
+                                                                        zsph_tmp_t t) {
+  if (*s.xf.flag == 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(s.xf.stats + 1, 1ull);
+  const int wid = threadIdx.x >> 5;
+  nblist_group<1, true, CW, false, false, SEGS>(kp, s, ptc, t, blockIdx.x * CW + wid, wid);
 }
 
 struct NbB1 {  // boundary loop 1
@@ -808,6 +858,23 @@ struct FeatAcc {
 // give 80 registers without spills for the plain variants.
 // REUSE: as k_boundary's (entries re-tested at the current positions).
 // governing_one: one thread's particle i, as boundary_one.
+// List transfer, in the predictor's fused integration: particle i's
+// predicted position (just written to `to`) goes to xfer_pos4, and the
+// corrector is told to build its lists in full (*xfer_flag) if the half-step
+// displacement exceeds the skin's allowance, a position is not finite, or
+// the corrector's hash of the position (hash.cu:12-23, exactly as the search
+// computes it) will kill the particle.
+__device__ __forceinline__ void xfer_note_prediction(const KParams& kp, const zsph_ptc_t& from, const zsph_ptc_t& to,
+                                                     int i) {
+  const float x = to.pos[3 * i], y = to.pos[3 * i + 1], z = to.pos[3 * i + 2];
+  const float d2 = dist2(x - from.pos[3 * i], y - from.pos[3 * i + 1], z - from.pos[3 * i + 2]);
+  const zsph_gpu_param_t& p = kp.p;
+  const int h = cell_hash(p, x, y, z, __frcp_rn(p.grid_size));
+  const bool bad = !(d2 <= kp.disp2max) || h < 0 || h > p.grid_hash_max - p.grid_hash_min;
+  kp.xfer_pos4[i] = make_float4(x, y, z, 0.0f);
+  if (bad) atomicOr(kp.xfer_flag, 1);
+}
+
 template <int GF, int MODE, bool FEAT, bool PRECISE, bool BATCH, bool RIGID, bool REUSE>
 __device__ __forceinline__ void governing_one(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
                                               const zsph_tmp_t& t, const zsph_ptc_t& out, const FeatOut& fo, int i,
@@ -944,6 +1011,8 @@ __device__ __forceinline__ void governing_one(const KParams& kp_arg, const Scrat
     if (fo.acc_copy) fo.acc_copy[i] = acc;
   }
   if (MODE != 0) integrate_one<MODE, PRECISE>(kp, ptc, out, i, acc);
+  if constexpr (MODE == 1 && !PRECISE && !BATCH && !REUSE)
+    if (kp.xfer_pos4) xfer_note_prediction(kp, ptc, out, i);
 }
 
 template <int GF, int MODE, bool FEAT = false, bool PRECISE = false, bool BATCH = false, bool RIGID = false,
@@ -1493,6 +1562,351 @@ __global__ void __launch_bounds__(kSearchBlock) k_nb_counts(KParams kp, Scratch 
   if (nb_governing) nb_governing[i] = cnt;
 }
 
+// ---- list transfer: the corrector's lists made from the predictor's -------
+//
+// The corrector's neighbour set of a particle is every candidate of its
+// stencil rows (cell bounds of the corrector's search) within 2h at the
+// predicted positions.  For a particle that stays in its cell, those rows
+// are the cells it had in the predictor's search, and a neighbour within 2h
+// now was within 2h + skin then if no particle moved more than half the
+// skin in the half step (the fused prediction checks that).  So its
+// predictor list, its skin list (2h < r <= 2h + skin) and the particles
+// handed over below hold the whole set: each is re-tested against the exact
+// threshold at the predicted positions and kept only if its corrector slot
+// lies in one of the particle's corrector row ranges (which reproduces the
+// rows row_range drops and the excluded last particle).  Sorting the 16-bit
+// entries (row << 11 | offset) restores the reference's visit order, so the
+// lists equal those of a full build entry for entry.
+//
+// The particles that change cell (about 1 % per half step on the dam break),
+// the predictor search's last particle (never anyone's candidate there),
+// those whose predictor list or skin list overflowed and those whose rows
+// meet stale cell bounds get a full search instead (k_xfer_classify lists
+// them, k_xfer_search gives each a warp).  That search also hands
+// such a particle to every neighbour whose predictor rows did not contain
+// it, the only pairs the transferred lists can lack.
+
+// Stale cell bounds: when a search's last particle is alone in its cell k,
+// grid_end[c >= k] and grid_start[c > k] keep earlier values (sort.cu:30-60).
+// A stencil row of cell c ends at cell c + XY + X + 1 at most, so only
+// particles in cells from lo = k - (XY + X + 1) on have rows that can reach
+// them.  k = lo = INT_MAX for a search without a lone last particle.
+struct XStale {
+  int kP, kC, loP, loC;  // predictor's and corrector's search
+};
+__device__ __forceinline__ XStale xfer_stale(const KParams& kp, const Scratch& s, const zsph_tmp_t& t) {
+  const int n = kp.n, reach = kp.XY + kp.p.grid_xdim + 1;
+  XStale x;
+  x.kP = s.xf.hashP[n - 1] != s.xf.hashP[n - 2] ? s.xf.hashP[n - 1] : INT_MAX;
+  x.kC = t.hash[n - 1] != t.hash[n - 2] ? t.hash[n - 1] : INT_MAX;
+  x.loP = x.kP == INT_MAX ? INT_MAX : x.kP - reach;
+  x.loC = x.kC == INT_MAX ? INT_MAX : x.kC - reach;
+  return x;
+}
+
+// For a particle in cell c in both searches: whether one of its kept rows
+// ends at a stale bound in one search only, or in both with a range that is
+// not empty in both.  Rows that are stale and empty in both searches select
+// nothing in either, and the transfer reproduces that through the corrector
+// row ranges it checks every entry against.
+__device__ bool xfer_stale_rows(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, const XStale& x, int c) {
+  const zsph_gpu_param_t& p = kp.p;
+  zsph_tmp_t tP = t;
+  tP.grid_start = s.xf.gsP;
+  tP.grid_end = s.xf.geP;
+  for (int r = 0; r < 9; ++r) {
+    const int cell = c + (r / 3 - 1) * kp.XY + (r % 3 - 1) * p.grid_xdim;
+    if (cell - 1 < p.grid_hash_min || cell + 1 > p.grid_hash_max) continue;  // row_range drops it
+    const bool sP = cell + 1 >= x.kP, sC = cell + 1 >= x.kC;
+    if (!sP && !sC) continue;
+    if (sP != sC) return true;
+    int aP, bP, aC, bC;
+    row_range<1>(kp, tP, c, r, aP, bP);
+    row_range<1>(kp, t, c, r, aC, bC);
+    if (aP < bP || aC < bC) return true;
+  }
+  return false;
+}
+
+// Whether corrector slot i gets a full search: the particle changed cell
+// between the searches, was the predictor search's last particle (never a
+// candidate there), its predictor list or skin list overflowed, or its rows
+// meet stale bounds (above).  src = its predictor index.
+__device__ __forceinline__ bool xfer_full(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, const XStale& x,
+                                          int i, int& src) {
+  src = t.index[i];
+  const int cC = t.hash[i], cP = s.xf.hashP[src];
+  if (cC != cP || src == kp.n - 1 || s.nb_cnt[src] == kOverflow || s.xf.sk_cnt[src] == kOverflow) return true;
+  return (cC >= x.loP || cC >= x.loC) && xfer_stale_rows(kp, s, t, x, cC);
+}
+
+// Whether predictor cell cm lies in one of the stencil rows row_range keeps
+// for cell cj (delta_ns.cu:39-46), i.e. a particle there (other than the
+// search's last) was a candidate of a particle in cj.  Rows with stale
+// bounds only matter where they are empty in both searches (xfer_full), and
+// there the corrector row check drops the pair whatever this says.
+__device__ __forceinline__ bool was_candidate(const KParams& kp, int cj, int cm) {
+  const zsph_gpu_param_t& p = kp.p;
+#pragma unroll
+  for (int z = -1; z <= 1; ++z)
+#pragma unroll
+    for (int y = -1; y <= 1; ++y) {
+      const int cell = cj + z * kp.XY + y * p.grid_xdim;
+      if (cell - 1 >= p.grid_hash_min && cell + 1 <= p.grid_hash_max && cm >= cell - 1 && cm <= cell + 1)
+        return true;
+    }
+  return false;
+}
+
+// Full-search particle (predictor index srcM, predictor cell cPM) found
+// within 2h of corrector slot j: hand it to j unless j searches in full too
+// or its predictor lists already hold the pair.  A slot without a full
+// search kept its cell, so its corrector hash is its predictor cell.
+__device__ __forceinline__ void xfer_hand_over(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, int j,
+                                               int srcM, int cPM) {
+  if (s.xf.fullb[j]) return;
+  if (srcM != kp.n - 1 && was_candidate(kp, t.hash[j], cPM)) return;
+  const int k = atomicAdd(s.xf.xcnt + j, 1);
+  if (k < kXtra) s.xf.xl[(size_t)j * kXtra + k] = srcM;
+  else atomicOr(s.xf.flag, 1);
+}
+
+// One warp's full search for corrector slot M: its list exactly as the
+// full build makes it (each row's range as row_range gives it, stale
+// bounds included; rows in order, candidates in order), plus the
+// hand-overs.  The hand-over scans each row's cells' true particle range,
+// the last particle included and rows at the ends of the hash range clamped
+// instead of dropped, so it reaches every particle whose rows hold M; those
+// ranges are disjoint, so no particle is handed M twice.
+__device__ __forceinline__ void xfer_full_search(const KParams& kp, const Scratch& s, const zsph_ptc_t& cur,
+                                                 const zsph_tmp_t& t, int M) {
+  const zsph_gpu_param_t& p = kp.p;
+  const int n = kp.n, lane = threadIdx.x & 31;
+  const int srcM = t.index[M];
+  const float px = cur.pos[3 * M], py = cur.pos[3 * M + 1], pz = cur.pos[3 * M + 2];
+  const int cM = t.hash[M], cPM = s.xf.hashP[srcM], lastcell = t.hash[n - 1];
+  int cnt = 0;
+  bool ovf = false;
+  for (int r = 0; r < 9; ++r) {
+    int a, b;  // the row as the full build scans it
+    row_range<1>(kp, t, cM, r, a, b);
+    const int cell = cM + (r / 3 - 1) * kp.XY + (r % 3 - 1) * p.grid_xdim;
+    const int cs = max(cell - 1, p.grid_hash_min), ce = min(cell + 1, p.grid_hash_max);
+    int a2 = n, b2 = n;  // the true range of the row's cells (empty when they are off the grid)
+    if (cs <= ce) {
+      a2 = cs > lastcell ? n : max(t.grid_start[cs], 0);
+      b2 = ce >= lastcell ? n : min(t.grid_end[ce], n);
+    }
+    // [lo, hi) in ascending order: the row's own range below the true one,
+    // the true one, the own range above it (the first and last are empty
+    // unless bounds are stale)
+    auto scan = [&](int lo, int hi) {
+      for (int j0 = lo; j0 < hi; j0 += 32) {
+        const int j = j0 + lane;
+        bool hit = false;
+        if (j < hi && j != M)
+          hit = interacts(kp, dist2(px - cur.pos[3 * j], py - cur.pos[3 * j + 1], pz - cur.pos[3 * j + 2]));
+        const bool own = hit && j >= a && j < b;
+        const unsigned om = __ballot_sync(0xffffffffu, own);
+        bool bad = false;
+        if (own) {
+          const int k = cnt + __popc(om & lanemask_lt());
+          const int off = j - a;
+          if (k < kMaxNb && off <= kOffMask)
+            s.xf.nb2[nb_vec(M, k >> 3) * 8 + (k & 7)] = (uint16_t)(((unsigned)r << kRowShift) | (unsigned)off);
+          else
+            bad = true;
+        }
+        cnt += __popc(om);
+        ovf |= __any_sync(0xffffffffu, bad);
+        if (hit && j >= a2 && j < b2) xfer_hand_over(kp, s, t, j, srcM, cPM);
+      }
+    };
+    if (a2 < b2) {
+      scan(a, min(b, a2));
+      scan(a2, b2);
+      scan(max(a, b2), b);
+    } else {
+      scan(a, b);
+    }
+  }
+  if (cnt > 254) ovf = true;
+  if (lane == 0) s.xf.nb_cnt2[M] = ovf ? kOverflow : (uint8_t)cnt;
+}
+
+// Corrector, after its search: each slot's class (fullb), its corrector
+// slot in its predicted-position record (pos4[src].w), and the list of the
+// slots that get a full search.  (The step needs n >= 64.)
+__global__ void __launch_bounds__(kSearchBlock) k_xfer_classify(KParams kp, Scratch s, zsph_tmp_t t) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool act = i < kp.n;
+  int src = 0;
+  bool full = false;
+  if (act) {
+    full = xfer_full(kp, s, t, xfer_stale(kp, s, t), i, src);
+    reinterpret_cast<int*>(s.xf.pos4)[4 * (size_t)src + 3] = i;
+    s.xf.fullb[i] = full ? 1 : 0;
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, full);
+  if (m) {
+    int base = 0;
+    if (lane == 0) {
+      base = atomicAdd(s.xf.acount, __popc(m));
+      atomicAdd(s.xf.stats + 2, (unsigned long long)__popc(m));
+    }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (full) s.xf.alist[base + __popc(m & lanemask_lt())] = i;
+  }
+}
+
+constexpr int kSearchWarps = 4;  // warps per CTA of k_xfer_search
+
+// The full searches, one warp per listed slot (grid-stride over the list).
+__global__ void __launch_bounds__(kSearchWarps * 32) k_xfer_search(KParams kp, Scratch s, zsph_ptc_t cur,
+                                                                    zsph_tmp_t t) {
+  const int na = *s.xf.acount;
+  const int w0 = blockIdx.x * kSearchWarps + (threadIdx.x >> 5), nw = gridDim.x * kSearchWarps;
+  for (int w = w0; w < na; w += nw) xfer_full_search(kp, s, cur, t, s.xf.alist[w]);
+}
+
+constexpr int kXferThreads = 64;            // threads (particles) per CTA of k_nblist_xfer
+constexpr int kXBuf = kMaxNb + kSkinCap;    // a particle's merged predictor and skin entries
+
+// Corrector: the transferred lists (see above), then each particle's wall
+// (rho, p) and packed shadow record exactly as the full build's end does.
+// Returns at once when the full build runs instead (*s.xf.flag).
+// Per particle: (1) its predictor list and skin list merged by their keys
+// into shared memory (both are in the predictor's candidate order, so the
+// merged entries, mapped to corrector slots, are out of order only where a
+// neighbour changed cell); (2) eight entries at a time, their predicted
+// positions loaded together, re-tested, and kept as corrector keys in place;
+// (3) the hand-overs; (4) an insertion sort back into candidate order.
+__global__ void __launch_bounds__(kXferThreads) k_nblist_xfer(KParams kp, Scratch s, zsph_ptc_t cur, zsph_tmp_t t) {
+  constexpr int B = kXferThreads;
+  // rows of kXBuf + 6 entries: 75 words, an odd stride, so the lanes' k-th
+  // entries fall in different banks
+  __shared__ __align__(16) uint16_t s_buf[B][kXBuf + 6];
+  __shared__ int s_row[27 * B];  // predictor row starts, corrector row starts and ends
+  if (*s.xf.flag) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(s.xf.stats, 1ull);
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * B + tid;
+  if (i >= kp.n) return;
+  const bool full = s.xf.fullb[i] != 0;
+  const int c = t.hash[i];
+  int cnt = 0;
+  bool ovf = false;
+  if (!full) {
+    const int src = t.index[i];
+    int* rsP = s_row + tid;
+    int* rsC = s_row + 9 * B + tid;
+    int* reC = s_row + 18 * B + tid;
+    zsph_tmp_t tP = t;
+    tP.grid_start = s.xf.gsP;
+    tP.grid_end = s.xf.geP;
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      int a, b;
+      row_range<1>(kp, tP, c, r, a, b);
+      rsP[r * B] = a;
+      row_range<1>(kp, t, c, r, a, b);
+      rsC[r * B] = a;
+      reC[r * B] = b;
+    }
+    uint16_t* buf = s_buf[tid];
+    // (1) merge
+    const int cl = s.nb_cnt[src], ks = s.xf.sk_cnt[src];
+    int m = 0, kk = 0;
+    unsigned skn = ks > 0 ? s.xf.sk[sk_idx(src, 0)] : 0x10000u;
+    const uint4* lst = reinterpret_cast<const uint4*>(s.nb);
+    for (int k = 0; k < cl; k += 8) {
+      const uint4 v = lst[nb_vec(src, k >> 3)];
+      const unsigned wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        if (k + e < cl) {
+          const unsigned ent = (wv[e >> 1] >> ((e & 1) * 16)) & 0xffffu;
+          while (skn < ent) {
+            buf[m++] = (uint16_t)skn;
+            skn = ++kk < ks ? s.xf.sk[sk_idx(src, kk)] : 0x10000u;
+          }
+          buf[m++] = (uint16_t)ent;
+        }
+      }
+    }
+    for (; kk < ks; ++kk) buf[m++] = s.xf.sk[sk_idx(src, kk)];
+    // (2) re-test at the predicted positions; keep as corrector keys
+    const float4 pi = s.xf.pos4[src];
+    auto keep = [&](float4 q, int hint) {
+      if (!interacts(kp, dist2(pi.x - q.x, pi.y - q.y, pi.z - q.z))) return;
+      const int jC = __float_as_int(q.w);
+      int rr = hint;
+      if (jC < rsC[rr * B] || jC >= reC[rr * B]) {  // the neighbour changed row (rare)
+        rr = -1;
+        for (int r = 0; r < 9; ++r)
+          if (jC >= rsC[r * B] && jC < reC[r * B]) rr = r;
+        if (rr < 0) return;  // in none of the particle's rows
+      }
+      const int off = jC - rsC[rr * B];
+      if (cnt < kMaxNb && off <= kOffMask) buf[cnt] = (uint16_t)(((unsigned)rr << kRowShift) | (unsigned)off);
+      else ovf = true;
+      ++cnt;
+    };
+    const int nmax = kp.n - 1;
+    for (int k0 = 0; k0 < m; k0 += 8) {
+      float4 q[8];
+      int rw[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        int jP = 0;
+        rw[e] = -1;
+        if (k0 + e < m) {
+          const unsigned ent = buf[k0 + e];
+          rw[e] = (int)(ent >> kRowShift);
+          // inside the predictor row it came from, so below n; the clamp
+          // only keeps the load in bounds should that ever not hold
+          jP = min(max(rsP[rw[e] * B] + (int)(ent & kOffMask), 0), nmax);
+        }
+        q[e] = s.xf.pos4[jP];
+      }
+      // cnt <= k0 + e here: the keys written never overtake the entries not yet read
+#pragma unroll
+      for (int e = 0; e < 8; ++e)
+        if (rw[e] >= 0) keep(q[e], rw[e]);
+    }
+    // (3) hand-overs (predictor indices of full-search particles)
+    const int kx = min(s.xf.xcnt[i], kXtra);
+    for (int k = 0; k < kx; ++k) keep(s.xf.pos4[min(max(s.xf.xl[(size_t)i * kXtra + k], 0), nmax)], 4);
+    if (cnt > 254) ovf = true;
+    if (!ovf) {
+      // (4) the candidate order: ascending (row, offset)
+      for (int k = 1; k < cnt; ++k) {
+        const uint16_t v = buf[k];
+        int j = k - 1;
+        while (j >= 0 && buf[j] > v) {
+          buf[j + 1] = buf[j];
+          --j;
+        }
+        buf[j + 1] = v;
+      }
+      uint4* nbv = reinterpret_cast<uint4*>(s.xf.nb2);
+      const uint32_t* bw = reinterpret_cast<const uint32_t*>(buf);  // rows are 4-byte aligned
+      for (int k = 0; k < cnt; k += 8)
+        nbv[nb_vec(i, k >> 3)] = make_uint4(bw[k / 2], bw[k / 2 + 1], bw[k / 2 + 2], bw[k / 2 + 3]);
+    }
+  } else {  // the list k_xfer_search wrote
+    cnt = s.xf.nb_cnt2[i];
+    ovf = cnt == kOverflow;
+  }
+  Scratch so = s;
+  so.nb = s.xf.nb2;
+  so.nb_cnt = s.xf.nb_cnt2;
+  const float2 rp = reinterpret_cast<const float2*>(cur.rhop)[i];
+  const float4 pc = make_float4(cur.pos[3 * i], cur.pos[3 * i + 1], cur.pos[3 * i + 2], packed_rho(rp.x, cur.type[i]));
+  list_tail<1, true, false>(kp, so, cur, t, i, c, ovf ? 0 : cnt, ovf, pc, rp, int3{0, 0, 0});
+}
+
 }  // namespace
 
 cudaError_t init_pair_kernels() {
@@ -1615,6 +2029,65 @@ cudaError_t launch_batch_persistent(const KParams& kp, const Scratch& s, const z
   void* args[] = {&a};
   return cudaLaunchCooperativeKernel((const void*)k_batch_persistent, dim3(grid), dim3(kPersistThreads), args,
                                      2 * pair_smem<1>(0, 0), st);
+}
+
+cudaError_t launch_xfer_pred_lists(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
+                                   cudaStream_t st, Prof* pf) {
+  if (kp.n == 0) return cudaSuccess;
+  if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.stage_windows || kp.equations != ZSPH_EQ_DELTA || !s.xf.sk)
+    return cudaErrorInvalidValue;
+  const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
+  const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
+  if (kp.tune_cw == 4) {
+    if (segs == 2) k_nblist_seq<1, true, 4, false, false, 2, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, true, 4, false, false, 3, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, true, 4, false, false, 4, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+  } else {
+    if (segs == 2) k_nblist_seq<1, true, 2, false, false, 2, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, true, 2, false, false, 3, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, true, 2, false, false, 4, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+  }
+  mark(pf, "nblist_wall", st);
+  k_boundary<1><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
+  mark(pf, "boundary", st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_xfer_corr_lists(const KParams& kp, const Scratch& s, const zsph_ptc_t& cur, const zsph_tmp_t& t,
+                                   cudaStream_t st, Prof* pf) {
+  if (kp.n == 0) return cudaSuccess;
+  if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.stage_windows || kp.equations != ZSPH_EQ_DELTA || !s.xf.nb2)
+    return cudaErrorInvalidValue;
+  k_xfer_classify<<<(kp.n + kSearchBlock - 1) / kSearchBlock, kSearchBlock, 0, st>>>(kp, s, t);
+  mark(pf, "xfer_classify", st);
+  static int sms = 0;  // SMs of the device (the same for every B200)
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sms = 148;
+  }
+  k_xfer_search<<<sms * 8, kSearchWarps * 32, 0, st>>>(kp, s, cur, t);
+  mark(pf, "xfer_search", st);
+  k_nblist_xfer<<<(kp.n + kXferThreads - 1) / kXferThreads, kXferThreads, 0, st>>>(kp, s, cur, t);
+  mark(pf, "nblist_xfer", st);
+  Scratch s2 = s;  // the walks read the corrector's lists
+  s2.nb = s.xf.nb2;
+  s2.nb_cnt = s.xf.nb_cnt2;
+  const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
+  const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
+  if (kp.tune_cw == 4) {
+    if (segs == 2) k_nblist_fallback<4, 2><<<g4, 128, 0, st>>>(kp, s2, cur, t);
+    else if (segs == 3) k_nblist_fallback<4, 3><<<g4, 128, 0, st>>>(kp, s2, cur, t);
+    else k_nblist_fallback<4, 4><<<g4, 128, 0, st>>>(kp, s2, cur, t);
+  } else {
+    if (segs == 2) k_nblist_fallback<2, 2><<<g2, 64, 0, st>>>(kp, s2, cur, t);
+    else if (segs == 3) k_nblist_fallback<2, 3><<<g2, 64, 0, st>>>(kp, s2, cur, t);
+    else k_nblist_fallback<2, 4><<<g2, 64, 0, st>>>(kp, s2, cur, t);
+  }
+  mark(pf, "nblist_fallback", st);
+  k_boundary<1><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s2, cur, t);
+  mark(pf, "boundary", st);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_nb_counts(const KParams& kp, const Scratch& s, int* nb_boundary, int* nb_governing,

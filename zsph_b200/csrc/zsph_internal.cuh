@@ -58,6 +58,15 @@ struct KParams {
   // grid row (y cell index) at the current positions, which decides the
   // boundary stencil's asymmetric rows y in [-GF, GF) (delta_ns.cu:37).
   const int* cur_cy;
+  // List transfer (plain step, set for the predictor's governing launch
+  // only; null otherwise): the fused prediction also writes each particle's
+  // predicted position to xfer_pos4 and sets *xfer_flag when the corrector
+  // must build its lists in full (a displacement above sqrt(disp2max), a
+  // non-finite position, or a position the corrector's hash will kill).
+  float4* xfer_pos4;
+  int* xfer_flag;
+  float disp2max;  // largest squared half-step displacement the transfer allows
+  float r2skin;    // predictor list build: squared outer radius of the skin lists
 };
 
 // Original-index range [first, first + count) of one rigid body.
@@ -149,6 +158,28 @@ struct Shadow {
   }
 };
 
+// List transfer: the corrector's neighbour lists made from the predictor's
+// (transfer.cu).  Device scratch, allocated when a handle enables it.
+constexpr int kSkinCap = 16;  // predictor skin entries per particle (2h < r <= 2h + skin)
+constexpr int kXtra = 8;      // corrector candidates handed to a particle by the full-search set
+struct Xfer {
+  uint16_t* nb2;     // corrector lists, blocked like Scratch::nb
+  uint8_t* nb_cnt2;  // [n]
+  uint16_t* sk;      // [ceil(n/32)*32 * kSkinCap] predictor skin lists, blocked by 32-particle groups
+  uint8_t* sk_cnt;   // [n] (255 = overflow)
+  float4* pos4;      // [n] predicted positions in predictor order; .w = the particle's corrector slot
+  int* xl;           // [n * kXtra] predictor indices handed to a particle by the full-search set
+  int* xcnt;         // [n] entries in xl (zeroed before the corrector's search)
+  int* hashP;        // [n] predictor search's hash and cell bounds, copied before the corrector's search
+  int* gsP;          // [G]
+  int* geP;          // [G]
+  int* flag;         // [1] nonzero: the corrector builds its lists in full this step
+  uint8_t* fullb;    // [n] 1: the corrector slot gets a full search
+  int* alist;        // [n] the corrector slots with a full search (unordered)
+  int* acount;       // [1] entries in alist (zeroed before the corrector's search)
+  unsigned long long* stats;  // [3] steps transferred, steps that built in full, full searches
+};
+
 // Device scratch owned by a handle; allocated once in zsph_create.
 struct Scratch {
   int* cnt;          // [G]   per-cell counts (kept zero between uses)
@@ -168,7 +199,9 @@ struct Scratch {
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
   int* flags;        // [1]   ZSPH_FLAG_* bits
   Shadow sh;
+  Xfer xf;           // list transfer scratch (null pointers when the handle has none)
 };
+
 
 // Learned-corrector inputs written by the predictor-stage governing walk
 // (k_governing<GF, 1, true>): kFeat non-dimensional neighbour aggregates per
@@ -237,6 +270,9 @@ struct Handle {
   unsigned* pbar = nullptr;            // the persistent kernel's grid-barrier words [2]
   unsigned spin_limit = 1u << 22;      // polls per barrier wait (about a second)
   int persist_graph = 0;               // 1: zsph_run replays a captured persistent launch; -1: capture refused
+  // list transfer (zsph_set_list_transfer): on/off and the skin as a multiple of h
+  int xfer_on = 0;
+  float xfer_skin = 0.05f;
 };
 
 // learn.cu: frees the handle's learned-corrector state
@@ -314,6 +350,13 @@ cudaError_t launch_governing(const KParams& kp, const Scratch& s, const zsph_ptc
                              const FeatOut* feat = nullptr);
 cudaError_t launch_nblist(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
                           cudaStream_t st);
+// List transfer (equations.cu): the predictor's list build with skin lists
+// plus its boundary pass; the corrector's transferred lists (full build when
+// the transfer's conditions failed) plus its boundary pass on s.xf's lists.
+cudaError_t launch_xfer_pred_lists(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp,
+                                   cudaStream_t st, Prof* pf);
+cudaError_t launch_xfer_corr_lists(const KParams& kp, const Scratch& s, const zsph_ptc_t& cur, const zsph_tmp_t& tmp,
+                                   cudaStream_t st, Prof* pf);
 // Batched form: nsteps full steps of every scene in one cooperative launch
 // (equations.cu, k_batch_persistent); bar: two zeroed device words of the
 // grid barrier, kept between launches.  spin_limit bounds each barrier wait;

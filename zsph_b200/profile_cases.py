@@ -8,6 +8,9 @@ kernel family at a time (python -m zsph_b200.profile_cases CASE).
   rigid        the floating cube (dx = 0.02 m, 362,408 particles) with
                contact on: two steps (k_rigid_contact, k_rigid_sum,
                k_rigid_step, k_rigid_place) and the FP64 sums (k_conserve)
+  transfer     the dam break at dx = 0.0075 m (1,367,542 particles) with the
+               list transfer on: three steps (skin-list build, k_xfer_classify,
+               k_xfer_search, k_nblist_xfer, k_nblist_fallback)
 
 Inputs are seeded and synthetic; the cases only launch kernels and print a
 one-line summary, they check nothing (the parity tests do).
@@ -64,7 +67,18 @@ def rigid():
     s.close()
 
 
-CASES = {"mlp_predict": mlp_predict, "mlp_train": mlp_train, "rigid": rigid}
+def transfer():
+    c = cases.dam_break(0.0075)
+    s = z.Solver.from_case(c)
+    s.set_list_transfer(True)
+    for _ in range(3):
+        s.step()
+    s.sync()
+    print(f"transfer: {c.n} particles, {s.list_transfer_info()}")
+    s.close()
+
+
+CASES = {"mlp_predict": mlp_predict, "mlp_train": mlp_train, "rigid": rigid, "transfer": transfer}
 
 if __name__ == "__main__":
     if len(sys.argv) != 2 or sys.argv[1] not in CASES:
