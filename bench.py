@@ -225,7 +225,7 @@ def stencil_candidates(sol, n):
     return float(tot.mean())
 
 
-def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks):
+def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks, full_size=True):
     """Rates of the pair kernels: candidate tests/s of the list build,
     interacting pair evaluations/s and FP32 FLOP/s of boundary and governing
     against the nominal FP32 peak (148 SMs x 128 lanes x 2 x max SM clock),
@@ -238,7 +238,7 @@ def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks):
     per_launch = lambda k: (kern[k]["ms_per_step"] / max(kern[k]["launches_per_step"], 1) / 1e3) if k in kern else 0
     t_nb = per_launch("nblist_wall")
     if t_nb:
-        tr = ncu_traffic("nblist_wall")
+        tr = ncu_traffic("nblist_wall") if full_size else None
         out["nblist_wall"] = {"ms_per_substep": t_nb * 1e3, "stencil_candidates_per_particle": cand,
                               "candidate_tests_per_s": cand * n / t_nb,
                               "dram_gbs": tr / t_nb / 1e9 if tr else None}
@@ -251,7 +251,7 @@ def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks):
             continue
         pairs = float(np.mean(nb[nb >= 0]))
         evals = pairs * n / t
-        tr = ncu_traffic(name)
+        tr = ncu_traffic(name) if full_size else None
         out[name] = {"ms_per_substep": t * 1e3, "interacting_pairs_per_particle": pairs, "pair_evals_per_s": evals,
                      "fp32_tflops": evals * FLOP_PER_PAIR[name] / 1e12,
                      "fp32_frac_of_nominal_peak": evals * FLOP_PER_PAIR[name] / 1e12 / fp32_peak,
@@ -510,9 +510,10 @@ def run_ours(args, dist: Dist):
                 "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": ach / peaks["hbm_gbs"] if peaks["hbm_gbs"] else None,
                 "peak_source": f"{peaks['source']} hbm_gbs (copy test)",
-                "traffic": ncu_traffic("search_group")}
+                # the committed ncu traffic is scaled to the dx = 0.005 case
+                "traffic": ncu_traffic("search_group") if args.workload == "config1" else None}
     gov_ms = kern.get("governing", {}).get("ms_per_step", 0) / 2
-    pair = pair_kernel_rates(sol, kern, nb_b, nb_g, n, ck)
+    pair = pair_kernel_rates(sol, kern, nb_b, nb_g, n, ck, full_size=args.workload == "config1")
     dominant = {"kernel": dom[0], "ms_per_step": dom[1]["ms_per_step"], "share": dom[1]["share"],
                 "bound": {"nblist_wall": "instruction issue (candidate tests and per-lane hit emission)",
                           "boundary": "L1 data pipe (scattered neighbour records)",
@@ -521,7 +522,7 @@ def run_ours(args, dist: Dist):
                          "; not HBM-bound, no tensor-core work on the pair path",
                 "interacting_pairs_per_particle": pairs_gov,
                 "governing_pair_evals_per_s": pairs_gov * n / (gov_ms / 1e3) if gov_ms else None,
-                "traffic": ncu_traffic(dom[0])}
+                "traffic": ncu_traffic(dom[0]) if args.workload == "config1" else None}
 
     # end to end through the C ABI from pinned host buffers
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
