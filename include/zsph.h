@@ -5,7 +5,10 @@
  * (ZSPH, single_gpu_sph_src/) for a caller that drives it the way
  * single_gpu_sph_src/deltasph/main.cu does.  All structs are plain C; every
  * device pointer is caller-owned; every call returns a ZSPH_* status and
- * never exits the process.  `stream` is a cudaStream_t passed as void*
+ * never exits the process.  The float arrays of a particle buffer must start
+ * on an 8-byte boundary (as cudaMalloc and zsph_alloc_ptc give them); calls
+ * given others return ZSPH_EINVAL (ZSPH_ECUDA from the learned and
+ * precision-form entry points) without launching anything.  `stream` is a cudaStream_t passed as void*
  * (NULL = the legacy default stream).
  *
  * Particle layout (unchanged from the reference, data_structure.cuh:158-182):

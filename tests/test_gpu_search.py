@@ -221,3 +221,23 @@ def test_profiled_steps_report_every_launch_and_group():
     assert np.array_equal(sa.pos, sb.pos) and np.array_equal(sa.table, sb.table)
     a.close()
     b.close()
+
+
+def test_misaligned_particle_buffer_is_refused_before_any_launch():
+    # the kernels move the float2 arrays with 8-byte accesses; a buffer
+    # whose float arrays do not start on an 8-byte boundary is rejected on the
+    # host (a view 4 bytes into the pos array, still inside its allocation)
+    import ctypes
+    c = cases.small(0.04)
+    sol = z.Solver.from_case(c)
+    bad = z.Ptc()
+    ctypes.memmove(ctypes.byref(bad), ctypes.byref(sol.old), ctypes.sizeof(z.Ptc))
+    bad.pos = sol.old.pos + 4
+    before = sol.download("new").pos.copy()
+    with pytest.raises(z.ZsphError) as e:
+        lib = z.lib
+        z.check(lib.zsph_neighbor_search(sol.h, ctypes.byref(bad), ctypes.byref(sol.new), ctypes.byref(sol.tmp), None),
+                sol.h)
+    assert e.value.code == z.ZSPH_EINVAL and "8-byte" in str(e.value)
+    assert np.array_equal(sol.download("new").pos, before)  # nothing ran
+    sol.close()

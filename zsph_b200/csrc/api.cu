@@ -104,6 +104,8 @@ int check_ptc(zsph_handle* h, const zsph_ptc_t* p) {
   if (h->kp.n > 0 && (!p->pos || !p->vel || !p->rhop || !p->tmp_pos || !p->tmp_vel || !p->tmp_rhop || !p->type ||
                       !p->table))
     return set_err(h, ZSPH_EINVAL, "a particle array pointer is null");
+  if (!ptc_aligned8(*p))
+    return set_err(h, ZSPH_EINVAL, "particle float arrays must start on an 8-byte boundary (cudaMalloc alignment)");
   return ZSPH_OK;
 }
 

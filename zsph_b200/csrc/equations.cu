@@ -2022,6 +2022,7 @@ cudaError_t launch_batch_persistent(const KParams& kp, const Scratch& s, const z
   if (!kp.scenes || kp.p.grid_factor != 1 || kp.equations != ZSPH_EQ_DELTA || kp.c3o || kp.rigid_f ||
       kp.stage_windows)
     return cudaErrorInvalidValue;
+  if (!ptc_aligned8(o) || !ptc_aligned8(w)) return cudaErrorMisalignedAddress;  // nothing launched
   int grid = 0;
   cudaError_t e = persistent_grid(&grid);
   if (e) return e;

@@ -341,6 +341,7 @@ cudaError_t launch_sort_data(const KParams& kp, const Scratch& s, int tiles, con
 cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const zsph_ptc_t& o, const zsph_ptc_t& w,
                           const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf) {
   if (kp.n == 0) return cudaSuccess;
+  if (!ptc_aligned8(o) || !ptc_aligned8(w)) return cudaErrorMisalignedAddress;  // nothing launched
   k_hash_count<<<blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st>>>(kp, o, s);
   mark(pf, "hash_count", st);
   k_scan_onepass<<<(kp.G + kOneTile - 1) / kOneTile, kSearchBlock, 0, st>>>(kp, s, tmp);

@@ -180,6 +180,16 @@ struct Xfer {
   unsigned long long* stats;  // [3] steps transferred, steps that built in full, full searches
 };
 
+// The kernels move the float2 particle arrays (rhop, tmp_rhop) with 8-byte
+// accesses: every float array of a particle buffer must start on an 8-byte
+// boundary (cudaMalloc gives 256).  Checked on the host before any launch.
+inline bool ptc_aligned8(const zsph_ptc_t& p) {
+  const void* a[] = {p.pos, p.vel, p.rhop, p.tmp_pos, p.tmp_vel, p.tmp_rhop};
+  for (const void* q : a)
+    if (reinterpret_cast<uintptr_t>(q) & 7u) return false;
+  return true;
+}
+
 // Device scratch owned by a handle; allocated once in zsph_create.
 struct Scratch {
   int* cnt;          // [G]   per-cell counts (kept zero between uses)
