@@ -236,13 +236,13 @@ def pair_kernel_rates(sol, kern, nb_b, nb_g, n, clocks, full_size=True):
     cand = stencil_candidates(sol, n)
     out = {"fp32_peak_tflops_nominal": fp32_peak}
     per_launch = lambda k: (kern[k]["ms_per_step"] / max(kern[k]["launches_per_step"], 1) / 1e3) if k in kern else 0
-    t_nb = per_launch("nblist_wall")
+    t_nb = per_launch("nblist")
     if t_nb:
-        tr = ncu_traffic("nblist_wall") if full_size else None
-        out["nblist_wall"] = {"ms_per_substep": t_nb * 1e3, "stencil_candidates_per_particle": cand,
+        tr = ncu_traffic("nblist") if full_size else None
+        out["nblist"] = {"ms_per_substep": t_nb * 1e3, "stencil_candidates_per_particle": cand,
                               "candidate_tests_per_s": cand * n / t_nb,
                               "dram_gbs": tr / t_nb / 1e9 if tr else None}
-    for name in ("xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback"):
+    for name in ("walls", "xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback"):
         if per_launch(name):
             out[name] = {"ms_per_substep": per_launch(name) * 1e3}
     for name, nb in (("boundary", nb_b), ("governing", nb_g)):
@@ -515,7 +515,7 @@ def run_ours(args, dist: Dist):
     gov_ms = kern.get("governing", {}).get("ms_per_step", 0) / 2
     pair = pair_kernel_rates(sol, kern, nb_b, nb_g, n, ck, full_size=args.workload == "config1")
     dominant = {"kernel": dom[0], "ms_per_step": dom[1]["ms_per_step"], "share": dom[1]["share"],
-                "bound": {"nblist_wall": "instruction issue (candidate tests and per-lane hit emission)",
+                "bound": {"nblist": "instruction issue (candidate tests and per-lane hit emission)",
                           "boundary": "L1 data pipe (scattered neighbour records)",
                           "governing": "L1 data pipe (scattered neighbour records)"}.get(
                               dom[0], "see profiles/kernels_medium.md") +

@@ -202,14 +202,15 @@ def test_profiled_steps_report_every_launch_and_group():
     per = a.step_profiled()
     names = [k for k, _ in per]
     search = ["hash_count", "scan", "scatter", "rank_gather"]
-    sub = search + ["nblist_wall", "boundary", "governing"]
+    sub = search + ["nblist", "walls", "boundary", "governing"]
     assert names == sub + sub
-    assert len(names) == a.launches_per_step() == 14
+    assert len(names) == a.launches_per_step() == 16
     # the corrector's lists by the list transfer (opt-in)
     a.set_list_transfer(True)
-    corr = search + ["xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback", "boundary", "governing"]
+    corr = search + ["xfer_classify", "xfer_search", "nblist_xfer", "nblist_fallback", "walls", "boundary",
+                     "governing"]
     assert [k for k, _ in a.step_profiled()] == sub + corr
-    assert a.launches_per_step() == 17
+    assert a.launches_per_step() == 19
     a.set_list_transfer(False)
     b.step()
     grp = a.step_profiled(groups=True)

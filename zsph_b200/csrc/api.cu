@@ -130,7 +130,7 @@ void free_xfer(Xfer& x) {
 
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
-                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.flags, s.sh.rec};
+                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.wl, s.flags, s.sh.rec};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   free_xfer(s.xf);
@@ -398,6 +398,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.big_list, (size_t)kBigListCap);
   if (!e) e = dalloc(s.nb, (size_t)kMaxNb * ((n + 31) & ~(size_t)31));  // whole 32-particle list groups
   if (!e) e = dalloc(s.nb_cnt, n);
+  if (!e) e = dalloc(s.wl, n);
   if (!e) e = dalloc(s.flags, 1);
   if (!e) e = dalloc(s.sh.rec, 2 * (size_t)n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
@@ -994,12 +995,12 @@ int zsph_step_profiled_groups(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_
 }
 
 int zsph_launches_per_step(zsph_handle_t* h) {
-  // per sub-step: hash_count, scan, scatter, rank_gather, nblist, boundary,
-  // governing; with the list transfer the corrector's nblist is
+  // per sub-step: hash_count, scan, scatter, rank_gather, nblist, walls,
+  // boundary, governing; with the list transfer the corrector's nblist is
   // xfer_classify, xfer_search, nblist_xfer and nblist_fallback (one of the
   // last two returns at once)
-  if (h && xfer_eligible(h)) return 7 + 10;
-  return 2 * 7;
+  if (h && xfer_eligible(h)) return 8 + 11;
+  return 2 * 8;
 }
 
 }  // extern "C"

@@ -1,7 +1,7 @@
 // delta-SPH pair-interaction kernels for sm_100a.
 //
 // Reference path replaced (single_gpu_sph_src/):
-//   equation/delta_ns.cu:5-177   cuda_boundary_ns  -> k_nblist_seq (list + wall pressure) + k_boundary
+//   equation/delta_ns.cu:5-177   cuda_boundary_ns  -> k_nblist_seq (lists) + k_walls (wall pressure) + k_boundary
 //   equation/delta_ns.cu:179-267 cuda_govering_ns  -> k_governing (optionally fused with time_int.cu)
 //   lib/time_int.cu:3-92         cuda_prediction / cuda_correction -> k_integrate or k_governing epilogue
 //
@@ -44,7 +44,7 @@
 // non-fluid particles (densities are non-negative).
 //
 // Wall densities: the reference writes them in place while neighbours read
-// them (a race, delta_ns.cu:65,130,151).  Here k_nblist_seq extrapolates every
+// them (a race, delta_ns.cu:65,130,151).  Here k_walls extrapolates every
 // wall's (rho, p) first and publishes it in the packed shadows; k_boundary
 // reads neighbours' densities from the shadows (new wall values) and a
 // wall's own old density from ptc.rhop, and writes the new wall values to
@@ -140,11 +140,15 @@ __device__ __forceinline__ void load_rows(const KParams& kp, const zsph_tmp_t& t
 // row; the fetch index is only clamped to fmax (the last particle, or the
 // window's last slot), which keeps every access in bounds without a
 // shared-memory load of the row end per entry.  Particles whose list
-// overflowed re-filter their stencil rows directly.
-template <int GF, bool BOUNDARY_ONLY, class Nb, class Fetch, class Use>
+// overflowed re-filter their stencil rows directly (in the precision form
+// with the candidates moved into the frame of the particle's cell ci).
+template <bool PRECISE>
+__device__ __forceinline__ float4 shadow_pr(const KParams& kp, const Scratch& s, int j, int3 ci);
+
+template <int GF, bool BOUNDARY_ONLY, class Nb, bool PRECISE = false, class Fetch, class Use>
 __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i, float4 pi, const int* rs,
                                      const int* re, const int* fb, int fdummy, int fmax, Fetch&& fetch,
-                                     Use&& use) {
+                                     Use&& use, int3 ci = int3{0, 0, 0}) {
   const int cnt = s.nb_cnt[i];
   if (cnt != kOverflow) {
     const uint4* lst = reinterpret_cast<const uint4*>(s.nb);
@@ -176,7 +180,7 @@ __device__ __forceinline__ void walk(const KParams& kp, const Scratch& s, int i,
     const int a = rs[r * kPairBlock], b = re[r * kPairBlock];
     for (int j = a; j < b; ++j) {
       if (j == i) continue;
-      const float4 pj = s.sh.pr(j);
+      const float4 pj = shadow_pr<PRECISE>(kp, s, j, ci);
       if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) use(fetch(fb[r * kPairBlock] + (j - a)));
     }
   }
@@ -320,13 +324,10 @@ __device__ __forceinline__ ShadowRec shadow_rec(const KParams& kp, const Scratch
   return r;
 }
 
-// Wall pressure contribution of fluid neighbour j of wall particle i
-// (delta_ns.cu:67-85), with the reference's IEEE sqrt and division.
-template <bool PRECISE = false>
-__device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, float4 pi, int j, float& rsum,
-                                          float& wsum, int3 ci = int3{0, 0, 0}) {
-  const float4 pj = shadow_pr<PRECISE>(kp, s, j, ci);
-  if (!fluid_of(pj.w)) return;
+// One fluid neighbour's term of a wall's (rho, p) extrapolation
+// (delta_ns.cu:61-85): neighbour position pj, its (rho, p) rp.
+__device__ __forceinline__ void wall_term_core(const KParams& kp, float4 pi, float4 pj, float2 rp, float& rsum,
+                                               float& wsum) {
   const zsph_gpu_param_t& p = kp.p;
   const float dz = pi.z - pj.z;
   const float q = __fsqrt_rn(dist2(pi.x - pj.x, pi.y - pj.y, dz)) / p.h;
@@ -334,9 +335,19 @@ __device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, f
   float w = aa * aa * aa;
   w = w * aa;
   w *= (2.0f * q + 1.0f) * p.adh;
-  const float p1 = s.sh.vp(j).w;
-  rsum += (p1 - pj.w * ((0.0f - p.g) * dz)) * w;
+  rsum += (rp.y - fabsf(rp.x) * ((0.0f - p.g) * dz)) * w;
   wsum += w;
+}
+
+// Wall pressure contribution of fluid neighbour j of wall particle i
+// (delta_ns.cu:67-85), from j's packed record (one 256-bit load; the sign of
+// its density marks a non-fluid particle).
+template <bool PRECISE = false>
+__device__ __forceinline__ void wall_term(const KParams& kp, const Scratch& s, float4 pi, int j, float& rsum,
+                                          float& wsum, int3 ci = int3{0, 0, 0}) {
+  const ShadowRec r = shadow_rec<PRECISE>(kp, s, j, ci);
+  if (!fluid_of(r.pr.w)) return;
+  wall_term_core(kp, pi, r.pr, make_float2(r.pr.w, r.vp.w), rsum, wsum);
 }
 
 // Particle j's position from the sorted arrays, in the precision form moved
@@ -353,17 +364,7 @@ template <bool PRECISE = false>
 __device__ __forceinline__ void wall_term_ptc(const KParams& kp, const zsph_ptc_t& ptc, float4 pi, int j,
                                               float& rsum, float& wsum, int3 ci = int3{0, 0, 0}) {
   if (ptc.type[j] != 1) return;
-  const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
-  const float2 rp = reinterpret_cast<const float2*>(ptc.rhop)[j];
-  const zsph_gpu_param_t& p = kp.p;
-  const float dz = pi.z - pj.z;
-  const float q = __fsqrt_rn(dist2(pi.x - pj.x, pi.y - pj.y, dz)) / p.h;
-  const float aa = 1.0f - q / 2.0f;
-  float w = aa * aa * aa;
-  w = w * aa;
-  w *= (2.0f * q + 1.0f) * p.adh;
-  rsum += (rp.y - fabsf(rp.x) * ((0.0f - p.g) * dz)) * w;
-  wsum += w;
+  wall_term_core(kp, pi, ptc_xyz<PRECISE>(kp, ptc, j, ci), reinterpret_cast<const float2*>(ptc.rhop)[j], rsum, wsum);
 }
 
 using u64 = unsigned long long;
@@ -392,57 +393,28 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
 }
 
 // The end of particle i's list build, once s.nb holds its finished list
-// (cnt entries, or ovf): with WALL a non-fluid particle extrapolates its
-// (rho, p) from the fluid neighbours of its boundary rows
-// (delta_ns.cu:61-85, :116-131), summed in list order; then the particle's
-// packed shadow record (with a wall's new values) and its list count.
-template <int GF, bool WALL, bool PRECISE>
-__device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc,
-                                          const zsph_tmp_t& t, int i, int c, int cnt, bool ovf, float4 pi,
-                                          float2 rp_self, int3 ci) {
-  constexpr int NR = Stencil<GF>::NR;
-  float rho_w = 0.0f, p_w = 0.0f;
-  bool wall_new = false;
-  if (WALL && !fluid_of(pi.w)) {
-    float rsum = 0.0f, wsum = 0.0f;
-    if (!ovf) {
-      for (int k = 0; k < cnt; ++k) {  // this particle's own list, just written
-        const unsigned e = s.nb[nb_vec(i, k >> 3) * 8 + (k & 7)];
-        const int r = (int)(e >> kRowShift);
-        if (Stencil<GF>::boundary_row(r)) {
-          int a, b;  // the row's start (its cell bounds are L1-resident by now)
-          row_range<GF>(kp, t, c, r, a, b);
-          wall_term_ptc<PRECISE>(kp, ptc, pi, a + (int)(e & kOffMask), rsum, wsum, ci);
-        }
-      }
-    } else {
-      for (int r = 0; r < NR; ++r) {
-        if (!Stencil<GF>::boundary_row(r)) continue;
-        int a, b;
-        row_range<GF>(kp, t, c, r, a, b);
-        for (int j = a; j < b; ++j) {
-          if (j == i) continue;
-          const float4 pj = ptc_xyz<PRECISE>(kp, ptc, j, ci);
-          if (interacts(kp, dist2(pi.x - pj.x, pi.y - pj.y, pi.z - pj.z))) wall_term_ptc<PRECISE>(kp, ptc, pi, j, rsum, wsum, ci);
-        }
-      }
-    }
-    const zsph_gpu_param_t& p = kp.p;
-    if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
-    if (rsum < 0.0f) rsum = 0.0f;
-    rho_w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
-    p_w = rsum;
-    wall_new = true;
-  }
-  float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
-  float4 pr = pi;
-  if (wall_new) {
-    pr.w = rho_w;
-    vp.w = p_w;
-  }
-  st_rec(&s.sh.pr(i), pr, vp);
+// (cnt entries, or ovf): the particle's packed shadow record and list
+// count, and, for a non-fluid particle, its slot appended to s.wl for the
+// wall pass (k_walls).  Every active lane of the warp calls it together.
+template <int GF, bool PRECISE>
+__device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, int i, int cnt,
+                                          bool ovf, float4 pi, float2 rp_self) {
+  const float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
+  st_rec(&s.sh.pr(i), pi, vp);
   s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+  const unsigned m = __activemask();
+  const bool wall = !fluid_of(pi.w);
+  const unsigned wm = __ballot_sync(m, wall);
+  if (wm) {  // one atomic per warp
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s.misc[7], __popc(wm));
+    base = __shfl_sync(m, base, leader);
+    const int slot = base + __popc(wm & lanemask_lt());
+    if (wall && slot < kp.n) s.wl[slot] = i;
+  }
 }
+
 
 constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // Builds the neighbour lists of 32 consecutive sorted particles per warp,
@@ -469,9 +441,7 @@ constexpr int kCellWarps = 4;  // warps per CTA in the list build
 // kernels); every candidate lies within GF cells of it, so each shift k * gs
 // is exact and one rounding forms every coordinate.
 //
-// With WALL, every non-fluid particle then extrapolates its (rho, p) from
-// the fluid neighbours of its boundary rows (delta_ns.cu:61-85, :116-131),
-// summed in the reference's visit order, and publishes it in the shadows.
+// The walls' (rho, p) come after, from the finished lists (k_walls).
 constexpr int kRing = 32;  // list-build ring entries per lane (power of two)
 constexpr int kSegs = 4;   // list build: cells whose lanes test their own rows concurrently
 constexpr int kStage = 66; // list build: staged candidates per segment (64) plus two floats of padding
@@ -486,7 +456,7 @@ template <int GF> constexpr int kSeqWarps = GF == 1 ? kCellWarps : 2;
 // 32*group .. 32*group+31); k_nblist_seq runs one group per warp, the
 // batched form's persistent kernel loops over groups.  The warp's staging
 // arrays are slot `wid` of the CTA's CW slots.
-template <int GF, bool WALL, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs, bool SKIN = false>
+template <int GF, int CW, bool BATCH, bool PRECISE, int SEGS = kSegs, bool SKIN = false>
 __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratch& s, const zsph_ptc_t& ptc,
                                              const zsph_tmp_t& t, int group, int wid) {
   constexpr int NR = Stencil<GF>::NR;
@@ -656,15 +626,15 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
   if (SKIN && act) s.xf.sk_cnt[i] = skovf ? kOverflow : (uint8_t)kc;
-  if (act) list_tail<GF, WALL, PRECISE>(kp, s, ptc, t, i, c, cnt, ovf, pi, rp_self, ci);
+  if (act) list_tail<GF, PRECISE>(kp, s, ptc, i, cnt, ovf, pi, rp_self);
 }
 
-template <int GF, bool WALL, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs,
+template <int GF, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs,
           bool SKIN = false>
 __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_seq(KParams kp_arg, Scratch s, zsph_ptc_t ptc,
                                                                    zsph_tmp_t t) {
   const int wid = threadIdx.x >> 5;
-  nblist_group<GF, WALL, CW, BATCH, PRECISE, SEGS, SKIN>(kp_arg, s, ptc, t, blockIdx.x * CW + wid, wid);
+  nblist_group<GF, CW, BATCH, PRECISE, SEGS, SKIN>(kp_arg, s, ptc, t, blockIdx.x * CW + wid, wid);
 }
 
 // The list transfer's fallback: the full list build of the corrector, run
@@ -676,7 +646,7 @@ __global__ void __launch_bounds__(CW * 32, 42 / CW) k_nblist_fallback(KParams kp
   if (*s.xf.flag == 0) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(s.xf.stats + 1, 1ull);
   const int wid = threadIdx.x >> 5;
-  nblist_group<1, true, CW, false, false, SEGS>(kp, s, ptc, t, blockIdx.x * CW + wid, wid);
+  nblist_group<1, CW, false, false, SEGS>(kp, s, ptc, t, blockIdx.x * CW + wid, wid);
 }
 
 struct NbB1 {  // boundary loop 1
@@ -715,6 +685,54 @@ template <int GF> struct PairSmem {
     win = reinterpret_cast<float4*>(dsm + 3 * NR * kPairBlock * 4 + kHdrBytes);
   }
 };
+
+// The walls' (rho, p) after the list build (delta_ns.cu:61-85, :116-131):
+// non-fluid particle i extrapolates from the fluid neighbours of its
+// boundary rows, summed in list order, and rewrites the (rho, p) of its
+// packed record (its density stays negative, non-fluid).  The list build has
+// written every record by then, so each neighbour costs one 256-bit load
+// (four ahead of the arithmetic, as in the pair walks), and no fluid record
+// read here is written.  A particle whose list overflowed re-filters its
+// boundary rows.
+template <int GF, bool PRECISE, bool BATCH>
+__device__ __forceinline__ void walls_one(const KParams& kp_arg, const Scratch& s, const zsph_tmp_t& t, int i,
+                                          const PairSmem<GF>& sm) {
+  KParams kp_scene;  // batched form: the parameters of the particle's scene
+  if constexpr (BATCH) kp_scene = kp_of_particle(kp_arg, i);
+  const KParams& kp = BATCH ? kp_scene : kp_arg;
+  const ShadowRec own = s.sh.load(i);
+  const float4 pi = own.pr;
+  const int3 ci = PRECISE ? unpack_cell(kp.c3n[i]) : int3{0, 0, 0};
+  load_rows<GF>(kp, t, t.hash[i], sm.rs, sm.re);
+  float rsum = 0.0f, wsum = 0.0f;
+  walk<GF, true, NbB1, PRECISE>(
+      kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
+      [&](int q) {
+        const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+        return NbB1{r.pr, r.vp};
+      },
+      [&](const NbB1& nb) {
+        if (fluid_of(nb.pr.w)) wall_term_core(kp, pi, nb.pr, make_float2(nb.pr.w, nb.vp.w), rsum, wsum);
+      },
+      ci);
+  const zsph_gpu_param_t& p = kp.p;
+  if (fabsf(wsum) > 1e-8f) rsum = rsum / wsum; else rsum = 0.0f;
+  if (rsum < 0.0f) rsum = 0.0f;
+  float4 pr = own.pr, vp = own.vp;
+  pr.w = -(rsum / p.cs2 + p.rho0);  // still non-fluid
+  vp.w = rsum;
+  st_rec(&s.sh.pr(i), pr, vp);
+}
+
+// The wall pass over the slots the list build listed in s.wl (grid-stride).
+template <int GF, bool PRECISE = false, bool BATCH = false>
+__global__ void __launch_bounds__(kPairBlock) k_walls(KParams kp, Scratch s, zsph_tmp_t t) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const PairSmem<GF> sm(dsm);
+  const int nw = min(s.misc[7], kp.n);
+  for (int q = blockIdx.x * kPairBlock + threadIdx.x; q < nw; q += gridDim.x * kPairBlock)
+    walls_one<GF, PRECISE, BATCH>(kp, s, t, s.wl[q], sm);
+}
 
 // cuda_boundary_ns main part (delta_ns.cu:35-174): renormalisation matrix and
 // div(v) over the boundary stencil, cofactor inverse, renormalised grad(rho).
@@ -788,11 +806,11 @@ __device__ __forceinline__ void boundary_one(const KParams& kp_arg, const Scratc
       walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapB - 1,
                            [&](int q) { return NbB1{win[2 * q], win[2 * q + 1]}; }, use1);
     else
-      walk<GF, true, NbB1>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
-                           [&](int q) {
-                             const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
-                             return NbB1{r.pr, r.vp};
-                           }, use1);
+      walk<GF, true, NbB1, PRECISE>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
+                                    [&](int q) {
+                                      const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+                                      return NbB1{r.pr, r.vp};
+                                    }, use1, ci);
   }
   // delta_ns.cu:99-114 (L is symmetric: L1 = (xx,xy,xz), L2 = (xy,yy,yz), L3 = (xz,yz,zz))
   const float det = Lxx * Lyy * Lzz + Lxy * Lyz * Lxz + Lxz * Lxy * Lyz - Lxz * Lyy * Lxz - Lxx * Lyz * Lyz -
@@ -959,11 +977,11 @@ __device__ __forceinline__ void governing_one(const KParams& kp_arg, const Scrat
     walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.fb, 0, kWinCapG - 1,
                          [&](int q) { return NbG{win[2 * q], win[2 * q + 1], win[2 * kWinCapG + q]}; }, use);
   else
-    walk<GF, false, NbG>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
-                         [&](int q) {
-                           const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
-                           return NbG{r.pr, r.vp, dg[q]};
-                         }, use);
+    walk<GF, false, NbG, PRECISE>(kp, s, i, pi, sm.rs, sm.re, sm.rs, i, kp.n - 1,
+                                  [&](int q) {
+                                    const ShadowRec r = shadow_rec<PRECISE>(kp, s, q, ci);
+                                    return NbG{r.pr, r.vp, dg[q]};
+                                  }, use, ci);
   if (rig) kp.rigid_f[i] = make_float4(rf.x, rf.y, rf.z, 0.f);
   acc.z += p.g;  // delta_ns.cu:264
   reinterpret_cast<float4*>(t.acc_drhodt)[i] = acc;
@@ -1034,7 +1052,7 @@ struct NbS {  // simple boundary / governing
 
 // single_gpu_sph_src/equation/simple_ns.cu:3-97: scalar div(v) over fluid
 // pairs of the boundary stencil into tmp.dofv; new wall (rho, p) (computed
-// by k_nblist_seq) into ptc.rhop.  Walls read only fluid densities here, so the
+// by k_walls) into ptc.rhop.  Walls read only fluid densities here, so the
 // reference has no wall-density race in this kernel.
 template <int GF>
 __global__ void __launch_bounds__(kPairBlock) k_boundary_simple(KParams kp, Scratch s, zsph_ptc_t ptc,
@@ -1124,7 +1142,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_integrate(KParams kp, zsph_ptc
 inline int thread_blocks(int n) { return (n + kPairBlock - 1) / kPairBlock; }
 
 // list build (grid factor 1) with the tuned number of cells per CTA
-template <bool WALL, bool BATCH>
+template <bool BATCH>
 void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                          cudaStream_t st) {
   // (eight cells per CTA would exceed the 48 KB of static shared memory)
@@ -1133,13 +1151,13 @@ void launch_nblist_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_t& 
   const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
   const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
   if (kp.tune_cw == 4) {
-    if (segs == 2) k_nblist_seq<1, WALL, 4, BATCH, false, 2><<<g4, 128, 0, st>>>(kp, s, ptc, t);
-    else if (segs == 3) k_nblist_seq<1, WALL, 4, BATCH, false, 3><<<g4, 128, 0, st>>>(kp, s, ptc, t);
-    else k_nblist_seq<1, WALL, 4, BATCH, false, 4><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    if (segs == 2) k_nblist_seq<1, 4, BATCH, false, 2><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, 4, BATCH, false, 3><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, 4, BATCH, false, 4><<<g4, 128, 0, st>>>(kp, s, ptc, t);
   } else {
-    if (segs == 2) k_nblist_seq<1, WALL, 2, BATCH, false, 2><<<g2, 64, 0, st>>>(kp, s, ptc, t);
-    else if (segs == 3) k_nblist_seq<1, WALL, 2, BATCH, false, 3><<<g2, 64, 0, st>>>(kp, s, ptc, t);
-    else k_nblist_seq<1, WALL, 2, BATCH, false, 4><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    if (segs == 2) k_nblist_seq<1, 2, BATCH, false, 2><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, 2, BATCH, false, 3><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, 2, BATCH, false, 4><<<g2, 64, 0, st>>>(kp, s, ptc, t);
   }
 }
 
@@ -1159,28 +1177,53 @@ void launch_governing_tuned(const KParams& kp, const Scratch& s, const zsph_ptc_
   }
 }
 
+// The wall pass: enough CTAs to fill the device, each looping over s.wl
+// (its length is known on the device only).
+template <int GF, bool PRECISE = false, bool BATCH = false>
+void launch_walls(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cudaStream_t st) {
+  static int sms = 0;  // SMs of the device (the same for every B200)
+  if (!sms) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      sms = 148;
+  }
+  k_walls<GF, PRECISE, BATCH><<<min(thread_blocks(kp.n), sms * 16), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, t);
+}
+
+// zeroes the wall-list length before a list build appends to it
+inline cudaError_t reset_walls(const Scratch& s, cudaStream_t st) {
+  return cudaMemsetAsync(s.misc + 7, 0, sizeof(int), st);
+}
+
 template <int GF>
 cudaError_t boundary_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, const zsph_tmp_t& t,
                         cudaStream_t st, Prof* pf) {
+  if (cudaError_t e = reset_walls(s, st)) return e;
   if (kp.scenes) {  // batched form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA || kp.c3o) return cudaErrorInvalidValue;
-    launch_nblist_tuned<true, true>(kp, s, ptc, t, st);
-    mark(pf, "nblist_wall", st);
+    launch_nblist_tuned<true>(kp, s, ptc, t, st);
+    mark(pf, "nblist", st);
+    launch_walls<1, false, true>(kp, s, t, st);
+    mark(pf, "walls", st);
     k_boundary<1, false, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
     mark(pf, "boundary", st);
     return cudaGetLastError();
   }
   if (kp.c3o) {  // precision form (grid factor 1, delta equations)
     if (GF != 1 || kp.equations != ZSPH_EQ_DELTA) return cudaErrorInvalidValue;
-    k_nblist_seq<1, true, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
-    mark(pf, "nblist_wall", st);
+    k_nblist_seq<1, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
+    mark(pf, "nblist", st);
+    launch_walls<1, true>(kp, s, t, st);
+    mark(pf, "walls", st);
     k_boundary<1, true><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
     mark(pf, "boundary", st);
     return cudaGetLastError();
   }
-  if (GF == 1) launch_nblist_tuned<true, false>(kp, s, ptc, t, st);
-  else k_nblist_seq<GF, true, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
-  mark(pf, "nblist_wall", st);
+  if (GF == 1) launch_nblist_tuned<false>(kp, s, ptc, t, st);
+  else k_nblist_seq<GF, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
+  mark(pf, "nblist", st);
+  launch_walls<GF>(kp, s, t, st);
+  mark(pf, "walls", st);
   if (kp.equations == ZSPH_EQ_SIMPLE)
     k_boundary_simple<GF><<<thread_blocks(kp.n), kPairBlock, pair_smem<GF>(0, 0), st>>>(kp, s, ptc, t);
   else
@@ -1260,12 +1303,12 @@ cudaError_t nblist_gf(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc
                       cudaStream_t st) {
   if (kp.scenes) {
     if (GF != 1) return cudaErrorInvalidValue;
-    launch_nblist_tuned<false, true>(kp, s, ptc, t, st);
+    launch_nblist_tuned<true>(kp, s, ptc, t, st);
   } else if (kp.c3o) {
     if (GF != 1) return cudaErrorInvalidValue;
-    k_nblist_seq<1, false, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
+    k_nblist_seq<1, kCellWarps, false, true><<<(kp.n + 32 * kCellWarps - 1) / (32 * kCellWarps), kCellWarps * 32, 0, st>>>(kp, s, ptc, t);
   } else {
-    k_nblist_seq<GF, false, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
+    k_nblist_seq<GF, kSeqWarps<GF>><<<(kp.n + 32 * kSeqWarps<GF> - 1) / (32 * kSeqWarps<GF>), kSeqWarps<GF> * 32, 0, st>>>(kp, s, ptc, t);
   }
   return cudaGetLastError();
 }
@@ -1406,7 +1449,7 @@ __global__ void __launch_bounds__(kPairBlock) k_rigid_contact(KParams kp, Scratc
 // blocks.  The stages of a sub-step (from = old_, to = new_, as the fused
 // step): hash and tickets | one-pass scan (tiles claimed in order) | scatter
 // | crowded cells sorted, if the scan listed any | rank and gather | list
-// build and wall pressure | boundary | governing with the prediction or
+// build | wall pressure | boundary | governing with the prediction or
 // correction into old_.
 //
 // Grid barrier: a CTA's thread 0 arrives on a counter and waits for the
@@ -1529,9 +1572,17 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_batch_persistent(Persist
       if (!grid_barrier(a)) return;
       for (int t = blockIdx.x * kPersistThreads + threadIdx.x; t < n; t += gridDim.x * kPersistThreads)
         rank_gather_one<false>(kp, s, a.o, a.w, a.t, t);
+      if (blockIdx.x == 0 && threadIdx.x == 0) s.misc[7] = 0;  // the wall list, appended by the list build
       if (!grid_barrier(a)) return;
       for (int g = blockIdx.x * kPersistWarps + wid; g < groups; g += gridDim.x * kPersistWarps)
-        nblist_group<1, true, kPersistWarps, true, false>(kp, s, a.w, a.t, g, wid);
+        nblist_group<1, kPersistWarps, true, false>(kp, s, a.w, a.t, g, wid);
+      if (!grid_barrier(a)) return;
+      {
+        const int nw = min(s.misc[7], n);
+        const PairSmem<1> sm(dsm + (threadIdx.x / kPairBlock) * pair_smem<1>(0, 0), threadIdx.x % kPairBlock);
+        for (int q = blockIdx.x * kPersistThreads + threadIdx.x; q < nw; q += gridDim.x * kPersistThreads)
+          walls_one<1, false, true>(kp, s, a.t, s.wl[q], sm);
+      }
       if (!grid_barrier(a)) return;
       persistent_pairs<0>(a, dsm);
       if (!grid_barrier(a)) return;
@@ -1904,7 +1955,7 @@ __global__ void __launch_bounds__(kXferThreads) k_nblist_xfer(KParams kp, Scratc
   so.nb_cnt = s.xf.nb_cnt2;
   const float2 rp = reinterpret_cast<const float2*>(cur.rhop)[i];
   const float4 pc = make_float4(cur.pos[3 * i], cur.pos[3 * i + 1], cur.pos[3 * i + 2], packed_rho(rp.x, cur.type[i]));
-  list_tail<1, true, false>(kp, so, cur, t, i, c, ovf ? 0 : cnt, ovf, pc, rp, int3{0, 0, 0});
+  list_tail<1, false>(kp, so, cur, i, ovf ? 0 : cnt, ovf, pc, rp);
 }
 
 }  // namespace
@@ -2037,18 +2088,21 @@ cudaError_t launch_xfer_pred_lists(const KParams& kp, const Scratch& s, const zs
   if (kp.n == 0) return cudaSuccess;
   if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.stage_windows || kp.equations != ZSPH_EQ_DELTA || !s.xf.sk)
     return cudaErrorInvalidValue;
+  if (cudaError_t e = reset_walls(s, st)) return e;
   const int segs = kp.tune_segs ? kp.tune_segs : kSegs;
   const int g4 = (kp.n + 127) / 128, g2 = (kp.n + 63) / 64;
   if (kp.tune_cw == 4) {
-    if (segs == 2) k_nblist_seq<1, true, 4, false, false, 2, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
-    else if (segs == 3) k_nblist_seq<1, true, 4, false, false, 3, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
-    else k_nblist_seq<1, true, 4, false, false, 4, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    if (segs == 2) k_nblist_seq<1, 4, false, false, 2, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, 4, false, false, 3, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, 4, false, false, 4, true><<<g4, 128, 0, st>>>(kp, s, ptc, t);
   } else {
-    if (segs == 2) k_nblist_seq<1, true, 2, false, false, 2, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
-    else if (segs == 3) k_nblist_seq<1, true, 2, false, false, 3, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
-    else k_nblist_seq<1, true, 2, false, false, 4, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    if (segs == 2) k_nblist_seq<1, 2, false, false, 2, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else if (segs == 3) k_nblist_seq<1, 2, false, false, 3, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
+    else k_nblist_seq<1, 2, false, false, 4, true><<<g2, 64, 0, st>>>(kp, s, ptc, t);
   }
-  mark(pf, "nblist_wall", st);
+  mark(pf, "nblist", st);
+  launch_walls<1>(kp, s, t, st);
+  mark(pf, "walls", st);
   k_boundary<1><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s, ptc, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();
@@ -2059,6 +2113,7 @@ cudaError_t launch_xfer_corr_lists(const KParams& kp, const Scratch& s, const zs
   if (kp.n == 0) return cudaSuccess;
   if (kp.p.grid_factor != 1 || kp.scenes || kp.c3o || kp.stage_windows || kp.equations != ZSPH_EQ_DELTA || !s.xf.nb2)
     return cudaErrorInvalidValue;
+  if (cudaError_t e = reset_walls(s, st)) return e;
   k_xfer_classify<<<(kp.n + kSearchBlock - 1) / kSearchBlock, kSearchBlock, 0, st>>>(kp, s, t);
   mark(pf, "xfer_classify", st);
   static int sms = 0;  // SMs of the device (the same for every B200)
@@ -2086,6 +2141,8 @@ cudaError_t launch_xfer_corr_lists(const KParams& kp, const Scratch& s, const zs
     else k_nblist_fallback<2, 4><<<g2, 64, 0, st>>>(kp, s2, cur, t);
   }
   mark(pf, "nblist_fallback", st);
+  launch_walls<1>(kp, s2, t, st);
+  mark(pf, "walls", st);
   k_boundary<1><<<thread_blocks(kp.n), kPairBlock, pair_smem<1>(0, 0), st>>>(kp, s2, cur, t);
   mark(pf, "boundary", st);
   return cudaGetLastError();

@@ -202,11 +202,13 @@ struct Scratch {
   int* tile_off;     // [tiles]
   int* tile_last;    // [tiles] last occupied cell of each tile (-1 if none)
   int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length,
-                     //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch
+                     //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch,
+                     //       7: entries in wl (zeroed before each list build)
   unsigned long long* tile_state;  // [tiles] one-pass scan: (tag << 32) | prefix value, tag from the epoch
   int* big_list;     // [kBigListCap]
   uint16_t* nb;      // [ceil(n/32)*32 * kMaxNb] neighbour lists, blocked by 32-particle groups (equations.cu)
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
+  int* wl;           // [n] sorted slots of the non-fluid particles, appended by the list build (unordered)
   int* flags;        // [1]   ZSPH_FLAG_* bits
   Shadow sh;
   Xfer xf;           // list transfer scratch (null pointers when the handle has none)
