@@ -305,3 +305,31 @@ def test_body_api_rejects_overlap_and_bad_contact():
     s.attach_body(b["first"], b["count"], 2 * b["mass"])  # same first index: replaces
     assert s.body_count() == 1 and s.body(0)["mass"] == 2 * b["mass"]
     s.close()
+
+
+def test_overflowed_lists_in_the_precision_form():
+    # a block of fluid compressed to 0.7 of its spacing: its particles have
+    # more than 128 neighbours within 2h, so the pair walks re-filter their
+    # stencil rows (with the candidates moved into the particle's cell frame
+    # in the precision form); both forms must then agree to FP32 rounding
+    dx = 0.04
+    c = cases.dam_break(dx, end_step=20)
+    pos = c.state.pos
+    fl = c.state.type == 1
+    ctr = np.median(pos[fl], axis=0).astype(np.float32)
+    box = fl & np.all(np.abs(pos - ctr) < 3.5 * dx, axis=1)
+    pos[box] = (ctr + np.float32(0.7) * (pos[box] - ctr)).astype(np.float32)
+    c.state.tmp_pos[:] = pos
+    c = dataclasses.replace(c, pos64=pos.astype(np.float64))
+    got = {}
+    for precise in (False, True):
+        s = _solver(c, precise)
+        s.run(2)
+        f = s.status()
+        assert f & z.FLAG_NB_OVERFLOW and not f & z.FLAG_NAN
+        st = s.download("old")
+        got[precise] = _by_id(st, c.n, st.vel.astype(np.float64))
+        s.close()
+    dv = np.abs(got[True] - got[False]).max()
+    scale = np.abs(got[False]).max()
+    assert dv < 1e-3 * scale, f"max |dv| {dv:.3e} of {scale:.3e}"

@@ -402,6 +402,7 @@ __device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, c
   const float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
   st_rec(&s.sh.pr(i), pi, vp);
   s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
+  if (ovf) atomicOr(s.flags, ZSPH_FLAG_NB_OVERFLOW);  // rare: the walks re-filter this particle's rows
   const unsigned m = __activemask();
   const bool wall = !fluid_of(pi.w);
   const unsigned wm = __ballot_sync(m, wall);
@@ -1783,6 +1784,7 @@ __device__ __forceinline__ void xfer_full_search(const KParams& kp, const Scratc
   }
   if (cnt > 254) ovf = true;
   if (lane == 0) s.xf.nb_cnt2[M] = ovf ? kOverflow : (uint8_t)cnt;
+  if (lane == 0 && ovf) atomicOr(s.flags, ZSPH_FLAG_NB_OVERFLOW);
 }
 
 // Corrector, after its search: each slot's class (fullb), its corrector
