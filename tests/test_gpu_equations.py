@@ -127,23 +127,31 @@ def test_run_graph_equals_steps():
     b.close()
 
 
-def test_step_matches_dropin_sequence():
+@pytest.mark.parametrize("mk,nsteps", [(lambda: cases.small(0.04), 1),
+                                       # 30 % of the particles killed into cell 0: a crowded cell
+                                       # (> 256 members) that the fused scatter pre-sorts every search
+                                       (lambda: cases.random_cloud(6000, 3, kill_frac=0.3), 3)],
+                         ids=["small_dam", "crowded_cell"])
+def test_step_matches_dropin_sequence(mk, nsteps):
     # zsph_step (fused search + fused integration) against the reference's
-    # call order through the drop-in entry points (main.cu:63-88)
-    c = cases.small(0.04)
+    # call order through the drop-in entry points (main.cu:63-88), step
+    # after step (the fused path's scratch carries state across searches)
+    c = mk()
     a = z.Solver.from_case(c)
     b = z.Solver.from_case(c)
-    a.step()
-    b.hash("old"); b.sort_index(); b.sort_data("old", "new")
-    b.boundary("new"); b.governing("new"); b.prediction("new")
-    b.hash("new"); b.sort_index(); b.sort_data("new", "old")
-    b.boundary("old"); b.governing("old"); b.correction("old")
+    for _ in range(nsteps):
+        a.step()
+        b.hash("old"); b.sort_index(); b.sort_data("old", "new")
+        b.boundary("new"); b.governing("new"); b.prediction("new")
+        b.hash("new"); b.sort_index(); b.sort_data("new", "old")
+        b.boundary("old"); b.governing("old"); b.correction("old")
+    bits = lambda v: np.ascontiguousarray(v).view(np.uint32)  # identical, NaNs included
     sa, sb = a.download("old"), b.download("old")
     for k in ("pos", "vel", "rhop", "table", "type", "tmp_pos", "tmp_vel", "tmp_rhop"):
-        assert np.array_equal(getattr(sa, k), getattr(sb, k)), k
+        assert np.array_equal(bits(getattr(sa, k)), bits(getattr(sb, k))), k
     ta, tb = a.download_tmp(), b.download_tmp()
     for k in ("hash", "index", "grid_start", "grid_end", "acc_drhodt", "dofv_grandrho"):
-        assert np.array_equal(ta[k], tb[k]), k
+        assert np.array_equal(bits(ta[k]), bits(tb[k])), k
     a.close()
     b.close()
 

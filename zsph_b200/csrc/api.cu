@@ -394,7 +394,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.tile_off, (size_t)h->tiles);
   if (!e) e = dalloc(s.tile_last, (size_t)h->tiles);
   if (!e) e = dalloc(s.tile_state, (size_t)h->tiles);
-  if (!e) e = dalloc(s.misc, 8);
+  if (!e) e = dalloc(s.misc, kMiscWords);
   if (!e) e = dalloc(s.big_list, (size_t)kBigListCap);
   if (!e) e = dalloc(s.nb, (size_t)kMaxNb * ((n + 31) & ~(size_t)31));  // whole 32-particle list groups
   if (!e) e = dalloc(s.nb_cnt, n);
@@ -402,7 +402,7 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.flags, 1);
   if (!e) e = dalloc(s.sh.rec, 2 * (size_t)n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
-  if (!e) e = cudaMemset(s.misc, 0, 8 * sizeof(int));
+  if (!e) e = cudaMemset(s.misc, 0, kMiscWords * sizeof(int));
   if (!e) e = cudaMemset(s.tile_state, 0, (size_t)h->tiles * sizeof(unsigned long long));
   if (!e) e = cudaMemset(s.flags, 0, sizeof(int));
   if (!e) e = cudaMemset(s.nb_cnt, 0, n ? n : 1);

@@ -409,7 +409,7 @@ __device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, c
   if (wm) {  // one atomic per warp
     const int leader = __ffs(m) - 1;
     int base = 0;
-    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s.misc[7], __popc(wm));
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&s.misc[kMiscWalls], __popc(wm));
     base = __shfl_sync(m, base, leader);
     const int slot = base + __popc(wm & lanemask_lt());
     if (wall && slot < kp.n) s.wl[slot] = i;
@@ -730,7 +730,7 @@ template <int GF, bool PRECISE = false, bool BATCH = false>
 __global__ void __launch_bounds__(kPairBlock) k_walls(KParams kp, Scratch s, zsph_tmp_t t) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const PairSmem<GF> sm(dsm);
-  const int nw = min(s.misc[7], kp.n);
+  const int nw = min(s.misc[kMiscWalls], kp.n);
   for (int q = blockIdx.x * kPairBlock + threadIdx.x; q < nw; q += gridDim.x * kPairBlock)
     walls_one<GF, PRECISE, BATCH>(kp, s, t, s.wl[q], sm);
 }
@@ -1193,7 +1193,7 @@ void launch_walls(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, cuda
 
 // zeroes the wall-list length before a list build appends to it
 inline cudaError_t reset_walls(const Scratch& s, cudaStream_t st) {
-  return cudaMemsetAsync(s.misc + 7, 0, sizeof(int), st);
+  return cudaMemsetAsync(s.misc + kMiscWalls, 0, sizeof(int), st);
 }
 
 template <int GF>
@@ -1573,13 +1573,13 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_batch_persistent(Persist
       if (!grid_barrier(a)) return;
       for (int t = blockIdx.x * kPersistThreads + threadIdx.x; t < n; t += gridDim.x * kPersistThreads)
         rank_gather_one<false>(kp, s, a.o, a.w, a.t, t);
-      if (blockIdx.x == 0 && threadIdx.x == 0) s.misc[7] = 0;  // the wall list, appended by the list build
+      if (blockIdx.x == 0 && threadIdx.x == 0) s.misc[kMiscWalls] = 0;  // the wall list, appended by the list build
       if (!grid_barrier(a)) return;
       for (int g = blockIdx.x * kPersistWarps + wid; g < groups; g += gridDim.x * kPersistWarps)
         nblist_group<1, kPersistWarps, true, false>(kp, s, a.w, a.t, g, wid);
       if (!grid_barrier(a)) return;
       {
-        const int nw = min(s.misc[7], n);
+        const int nw = min(s.misc[kMiscWalls], n);
         const PairSmem<1> sm(dsm + (threadIdx.x / kPairBlock) * pair_smem<1>(0, 0), threadIdx.x % kPairBlock);
         for (int q = blockIdx.x * kPersistThreads + threadIdx.x; q < nw; q += gridDim.x * kPersistThreads)
           walls_one<1, false, true>(kp, s, a.t, s.wl[q], sm);

@@ -190,6 +190,9 @@ inline bool ptc_aligned8(const zsph_ptc_t& p) {
   return true;
 }
 
+constexpr int kMiscWords = 16;  // Scratch::misc
+constexpr int kMiscWalls = 8;   // misc word holding the wall list's length
+
 // Device scratch owned by a handle; allocated once in zsph_create.
 struct Scratch {
   int* cnt;          // [G]   per-cell counts (kept zero between uses)
@@ -201,9 +204,10 @@ struct Scratch {
   int* tile_sum;     // [tiles]
   int* tile_off;     // [tiles]
   int* tile_last;    // [tiles] last occupied cell of each tile (-1 if none)
-  int* misc;         // [8]   0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length,
+  int* misc;         // [kMiscWords] 0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length,
                      //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch,
-                     //       7: entries in wl (zeroed before each list build)
+                     //       7: the fused scatter's finished-CTA counter (crowded cells),
+                     //       kMiscWalls: entries in wl (zeroed before each list build)
   unsigned long long* tile_state;  // [tiles] one-pass scan: (tag << 32) | prefix value, tag from the epoch
   int* big_list;     // [kBigListCap]
   uint16_t* nb;      // [ceil(n/32)*32 * kMaxNb] neighbour lists, blocked by 32-particle groups (equations.cu)
