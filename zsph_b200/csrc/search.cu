@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp_in, zsph_ptc_t
 }
 
 __global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp_in, zsph_ptc_t s, Scratch sc) {
+  pdl_wait();
   hash_count_body(kp_in, s, sc, blockIdx.x);
 }
 
@@ -170,6 +171,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_scan_cells(KParams kp, Scratch
 
 __global__ void __launch_bounds__(kSearchBlock) k_scan_onepass(KParams kp, Scratch sc, zsph_tmp_t t) {
   __shared__ int s_tile;
+  pdl_wait();
   if (threadIdx.x == 0) s_tile = atomicAdd(&sc.misc[5], 1);
   __syncthreads();
   scan_onepass_body(kp, sc, t, s_tile);
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_scatter(KParams kp, Scratch sc
 // that protocol, and the common case costs no extra launch.
 __global__ void __launch_bounds__(kSearchBlock) k_scatter_fused(KParams kp, Scratch sc) {
   __shared__ bool s_last;
+  pdl_wait();
   const bool crowded = sc.misc[3] != 0;
   scatter_body(kp, sc, blockIdx.x);
   if (!crowded) return;
@@ -244,6 +247,7 @@ __global__ void __launch_bounds__(1024) k_sort_big_cells(KParams kp, Scratch sc)
 // particle's arrays anyway.
 __global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
                                                               zsph_tmp_t t) {
+  pdl_wait();
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot >= kp.n) return;
   rank_gather_one(kp, sc, o, w, t, slot);
@@ -342,15 +346,17 @@ cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const 
                           const zsph_tmp_t& tmp, cudaStream_t st, Prof* pf) {
   if (kp.n == 0) return cudaSuccess;
   if (!ptc_aligned8(o) || !ptc_aligned8(w)) return cudaErrorMisalignedAddress;  // nothing launched
-  k_hash_count<<<blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st>>>(kp, o, s);
+  // each kernel waits for its predecessor's completion first (pdl_wait), so
+  // only the launches overlap the predecessors' drain
+  cudaError_t e = launch_pdl(k_hash_count, blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st, kp, o, s);
   mark(pf, "hash_count", st);
-  k_scan_onepass<<<(kp.G + kOneTile - 1) / kOneTile, kSearchBlock, 0, st>>>(kp, s, tmp);
+  if (!e) e = launch_pdl(k_scan_onepass, (kp.G + kOneTile - 1) / kOneTile, kSearchBlock, 0, st, kp, s, tmp);
   mark(pf, "scan", st);
-  k_scatter_fused<<<blocks_for(kp.n, kSearchBlock * kScatterItems), kSearchBlock, 0, st>>>(kp, s);
+  if (!e) e = launch_pdl(k_scatter_fused, blocks_for(kp.n, kSearchBlock * kScatterItems), kSearchBlock, 0, st, kp, s);
   mark(pf, "scatter", st);
-  k_rank_gather<<<blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st>>>(kp, s, o, w, tmp);
+  if (!e) e = launch_pdl(k_rank_gather, blocks_for(kp.n, kSearchBlock), kSearchBlock, 0, st, kp, s, o, w, tmp);
   mark(pf, "rank_gather", st);
-  return cudaGetLastError();
+  return e ? e : cudaGetLastError();
 }
 
 cudaError_t launch_pack_shadows(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, cudaStream_t st) {

@@ -193,6 +193,27 @@ inline bool ptc_aligned8(const zsph_ptc_t& p) {
 constexpr int kMiscWords = 16;  // Scratch::misc
 constexpr int kMiscWalls = 8;   // misc word holding the wall list's length
 
+// Programmatic dependent launch: the kernel's grid may start while the
+// previous kernel in the stream drains (a CUDA graph keeps the relation as
+// a programmatic edge).  Such a kernel calls pdl_wait() before anything
+// else: it returns once the previous grid has completed and its writes are
+// visible (and at once when there is no such grid).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Device scratch owned by a handle; allocated once in zsph_create.
 struct Scratch {
   int* cnt;          // [G]   per-cell counts (kept zero between uses)
