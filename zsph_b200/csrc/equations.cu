@@ -1826,8 +1826,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32) k_xfer_search(KParams kp, S
 constexpr int kXferThreads = 64;            // threads (particles) per CTA of k_nblist_xfer
 constexpr int kXBuf = kMaxNb + kSkinCap;    // a particle's merged predictor and skin entries
 
-// Corrector: the transferred lists (see above), then each particle's wall
-// (rho, p) and packed shadow record exactly as the full build's end does.
+// Corrector: the transferred lists (see above), then each particle's packed
+// shadow record, list count and wall-list entry exactly as the full build's
+// end does (the walls' (rho, p) follow in k_walls).
 // Returns at once when the full build runs instead (*s.xf.flag).
 // Per particle: (1) its predictor list and skin list merged by their keys
 // into shared memory (both are in the predictor's candidate order, so the
