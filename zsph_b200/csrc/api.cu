@@ -130,7 +130,7 @@ void free_xfer(Xfer& x) {
 
 void free_scratch(Scratch& s) {
   void* ptrs[] = {s.cnt, s.cell_lb, s.key, s.ticket, s.perm, s.val, s.tile_sum, s.tile_off, s.tile_last,
-                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.wl, s.flags, s.sh.rec};
+                  s.tile_state, s.misc, s.big_list, s.nb, s.nb_cnt, s.wl, s.cfe, s.flags, s.sh.rec};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   free_xfer(s.xf);
@@ -399,9 +399,11 @@ int zsph_create(const zsph_gpu_param_t* gp, int grid_num, zsph_handle_t** out) {
   if (!e) e = dalloc(s.nb, (size_t)kMaxNb * ((n + 31) & ~(size_t)31));  // whole 32-particle list groups
   if (!e) e = dalloc(s.nb_cnt, n);
   if (!e) e = dalloc(s.wl, n);
+  if (!e) e = dalloc(s.cfe, G);
   if (!e) e = dalloc(s.flags, 1);
   if (!e) e = dalloc(s.sh.rec, 2 * (size_t)n);
   if (!e) e = cudaMemset(s.cnt, 0, G * sizeof(int));
+  if (!e) e = cudaMemset(s.cfe, 0, G * sizeof(int));
   if (!e) e = cudaMemset(s.misc, 0, kMiscWords * sizeof(int));
   if (!e) e = cudaMemset(s.tile_state, 0, (size_t)h->tiles * sizeof(unsigned long long));
   if (!e) e = cudaMemset(s.flags, 0, sizeof(int));

@@ -392,19 +392,54 @@ __device__ __forceinline__ u64 fma2(u64 a, u64 b, u64 c) {
   return r;
 }
 
+// Whether a non-fluid particle in cell c can have a fluid neighbour in its
+// boundary rows (grid factor 1): a kept row (row_range) with possibly stale
+// bounds (sort.cu:30-60: a lone last particle in cell klast leaves the
+// bounds of cells >= klast) or a cell stamped by this search's gather as
+// holding a fluid particle.  False means the wall pass would sum nothing.
+// Without valid stamps (the drop-in gather ran) the answer is true.
+__device__ __forceinline__ bool walls_fluid_near(const KParams& kp, const Scratch& s, const zsph_tmp_t& t, int c) {
+  const int ep = s.misc[kMiscFluidEpoch];
+  if (ep == 0) return true;
+  const zsph_gpu_param_t& p = kp.p;
+  const int n = kp.n, klast = t.hash[n - 1];
+  const bool lone = n < 2 || klast != t.hash[n - 2];
+  bool any = false;
+#pragma unroll
+  for (int dz = -1; dz <= 1; ++dz)
+#pragma unroll
+    for (int dy = -1; dy <= 0; ++dy) {  // the boundary rows, y = -1 and 0 (delta_ns.cu:37)
+      const int cell = c + dz * kp.XY + dy * p.grid_xdim;
+      const int cs = cell - 1, ce = cell + 1;
+      if (cs < p.grid_hash_min || ce > p.grid_hash_max) continue;  // row_range drops it: no candidates
+      any |= (lone && ce >= klast) || s.cfe[cs] == ep || s.cfe[cell] == ep || s.cfe[ce] == ep;
+    }
+  return any;
+}
+
 // The end of particle i's list build, once s.nb holds its finished list
 // (cnt entries, or ovf): the particle's packed shadow record and list
-// count, and, for a non-fluid particle, its slot appended to s.wl for the
-// wall pass (k_walls).  Every active lane of the warp calls it together.
+// count, and, for a non-fluid particle that can have a fluid neighbour in
+// its boundary rows (fluid_nb), its slot appended to s.wl for the wall pass
+// (k_walls).  A non-fluid particle that cannot gets the wall pass's result
+// for an empty sum here: p = 0, rho = rho0.  Every active lane of the warp
+// calls it together.
 template <int GF, bool PRECISE>
 __device__ __forceinline__ void list_tail(const KParams& kp, const Scratch& s, const zsph_ptc_t& ptc, int i, int cnt,
-                                          bool ovf, float4 pi, float2 rp_self) {
-  const float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
-  st_rec(&s.sh.pr(i), pi, vp);
+                                          bool ovf, float4 pi, float2 rp_self, bool fluid_nb) {
+  float4 vp = make_float4(ptc.vel[3 * i], ptc.vel[3 * i + 1], ptc.vel[3 * i + 2], rp_self.y);
+  float4 pr = pi;
+  const bool nonfluid = !fluid_of(pi.w);
+  if (nonfluid && !fluid_nb) {
+    const float rsum = 0.0f;
+    pr.w = -(rsum / kp.p.cs2 + kp.p.rho0);  // still non-fluid
+    vp.w = rsum;
+  }
+  st_rec(&s.sh.pr(i), pr, vp);
   s.nb_cnt[i] = ovf ? kOverflow : (uint8_t)cnt;
   if (ovf) atomicOr(s.flags, ZSPH_FLAG_NB_OVERFLOW);  // rare: the walks re-filter this particle's rows
   const unsigned m = __activemask();
-  const bool wall = !fluid_of(pi.w);
+  const bool wall = nonfluid && fluid_nb;
   const unsigned wm = __ballot_sync(m, wall);
   if (wm) {  // one atomic per warp
     const int leader = __ffs(m) - 1;
@@ -627,7 +662,10 @@ __device__ __forceinline__ void nblist_group(const KParams& kp_arg, const Scratc
   if (cnt > 254) ovf = true;
   if (act && !ovf && (cnt & 7)) nbv[nb_vec(i, cnt >> 3)] = *reinterpret_cast<const uint4*>(ring + (cnt & (kRing - 8)));
   if (SKIN && act) s.xf.sk_cnt[i] = skovf ? kOverflow : (uint8_t)kc;
-  if (act) list_tail<GF, PRECISE>(kp, s, ptc, i, cnt, ovf, pi, rp_self);
+  if (act) {
+    const bool fluid_nb = GF != 1 || fluid_of(pi.w) || walls_fluid_near(kp, s, t, c);
+    list_tail<GF, PRECISE>(kp, s, ptc, i, cnt, ovf, pi, rp_self, fluid_nb);
+  }
 }
 
 template <int GF, int CW = kCellWarps, bool BATCH = false, bool PRECISE = false, int SEGS = kSegs,
@@ -1573,7 +1611,10 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_batch_persistent(Persist
       if (!grid_barrier(a)) return;
       for (int t = blockIdx.x * kPersistThreads + threadIdx.x; t < n; t += gridDim.x * kPersistThreads)
         rank_gather_one<false>(kp, s, a.o, a.w, a.t, t);
-      if (blockIdx.x == 0 && threadIdx.x == 0) s.misc[kMiscWalls] = 0;  // the wall list, appended by the list build
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s.misc[kMiscWalls] = 0;                // the wall list, appended by the list build
+        s.misc[kMiscFluidEpoch] = s.misc[6];   // the cell stamps rank_gather_one wrote
+      }
       if (!grid_barrier(a)) return;
       for (int g = blockIdx.x * kPersistWarps + wid; g < groups; g += gridDim.x * kPersistWarps)
         nblist_group<1, kPersistWarps, true, false>(kp, s, a.w, a.t, g, wid);
@@ -1958,7 +1999,7 @@ __global__ void __launch_bounds__(kXferThreads) k_nblist_xfer(KParams kp, Scratc
   so.nb_cnt = s.xf.nb_cnt2;
   const float2 rp = reinterpret_cast<const float2*>(cur.rhop)[i];
   const float4 pc = make_float4(cur.pos[3 * i], cur.pos[3 * i + 1], cur.pos[3 * i + 2], packed_rho(rp.x, cur.type[i]));
-  list_tail<1, false>(kp, so, cur, i, ovf ? 0 : cnt, ovf, pc, rp);
+  list_tail<1, false>(kp, so, cur, i, ovf ? 0 : cnt, ovf, pc, rp, true);  // every wall to the wall pass
 }
 
 }  // namespace

@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratc
                                                               zsph_tmp_t t) {
   pdl_wait();
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot == 0) sc.misc[kMiscFluidEpoch] = sc.misc[6];  // this search's cell stamps are valid
   if (slot >= kp.n) return;
   rank_gather_one(kp, sc, o, w, t, slot);
 }
@@ -268,6 +269,7 @@ __global__ void __launch_bounds__(kSearchBlock) k_rank_values(KParams kp, Scratc
 __global__ void __launch_bounds__(kSearchBlock) k_gather_by_index(KParams kp, Scratch sc, zsph_ptc_t o,
                                                                   zsph_ptc_t w, zsph_tmp_t t) {
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+  if (slot == 0) sc.misc[kMiscFluidEpoch] = 0;  // no cell stamps for this sort: the wall pass takes every wall
   if (slot >= kp.n) return;
   gather_one(o, w, t.index[slot], slot);
 }

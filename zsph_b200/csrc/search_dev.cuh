@@ -515,6 +515,7 @@ __device__ __forceinline__ void rank_gather_one(const KParams& kp, const Scratch
   const int dst = ranked_slot<NC>(sc, slot, i, c);
   t.index[dst] = i;
   t.hash[dst] = c;
+  if (r.type == 1) sc.cfe[c] = sc.misc[6];  // a fluid particle in cell c in this search
   store_rec(w, r, i, dst);
   if (kp.c3o) kp.c3n[dst] = cpk;
 }

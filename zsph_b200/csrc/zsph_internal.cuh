@@ -192,6 +192,7 @@ inline bool ptc_aligned8(const zsph_ptc_t& p) {
 
 constexpr int kMiscWords = 16;  // Scratch::misc
 constexpr int kMiscWalls = 8;   // misc word holding the wall list's length
+constexpr int kMiscFluidEpoch = 9;  // misc word: the search epoch whose cfe stamps are valid (0: none)
 
 // Programmatic dependent launch: the kernel's grid may start while the
 // previous kernel in the stream drains (a CUDA graph keeps the relation as
@@ -228,12 +229,14 @@ struct Scratch {
   int* misc;         // [kMiscWords] 0: tiles done, 1: last key, 2: count of last key, 3: big-cell list length,
                      //       4: largest key (one-pass scan), 5: one-pass scan tile counter, 6: one-pass scan epoch,
                      //       7: the fused scatter's finished-CTA counter (crowded cells),
-                     //       kMiscWalls: entries in wl (zeroed before each list build)
+                     //       kMiscWalls: entries in wl (zeroed before each list build),
+                     //       kMiscFluidEpoch: the epoch of the cfe stamps (0 after the drop-in gather)
   unsigned long long* tile_state;  // [tiles] one-pass scan: (tag << 32) | prefix value, tag from the epoch
   int* big_list;     // [kBigListCap]
   uint16_t* nb;      // [ceil(n/32)*32 * kMaxNb] neighbour lists, blocked by 32-particle groups (equations.cu)
   uint8_t* nb_cnt;   // [n] neighbour count (255 = overflow)
   int* wl;           // [n] sorted slots of the non-fluid particles, appended by the list build (unordered)
+  int* cfe;          // [G] per cell: the search epoch (misc[6]) in which the fused gather put a fluid particle there
   int* flags;        // [1]   ZSPH_FLAG_* bits
   Shadow sh;
   Xfer xf;           // list transfer scratch (null pointers when the handle has none)
