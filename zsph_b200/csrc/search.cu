@@ -45,9 +45,11 @@ __global__ void __launch_bounds__(kSearchBlock) k_hash(KParams kp_in, zsph_ptc_t
   t.index[i] = i;
 }
 
+// PLAIN: the single-scene FP32 form (no packed cells, no scene table).
+template <bool PLAIN>
 __global__ void __launch_bounds__(kSearchBlock) k_hash_count(KParams kp_in, zsph_ptc_t s, Scratch sc) {
   pdl_wait();
-  hash_count_body(kp_in, s, sc, blockIdx.x);
+  hash_count_body<PLAIN>(kp_in, s, sc, blockIdx.x);
 }
 
 // Drop-in sort_index, step 1: copy keys and carried values, count.
@@ -350,7 +352,9 @@ cudaError_t launch_search(const KParams& kp, const Scratch& s, int tiles, const 
   if (!ptc_aligned8(o) || !ptc_aligned8(w)) return cudaErrorMisalignedAddress;  // nothing launched
   // each kernel waits for its predecessor's completion first (pdl_wait), so
   // only the launches overlap the predecessors' drain
-  cudaError_t e = launch_pdl(k_hash_count, blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st, kp, o, s);
+  const bool plain = !kp.c3o && !kp.scenes;
+  cudaError_t e = launch_pdl(plain ? k_hash_count<true> : k_hash_count<false>,
+                             blocks_for(kp.n, kSearchBlock * kHashItems), kSearchBlock, 0, st, kp, o, s);
   mark(pf, "hash_count", st);
   if (!e) e = launch_pdl(k_scan_onepass, (kp.G + kOneTile - 1) / kOneTile, kSearchBlock, 0, st, kp, s, tmp);
   mark(pf, "scan", st);

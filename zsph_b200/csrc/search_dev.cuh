@@ -52,13 +52,16 @@ __device__ __forceinline__ int cell_hash(const zsph_gpu_param_t& p, float x, flo
 // hash.cu:16-23: a particle outside the grid becomes type 100 at the grid
 // origin with zero velocity and (rho0, 0); its key becomes 0.  Takes the
 // particle's position (x, y, z) or, in the precision form, its packed cell
-// (cpk), already loaded.
+// (cpk), already loaded.  PLAIN: the single-scene FP32 form (no packed
+// cells, no scene table), resolved at compile time.
+template <bool PLAIN = false>
 __device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_ptc_t& s, int i, float x, float y,
                                                 float z, int cpk, int* flags, float rc) {
   const zsph_gpu_param_t& p = kp.p;
+  const bool c3 = !PLAIN && kp.c3o;
   int h;
   bool out;
-  if (kp.c3o) {  // precision form: the cell is stored, the offset is local
+  if (c3) {  // precision form: the cell is stored, the offset is local
     const int3 c = unpack_cell(cpk);
     out = c.x >= p.grid_xdim || c.y >= p.grid_ydim || c.z >= p.grid_zdim;
     h = (c.z * p.grid_ydim + c.y) * p.grid_xdim + c.x;
@@ -70,7 +73,7 @@ __device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_pt
   }
   if (out) {
     s.type[i] = 100;
-    if (kp.c3o) {  // the grid origin: cell (0, 0, 0), offset 0
+    if (c3) {  // the grid origin: cell (0, 0, 0), offset 0
       kp.c3o[i] = 0;
       s.pos[3 * i] = 0.0f;
       s.pos[3 * i + 1] = 0.0f;
@@ -85,7 +88,7 @@ __device__ __forceinline__ int hash_and_kill_at(const KParams& kp, const zsph_pt
     s.vel[3 * i + 2] = 0.0f;
     s.rhop[2 * i] = p.rho0;
     s.rhop[2 * i + 1] = 0.0f;
-    h = kp.scenes ? p.grid_hash_min : 0;  // the scene's first cell (batched form)
+    h = !PLAIN && kp.scenes ? p.grid_hash_min : 0;  // the scene's first cell (batched form)
     atomicOr(flags, ZSPH_FLAG_KILLED);
   }
   return h;
@@ -126,7 +129,10 @@ __device__ __forceinline__ int warp_ticket(int* cnt, int key, unsigned active) {
 // (misc[6]) and an empty big-cell list (misc[3]).
 // hash_count_body is one CTA's chunk `chunk` of the particles; k_hash_count
 // runs one chunk per CTA, the batched form's persistent kernel loops over
-// chunks (every thread of the CTA takes part).
+// chunks (every thread of the CTA takes part).  PLAIN: kp_in has neither
+// packed cells nor scenes, so the per-particle parameter lookup and those
+// branches are left out at compile time (the same arithmetic).
+template <bool PLAIN = false>
 __device__ __forceinline__ void hash_count_body(const KParams& kp_in, const zsph_ptc_t& s, const Scratch& sc,
                                                 int chunk) {
   __shared__ int s_max[kSearchBlock / 32];
@@ -146,7 +152,7 @@ __device__ __forceinline__ void hash_count_body(const KParams& kp_in, const zsph
     x[k] = y[k] = z[k] = 0.0f;
     cpk[k] = 0;
     if (i < n) {
-      if (kp_in.c3o) {
+      if (!PLAIN && kp_in.c3o) {
         cpk[k] = kp_in.c3o[i];
       } else {
         x[k] = s.pos[3 * i];
@@ -163,9 +169,13 @@ __device__ __forceinline__ void hash_count_body(const KParams& kp_in, const zsph
     const int i = base + k * kSearchBlock;
     h[k] = 0;
     if (i < n) {
-      const KParams kp = kp_of_particle(kp_in, i);
-      const float rc = kp_in.scenes ? __frcp_rn(kp.p.grid_size) : rc0;  // a scene's own cell size
-      h[k] = hash_and_kill_at(kp, s, i, x[k], y[k], z[k], cpk[k], sc.flags, rc);
+      if constexpr (PLAIN) {
+        h[k] = hash_and_kill_at<true>(kp_in, s, i, x[k], y[k], z[k], 0, sc.flags, rc0);
+      } else {
+        const KParams kp = kp_of_particle(kp_in, i);
+        const float rc = kp_in.scenes ? __frcp_rn(kp.p.grid_size) : rc0;  // a scene's own cell size
+        h[k] = hash_and_kill_at(kp, s, i, x[k], y[k], z[k], cpk[k], sc.flags, rc);
+      }
       sc.key[i] = h[k];
       kmax = max(kmax, h[k]);
     }
