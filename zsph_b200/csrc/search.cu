@@ -246,9 +246,9 @@ __global__ void __launch_bounds__(1024) k_sort_big_cells(KParams kp, Scratch sc)
 // Fused search, last step: rank, write sorted hash/index, gather the eight
 // particle arrays (sort.cu:62-82) (rank_gather_one).  The packed records of
 // the sorted state are written by the list build, which reads each
-// particle's arrays anyway.
-__global__ void __launch_bounds__(kSearchBlock) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
-                                                              zsph_tmp_t t) {
+// particle's arrays anyway.  Eight resident CTAs (32 registers, no spills).
+__global__ void __launch_bounds__(kSearchBlock, 8) k_rank_gather(KParams kp, Scratch sc, zsph_ptc_t o, zsph_ptc_t w,
+                                                                 zsph_tmp_t t) {
   pdl_wait();
   const int slot = blockIdx.x * blockDim.x + threadIdx.x;
   if (slot == 0) sc.misc[kMiscFluidEpoch] = sc.misc[6];  // this search's cell stamps are valid

@@ -484,15 +484,19 @@ struct PtcRec {
   int type, table;
 };
 
-__device__ __forceinline__ void load_rec(const zsph_ptc_t& o, int src, PtcRec& r) {
+// The record in two halves: the current state (pos, vel, rhop, type,
+// table) and the predictor's copies (tmp_pos, tmp_vel, tmp_rhop).
+__device__ __forceinline__ void load_rec_state(const zsph_ptc_t& o, int src, PtcRec& r) {
   r.x = o.pos[3 * src]; r.y = o.pos[3 * src + 1]; r.z = o.pos[3 * src + 2];
   r.vx = o.vel[3 * src]; r.vy = o.vel[3 * src + 1]; r.vz = o.vel[3 * src + 2];
   r.rp = reinterpret_cast<const float2*>(o.rhop)[src];
+  r.type = o.type[src];
+  r.table = o.table[src];
+}
+__device__ __forceinline__ void load_rec_tmp(const zsph_ptc_t& o, int src, PtcRec& r) {
   r.tx = o.tmp_pos[3 * src]; r.ty = o.tmp_pos[3 * src + 1]; r.tz = o.tmp_pos[3 * src + 2];
   r.ux = o.tmp_vel[3 * src]; r.uy = o.tmp_vel[3 * src + 1]; r.uz = o.tmp_vel[3 * src + 2];
   r.trp = reinterpret_cast<const float2*>(o.tmp_rhop)[src];
-  r.type = o.type[src];
-  r.table = o.table[src];
 }
 
 __device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const PtcRec& r, int src, int dst) {
@@ -508,10 +512,14 @@ __device__ __forceinline__ void store_rec(const zsph_ptc_t& w, const PtcRec& r, 
 
 
 // Fused search, last step: rank, write sorted hash/index, gather the eight
-// particle arrays (sort.cu:62-82).  The source record's
-// loads are issued as soon as the source is known, before the rank (which
-// needs the key, the cell's range and its members) is counted, so they
-// overlap that dependent chain.
+// particle arrays (sort.cu:62-82).  The current-state half of the source
+// record is loaded as soon as the source is known, before the rank (which
+// needs the key, the cell's range and its members) is counted, so those
+// loads overlap that dependent chain; the tmp half follows the rank.  That
+// split fits 32 registers, so k_rank_gather keeps 64 warps per SM: loading
+// the whole record first needs 40 registers (48 warps), and loading all of
+// it after the rank leaves the rank's latency exposed (both measured
+// slower).
 // rank_gather_one: sorted slot `slot`.  NC: the members of the cell are read
 // through the read-only path (only where the scatter ran in an earlier launch).
 template <bool NC = true>
@@ -519,10 +527,11 @@ __device__ __forceinline__ void rank_gather_one(const KParams& kp, const Scratch
                                                 const zsph_ptc_t& w, const zsph_tmp_t& t, int slot) {
   const int i = sc.perm[slot];
   PtcRec r;
-  load_rec(o, i, r);
+  load_rec_state(o, i, r);
   const int cpk = kp.c3o ? kp.c3o[i] : 0;
   const int c = sc.key[i];
   const int dst = ranked_slot<NC>(sc, slot, i, c);
+  load_rec_tmp(o, i, r);
   t.index[dst] = i;
   t.hash[dst] = c;
   if (r.type == 1) sc.cfe[c] = sc.misc[6];  // a fluid particle in cell c in this search
