@@ -166,6 +166,19 @@ def test_read_json_type_and_syntax_errors(tmp_path):
         z.read_json(str(tmp_path / "missing.json"))
 
 
+@pytest.mark.parametrize("value", [1e20, -3e9, float("inf")])
+def test_read_json_int_key_out_of_range_is_an_error(tmp_path, value):
+    # a number outside the int range cannot become an int key: an error code,
+    # not an undefined conversion
+    d = case_dict(cases.config0())
+    d["ptc_num"] = value
+    p = tmp_path / "input.json"
+    p.write_text(json.dumps(d))
+    with pytest.raises(z.ZsphError) as e:
+        z.read_json(str(p))
+    assert e.value.code == z.ZSPH_EIO and "ptc_num" in str(e.value)
+
+
 def test_create_rejects_bad_grid_and_factor():
     c = cases.small(0.04)
     cp, gp = z.params_from_json(c.json)

@@ -123,6 +123,59 @@ def test_reader_errors(tmp_path):
         z.read_vtk(str(tmp_path / "missing.vtk"), 3)
 
 
+def _ascii_case(n, *sections):
+    head = ["# vtk DataFile Version 3.0", "case", "ASCII", "DATASET UNSTRUCTURED_GRID",
+            f"POINTS {n} double", " ".join("0.125" for _ in range(3 * n))]
+    return "\n".join(head + list(sections)) + "\n"
+
+
+MALFORMED = {
+    # a component count of zero or a negative one
+    "zero_components": ["POINT_DATA 5", "SCALARS type int 0", "LOOKUP_TABLE default"],
+    "negative_components": ["POINT_DATA 5", "SCALARS type int -2", "LOOKUP_TABLE default", "1 1 1 1 1"],
+    # a field array with fewer tuples than points, and one of the wrong width
+    "short_field": ["POINT_DATA 5", "FIELD FieldData 1", "type 1 2 int", "1 1"],
+    "wide_field": ["POINT_DATA 5", "FIELD FieldData 1", "type 2 5 int", " ".join(["1"] * 10)],
+    # sizes far beyond the file, and negative ones
+    "huge_cells": ["CELLS 1 4000000000000", "POINT_DATA 5"],
+    "negative_cells": ["CELLS 1 -5", "POINT_DATA 5"],
+    "huge_field": ["POINT_DATA 5", "FIELD FieldData 1", "type 1 999999999999999999 int"],
+    "truncated_values": ["POINT_DATA 5", "SCALARS type int 1", "LOOKUP_TABLE default", "1 1"],
+}
+
+
+@pytest.mark.parametrize("name", sorted(MALFORMED))
+def test_malformed_files_are_errors_not_crashes(tmp_path, name):
+    # sizes and component counts come from the file: each is checked before it
+    # is used to allocate or to index, and the reader returns ZSPH_EIO
+    p = tmp_path / f"{name}.vtk"
+    p.write_text(_ascii_case(5, *MALFORMED[name]))
+    with pytest.raises(z.ZsphError) as e:
+        z.read_vtk(str(p), 5)
+    assert e.value.code == z.ZSPH_EIO
+
+
+def test_binary_block_checks(tmp_path):
+    st, acc = _state(20, 6)
+    p = str(tmp_path / "f.vtk")
+    z.write_vtk(p, st, acc=acc, flags=z.OUT_REFERENCE)
+    data = open(p, "rb").read()
+    # cut inside the last binary block
+    open(p, "wb").write(data[:-40])
+    with pytest.raises(z.ZsphError) as e:
+        z.read_vtk(p, st.n)
+    assert e.value.code == z.ZSPH_EIO
+    # a binary block of a type whose width the reader does not take
+    open(p, "wb").write(data.replace(b"SCALARS type int", b"SCALARS type unsigned_char", 1))
+    with pytest.raises(z.ZsphError) as e:
+        z.read_vtk(p, st.n)
+    assert e.value.code == z.ZSPH_EIO and "unsigned_char" in str(e.value)
+    # the untouched file still reads
+    open(p, "wb").write(data)
+    got, _ = z.read_vtk(p, st.n)
+    assert np.array_equal(got.type, st.type)
+
+
 def test_dam_break_case_round_trips_through_vtk(tmp_path):
     c = cases.small(0.04)
     p = str(tmp_path / "input.vtk")

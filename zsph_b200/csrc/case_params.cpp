@@ -140,8 +140,9 @@ void copy_str(char* dst, size_t cap, const std::string& s) {
 
 }  // namespace
 
-extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int errlen) {
-  if (!path || !out) { set_err(err, errlen, "null argument"); return ZSPH_EINVAL; }
+namespace {
+
+int read_json_file(const char* path, zsph_json_t* out, char* err, int errlen) {
   std::ifstream f(path);
   if (!f) { set_err(err, errlen, std::string("cannot open ") + path); return ZSPH_EIO; }
   std::stringstream ss;
@@ -162,7 +163,17 @@ extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int
     return true;
   };
   auto fnum = [&](const char* k, float& dst) { double v; if (num(k, v)) dst = (float)v; };
-  auto inum = [&](const char* k, int& dst) { double v; if (num(k, v)) dst = (int)v; };
+  // An int key takes any number and truncates it, as nlohmann's get<int> does;
+  // one outside the int range (where the conversion is undefined) is an error.
+  auto inum = [&](const char* k, int& dst) {
+    double v;
+    if (!num(k, v)) return;
+    if (!(v > -2147483649.0 && v < 2147483648.0)) {
+      if (missing.empty()) missing = std::string("key is out of the int range: ") + k;
+      return;
+    }
+    dst = (int)v;
+  };
   auto sval = [&](const char* k, char* dst, size_t cap) {
     auto it = kv.find(k);
     if (it == kv.end() || it->second.kind != JValue::STR) {
@@ -207,6 +218,22 @@ extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int
   if (!missing.empty()) { set_err(err, errlen, missing); return ZSPH_EIO; }
   set_err(err, errlen, "");
   return ZSPH_OK;
+}
+
+}  // namespace
+
+extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int errlen) {
+  if (!path || !out) { set_err(err, errlen, "null argument"); return ZSPH_EINVAL; }
+  // No C++ exception leaves through the C ABI: it becomes an error code.
+  try {
+    return read_json_file(path, out, err, errlen);
+  } catch (const std::exception& e) {
+    set_err(err, errlen, std::string("zsph_read_json: ") + e.what());
+    return ZSPH_EIO;
+  } catch (...) {
+    set_err(err, errlen, "zsph_read_json: unknown error");
+    return ZSPH_EIO;
+  }
 }
 
 extern "C" int zsph_check_dt(const zsph_cpu_param_t* param, float* dt_max_out) {

@@ -16,6 +16,7 @@
 //                       of spinning on an atomic flag.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cctype>
 #include <condition_variable>
 #include <cstdint>
@@ -82,21 +83,38 @@ struct Cursor {
   }
 };
 
-// Reads `count` values of `type` (float, double, int) as doubles.
-bool read_values(Cursor& c, bool binary, const std::string& type, size_t count, std::vector<double>& out) {
-  out.resize(count);
+// Bytes per value of a binary block's data type; 0 for a type this reader
+// does not take.  The reference's writer uses float, double and int.
+size_t binary_width(const std::string& type) {
+  if (type == "double") return 8;
+  if (type == "float" || type == "int") return 4;
+  return 0;
+}
+
+// Reads `count` values of `type` (float, double, int) as doubles.  The count
+// comes from the file, so it is checked against the bytes left before anything
+// is allocated: a binary block needs count * width bytes, an ASCII one at least
+// one character per value.  Returns an empty string or the reason it failed.
+std::string read_values(Cursor& c, bool binary, const std::string& type, long long count, std::vector<double>& out) {
+  if (count < 0) return "negative value count";
+  const size_t left = c.s.size() - std::min(c.p, c.s.size());
   if (!binary) {
-    for (size_t k = 0; k < count; ++k) {
+    if ((unsigned long long)count > left) return "fewer values than declared";
+    out.resize((size_t)count);
+    for (size_t k = 0; k < (size_t)count; ++k) {
       const std::string t = c.token();
-      if (t.empty()) return false;
+      if (t.empty()) return "fewer values than declared";
       out[k] = std::strtod(t.c_str(), nullptr);
     }
-    return true;
+    return "";
   }
+  const size_t w = binary_width(type);
+  if (w == 0) return "unsupported binary data type \"" + type + "\"";
   c.skip_line_end();
-  const size_t w = (type == "double") ? 8 : 4;
-  if (c.p + count * w > c.s.size()) return false;
-  for (size_t k = 0; k < count; ++k) {
+  const size_t avail = c.s.size() - c.p;
+  if ((unsigned long long)count > avail / w) return "fewer bytes than declared";
+  out.resize((size_t)count);
+  for (size_t k = 0; k < (size_t)count; ++k) {
     const char* q = c.s.data() + c.p + k * w;
     if (w == 8) {
       uint64_t u;
@@ -120,8 +138,17 @@ bool read_values(Cursor& c, bool binary, const std::string& type, size_t count, 
       }
     }
   }
-  c.p += count * w;
-  return true;
+  c.p += (size_t)count * w;
+  return "";
+}
+
+// A count or component number from the file's text; -1 when it is not a
+// plain non-negative decimal number.
+long long parse_count(const std::string& t) {
+  if (t.empty() || t.size() > 18) return -1;
+  for (char ch : t)
+    if (ch < '0' || ch > '9') return -1;
+  return std::strtoll(t.c_str(), nullptr, 10);
 }
 
 struct Array {
@@ -130,65 +157,7 @@ struct Array {
   std::vector<double> v;
 };
 
-}  // namespace
-
-extern "C" {
-
-int zsph_write_vtk(const char* path, int n, const float* pos, const float* vel, const float* rhop, const int* type,
-                   const float* acc, const int* hash, const int* table, int flags) {
-  if (!path || n < 0 || (n > 0 && !pos)) return fail(ZSPH_EINVAL, "zsph_write_vtk: bad argument");
-  std::string out;
-  out.reserve((size_t)n * 48 + 512);
-  std::ostringstream hdr;
-  hdr << "# vtk DataFile Version 3.0\nzsph data\nBINARY\nDATASET UNSTRUCTURED_GRID\n";  // write_vtk.cu:36-39
-  hdr << "POINTS " << n << " float\n";
-  out += hdr.str();
-  put_be(out, pos, (size_t)n * 3);
-  out += "\nPOINT_DATA " + std::to_string(n) + "\n";
-  auto scalar_f = [&](const char* name, const float* base, int stride) {
-    out += std::string("SCALARS ") + name + " float 1\nLOOKUP_TABLE default\n";
-    const size_t at = out.size();
-    out.resize(at + (size_t)n * 4);
-    for (int i = 0; i < n; ++i) {
-      uint32_t u;
-      std::memcpy(&u, &base[(size_t)i * stride], 4);
-      u = bswap32(u);
-      std::memcpy(&out[at + 4 * (size_t)i], &u, 4);
-    }
-    out += "\n";
-  };
-  auto scalar_i = [&](const char* name, const int* v) {
-    out += std::string("SCALARS ") + name + " int 1\nLOOKUP_TABLE default\n";
-    put_be(out, v, (size_t)n);
-    out += "\n";
-  };
-  auto vector_f = [&](const char* name, const float* base, int stride) {
-    out += std::string("VECTORS ") + name + " float\n";
-    const size_t at = out.size();
-    out.resize(at + (size_t)n * 12);
-    for (int i = 0; i < n; ++i)
-      for (int k = 0; k < 3; ++k) {
-        uint32_t u;
-        std::memcpy(&u, &base[(size_t)i * stride + k], 4);
-        u = bswap32(u);
-        std::memcpy(&out[at + 12 * (size_t)i + 4 * k], &u, 4);
-      }
-    out += "\n";
-  };
-  if ((flags & ZSPH_OUT_RHO) && rhop) scalar_f("rho", rhop, 2);
-  if ((flags & ZSPH_OUT_P) && rhop) scalar_f("p", rhop + 1, 2);           // write_vtk.cu:66-74
-  if ((flags & ZSPH_OUT_TYPE) && type) scalar_i("type", type);            // :76-84
-  if ((flags & ZSPH_OUT_HASH) && hash) scalar_i("hash", hash);            // :86-94
-  if ((flags & ZSPH_OUT_TABLE) && table) scalar_i("table", table);
-  if ((flags & ZSPH_OUT_VEL) && vel) vector_f("vel", vel, 3);             // :106-116
-  if ((flags & ZSPH_OUT_ACC) && acc) vector_f("acc", acc, 4);             // :118-128
-  std::ofstream f(path, std::ios::binary);
-  if (!f) return fail(ZSPH_EIO, std::string("zsph_write_vtk: cannot open ") + path);
-  f.write(out.data(), (std::streamsize)out.size());
-  return f ? ZSPH_OK : fail(ZSPH_EIO, std::string("zsph_write_vtk: write failed: ") + path);
-}
-
-int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* pos, float* vel, float* rhop,
+int read_vtk_file(const char* path, int n, float rho0, int accept_float, float* pos, float* vel, float* rhop,
                   float* acc, int* type, int* table) {
   if (!path || n < 0) return fail(ZSPH_EINVAL, "zsph_read_vtk: bad argument");
   std::ifstream f(path, std::ios::binary);
@@ -204,58 +173,69 @@ int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* 
   if (!binary && fmt != "ASCII") return fail(ZSPH_EIO, "zsph_read_vtk: format must be ASCII or BINARY");
   std::vector<double> pts;
   std::vector<std::pair<std::string, Array>> arrays;
-  long npts = -1;
+  long long npts = -1;
+  auto values = [&](const std::string& what, const std::string& ty, long long count, std::vector<double>& out) {
+    const std::string why = read_values(c, binary, ty, count, out);
+    return why.empty() ? ZSPH_OK : fail(ZSPH_EIO, "zsph_read_vtk: " + what + ": " + why);
+  };
   for (;;) {
     const std::string kw = c.token();
     if (kw.empty()) break;
+    int rc = ZSPH_OK;
     if (kw == "DATASET") {
       if (c.token() != "UNSTRUCTURED_GRID") return fail(ZSPH_EIO, "zsph_read_vtk: dataset must be UNSTRUCTURED_GRID");
     } else if (kw == "POINTS") {
-      npts = std::strtol(c.token().c_str(), nullptr, 10);
+      const std::string cnt = c.token();
+      npts = parse_count(cnt);
       const std::string ty = c.token();
       if (npts != n)  // read_vkt.cu:14 asserts this
-        return fail(ZSPH_EINVAL, "zsph_read_vtk: file has " + std::to_string(npts) + " points, ptc_num is " +
-                                     std::to_string(n));
-      if (!read_values(c, binary, ty, (size_t)npts * 3, pts)) return fail(ZSPH_EIO, "zsph_read_vtk: short POINTS");
+        return fail(ZSPH_EINVAL, "zsph_read_vtk: file has " + cnt + " points, ptc_num is " + std::to_string(n));
+      rc = values("POINTS", ty, npts * 3, pts);
     } else if (kw == "CELLS" || kw == "CELL_TYPES") {
-      const long a = std::strtol(c.token().c_str(), nullptr, 10);
-      long cnt = a;
-      if (kw == "CELLS") cnt = std::strtol(c.token().c_str(), nullptr, 10);
+      long long cnt = parse_count(c.token());
+      if (kw == "CELLS") cnt = parse_count(c.token());
+      if (cnt < 0) return fail(ZSPH_EIO, "zsph_read_vtk: bad " + kw + " size");
       std::vector<double> skip;
-      if (!read_values(c, binary, "int", (size_t)cnt, skip)) return fail(ZSPH_EIO, "zsph_read_vtk: short " + kw);
+      rc = values(kw, "int", cnt, skip);
     } else if (kw == "POINT_DATA" || kw == "CELL_DATA") {
       c.token();
     } else if (kw == "SCALARS") {
       Array a;
       const std::string name = c.token();
       a.type = c.token();
-      // optional component count, then LOOKUP_TABLE
+      // optional component count (1 to 4), then LOOKUP_TABLE
       std::string t = c.token();
       if (t != "LOOKUP_TABLE") {
-        a.comps = std::atoi(t.c_str());
+        const long long comps = parse_count(t);
+        if (comps < 1 || comps > 4) return fail(ZSPH_EIO, "zsph_read_vtk: SCALARS " + name + ": bad component count " + t);
+        a.comps = (int)comps;
         t = c.token();
       }
       c.token();  // table name
-      if (!read_values(c, binary, a.type, (size_t)n * a.comps, a.v)) return fail(ZSPH_EIO, "zsph_read_vtk: short " + name);
+      rc = values("SCALARS " + name, a.type, (long long)n * a.comps, a.v);
       arrays.emplace_back(name, std::move(a));
     } else if (kw == "VECTORS") {
       Array a;
       const std::string name = c.token();
       a.type = c.token();
       a.comps = 3;
-      if (!read_values(c, binary, a.type, (size_t)n * 3, a.v)) return fail(ZSPH_EIO, "zsph_read_vtk: short " + name);
+      rc = values("VECTORS " + name, a.type, (long long)n * 3, a.v);
       arrays.emplace_back(name, std::move(a));
     } else if (kw == "FIELD") {
       c.token();
-      const int narr = std::atoi(c.token().c_str());
-      for (int k = 0; k < narr; ++k) {
+      const long long narr = parse_count(c.token());
+      if (narr < 0) return fail(ZSPH_EIO, "zsph_read_vtk: bad FIELD array count");
+      for (long long k = 0; k < narr && rc == ZSPH_OK; ++k) {
         Array a;
         const std::string name = c.token();
-        a.comps = std::atoi(c.token().c_str());
-        const long tuples = std::strtol(c.token().c_str(), nullptr, 10);
+        const long long comps = parse_count(c.token());
+        const long long tuples = parse_count(c.token());
         a.type = c.token();
-        if (!read_values(c, binary, a.type, (size_t)tuples * a.comps, a.v))
-          return fail(ZSPH_EIO, "zsph_read_vtk: short field " + name);
+        if (comps < 1 || comps > 16 || tuples < 0)
+          return fail(ZSPH_EIO, "zsph_read_vtk: field " + name + ": bad component or tuple count");
+        if (tuples > (1LL << 40)) return fail(ZSPH_EIO, "zsph_read_vtk: field " + name + ": fewer values than declared");
+        a.comps = (int)comps;
+        rc = values("field " + name, a.type, tuples * comps, a.v);
         arrays.emplace_back(name, std::move(a));
       }
     } else if (kw == "LOOKUP_TABLE" || kw == "METADATA") {
@@ -263,26 +243,40 @@ int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* 
     } else {
       return fail(ZSPH_EIO, "zsph_read_vtk: unexpected keyword " + kw);
     }
+    if (rc != ZSPH_OK) return rc;
   }
   if (npts < 0) return fail(ZSPH_EIO, "zsph_read_vtk: no POINTS");
   // read_vkt.cu:61-83: p, vel, acc, rho must be double arrays (a float array is
-  // ignored and the default used) unless accept_float; type and table int arrays
-  auto find = [&](const char* name, bool want_int) -> const Array* {
+  // ignored and the default used) unless accept_float; type and table int
+  // arrays.  An array that is taken must hold one tuple of the expected width
+  // per point (1 for p, rho, type, table; 3 for vel, acc): a shorter or wider
+  // one is an error rather than a read past its end.
+  std::string bad;
+  auto find = [&](const char* name, bool want_int, int comps) -> const Array* {
     for (auto& kv : arrays)
       if (kv.first == name) {
-        const std::string& t = kv.second.type;
-        if (want_int) return (t == "int") ? &kv.second : nullptr;
-        if (t == "double" || (accept_float && t == "float")) return &kv.second;
-        return nullptr;
+        const Array& arr = kv.second;
+        const std::string& t = arr.type;
+        const bool taken = want_int ? (t == "int") : (t == "double" || (accept_float && t == "float"));
+        if (!taken) return nullptr;
+        if (arr.comps != comps || arr.v.size() != (size_t)n * (size_t)comps) {
+          if (bad.empty())
+            bad = std::string("zsph_read_vtk: array \"") + name + "\" holds " + std::to_string(arr.v.size()) +
+                  " values in tuples of " + std::to_string(arr.comps) + "; expected " + std::to_string(n) +
+                  " tuples of " + std::to_string(comps);
+          return nullptr;
+        }
+        return &arr;
       }
     return nullptr;
   };
-  const Array* ap = find("p", false);
-  const Array* ar = find("rho", false);
-  const Array* av = find("vel", false);
-  const Array* aa = find("acc", false);
-  const Array* at = find("type", true);
-  const Array* ab = find("table", true);
+  const Array* ap = find("p", false, 1);
+  const Array* ar = find("rho", false, 1);
+  const Array* av = find("vel", false, 3);
+  const Array* aa = find("acc", false, 3);
+  const Array* at = find("type", true, 1);
+  const Array* ab = find("table", true, 1);
+  if (!bad.empty()) return fail(ZSPH_EIO, bad);
   if (!at) return fail(ZSPH_EIO, "zsph_read_vtk: the int array \"type\" is required");  // read_vkt.cu:101
   for (int i = 0; i < n; ++i) {  // read_vkt.cu:85-126
     for (int k = 0; k < 3; ++k) {
@@ -299,6 +293,85 @@ int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* 
     if (table) table[i] = ab ? (int)ab->v[i] : 0;
   }
   return ZSPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zsph_write_vtk(const char* path, int n, const float* pos, const float* vel, const float* rhop, const int* type,
+                   const float* acc, const int* hash, const int* table, int flags) {
+  if (!path || n < 0 || (n > 0 && !pos)) return fail(ZSPH_EINVAL, "zsph_write_vtk: bad argument");
+  // No C++ exception leaves through the C ABI (a std::bad_alloc for a very
+  // large n, for example): it becomes an error code.
+  try {
+    std::string out;
+    out.reserve((size_t)n * 48 + 512);
+    std::ostringstream hdr;
+    hdr << "# vtk DataFile Version 3.0\nzsph data\nBINARY\nDATASET UNSTRUCTURED_GRID\n";  // write_vtk.cu:36-39
+    hdr << "POINTS " << n << " float\n";
+    out += hdr.str();
+    put_be(out, pos, (size_t)n * 3);
+    out += "\nPOINT_DATA " + std::to_string(n) + "\n";
+    auto scalar_f = [&](const char* name, const float* base, int stride) {
+      out += std::string("SCALARS ") + name + " float 1\nLOOKUP_TABLE default\n";
+      const size_t at = out.size();
+      out.resize(at + (size_t)n * 4);
+      for (int i = 0; i < n; ++i) {
+        uint32_t u;
+        std::memcpy(&u, &base[(size_t)i * stride], 4);
+        u = bswap32(u);
+        std::memcpy(&out[at + 4 * (size_t)i], &u, 4);
+      }
+      out += "\n";
+    };
+    auto scalar_i = [&](const char* name, const int* v) {
+      out += std::string("SCALARS ") + name + " int 1\nLOOKUP_TABLE default\n";
+      put_be(out, v, (size_t)n);
+      out += "\n";
+    };
+    auto vector_f = [&](const char* name, const float* base, int stride) {
+      out += std::string("VECTORS ") + name + " float\n";
+      const size_t at = out.size();
+      out.resize(at + (size_t)n * 12);
+      for (int i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+          uint32_t u;
+          std::memcpy(&u, &base[(size_t)i * stride + k], 4);
+          u = bswap32(u);
+          std::memcpy(&out[at + 12 * (size_t)i + 4 * k], &u, 4);
+        }
+      out += "\n";
+    };
+    if ((flags & ZSPH_OUT_RHO) && rhop) scalar_f("rho", rhop, 2);
+    if ((flags & ZSPH_OUT_P) && rhop) scalar_f("p", rhop + 1, 2);           // write_vtk.cu:66-74
+    if ((flags & ZSPH_OUT_TYPE) && type) scalar_i("type", type);            // :76-84
+    if ((flags & ZSPH_OUT_HASH) && hash) scalar_i("hash", hash);            // :86-94
+    if ((flags & ZSPH_OUT_TABLE) && table) scalar_i("table", table);
+    if ((flags & ZSPH_OUT_VEL) && vel) vector_f("vel", vel, 3);             // :106-116
+    if ((flags & ZSPH_OUT_ACC) && acc) vector_f("acc", acc, 4);             // :118-128
+    std::ofstream f(path, std::ios::binary);
+    if (!f) return fail(ZSPH_EIO, std::string("zsph_write_vtk: cannot open ") + path);
+    f.write(out.data(), (std::streamsize)out.size());
+    return f ? ZSPH_OK : fail(ZSPH_EIO, std::string("zsph_write_vtk: write failed: ") + path);
+  } catch (const std::exception& e) {
+    return fail(ZSPH_EIO, std::string("zsph_write_vtk: ") + e.what());
+  } catch (...) {
+    return fail(ZSPH_EIO, "zsph_write_vtk: unknown error");
+  }
+}
+
+int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* pos, float* vel, float* rhop,
+                  float* acc, int* type, int* table) {
+  // A malformed file must come back as an error code, never as a C++
+  // exception through the C ABI (a std::bad_alloc, for example).
+  try {
+    return read_vtk_file(path, n, rho0, accept_float, pos, vel, rhop, acc, type, table);
+  } catch (const std::exception& e) {
+    return fail(ZSPH_EIO, std::string("zsph_read_vtk: ") + e.what());
+  } catch (...) {
+    return fail(ZSPH_EIO, "zsph_read_vtk: unknown error");
+  }
 }
 
 }  // extern "C"
