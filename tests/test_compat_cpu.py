@@ -57,3 +57,14 @@ def test_missing_input_vtk_is_reported_before_any_step(tmp_path):
         rc, steps = _run(path, mode)
         assert rc != z.ZSPH_OK and steps == 0
         assert "read_vtk" in z.last_error()
+
+
+def test_negative_particle_count_is_rejected(tmp_path):
+    path = _case_json_without_input(str(tmp_path))
+    with open(path) as f:
+        j = json.load(f)
+    j["ptc_num"] = -1
+    with open(path, "w") as f:
+        json.dump(j, f)
+    assert _run(path, z.COMPAT_FUSED) == (z.ZSPH_EINVAL, 0)
+    assert "negative ptc_num" in z.last_error()

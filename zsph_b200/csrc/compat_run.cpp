@@ -37,13 +37,7 @@ std::string last_error(zsph_handle_t* h) {
   return b;
 }
 
-}  // namespace
-
-extern "C" {
-
-int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
-  if (steps_done) *steps_done = 0;
-  if (!json_path) return fail(ZSPH_EINVAL, "null json path");
+int compat_run(const char* json_path, int mode, int* steps_done) {
   const bool simple = (mode & ZSPH_COMPAT_SIMPLE) != 0;
   mode &= ~ZSPH_COMPAT_SIMPLE;
   if (mode != ZSPH_COMPAT_SEPARATE && mode != ZSPH_COMPAT_FUSED) return fail(ZSPH_EINVAL, "unknown mode");
@@ -55,6 +49,7 @@ int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
   rc = zsph_set_cpu_param(&cp, &j);
   if (rc) return fail(rc, "set_cpu_param: " + last_error(nullptr));
   const int n = cp.ptc_num;
+  if (n < 0) return fail(ZSPH_EINVAL, "negative ptc_num in the case file");
   std::vector<float> pos(3 * (size_t)n), vel(3 * (size_t)n), rhop(2 * (size_t)n), acc(4 * (size_t)n);
   std::vector<int> type((size_t)n), table((size_t)n);
   const std::string input = std::string(cp.input_path) + "/input.vtk";
@@ -143,6 +138,24 @@ int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
   zsph_free_tmp(&t);
   if (steps_done) *steps_done = done;
   return rc ? fail(rc, what) : ZSPH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
+  if (steps_done) *steps_done = 0;
+  if (!json_path) return fail(ZSPH_EINVAL, "null json path");
+  // No C++ exception leaves through the C ABI (a std::bad_alloc for the host
+  // copies of a very large case, for example): it becomes an error code.
+  try {
+    return compat_run(json_path, mode, steps_done);
+  } catch (const std::exception& e) {
+    return fail(ZSPH_EIO, e.what());
+  } catch (...) {
+    return fail(ZSPH_EIO, "unknown error");
+  }
 }
 
 }  // extern "C"
