@@ -430,11 +430,17 @@ extern "C" {
 int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthreads, zsph_writer_t** out) {
   if (!output_path || ptc_num < 0 || nthreads < 1 || !out) return fail(ZSPH_EINVAL, "zsph_writer_create: bad argument");
   *out = nullptr;
-  auto* w = new zsph_writer();
-  w->out_dir = output_path;
-  w->n = ptc_num;
-  w->flags = flags;
-  w->slots.resize((size_t)nthreads);
+  zsph_writer* w = nullptr;
+  try {  // host allocation failures become a status code, not an exception through the C ABI
+    w = new zsph_writer();
+    w->out_dir = output_path;
+    w->n = ptc_num;
+    w->flags = flags;
+    w->slots.resize((size_t)nthreads);
+  } catch (const std::exception& ex) {
+    delete w;
+    return fail(ZSPH_EIO, std::string("zsph_writer_create: ") + ex.what());
+  }
   const size_t N = (size_t)(ptc_num ? ptc_num : 1);
   cudaError_t e = cudaSuccess;
   for (auto& s : w->slots) {
@@ -451,7 +457,12 @@ int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthr
     zsph_writer_destroy(w);
     return fail(ZSPH_ECUDA, std::string("zsph_writer_create: ") + cudaGetErrorString(e));
   }
-  for (int t = 0; t < nthreads; ++t) w->threads.emplace_back([w] { w->run(); });
+  try {
+    for (int t = 0; t < nthreads; ++t) w->threads.emplace_back([w] { w->run(); });
+  } catch (const std::exception& ex) {  // a thread that could not start: stop and join the others
+    zsph_writer_destroy(w);
+    return fail(ZSPH_EIO, std::string("zsph_writer_create: cannot start a writer thread: ") + ex.what());
+  }
   *out = w;
   return ZSPH_OK;
 }
