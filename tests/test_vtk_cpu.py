@@ -176,6 +176,29 @@ def test_binary_block_checks(tmp_path):
     assert np.array_equal(got.type, st.type)
 
 
+def test_field_arrays_with_metadata_blocks(tmp_path):
+    # point arrays as FIELD data, each followed by the METADATA block that
+    # VTK's own legacy writer emits (component names, information keys),
+    # which ends at an empty line
+    n = 4
+    lines = ["# vtk DataFile Version 5.1", "vtk output", "ASCII", "DATASET UNSTRUCTURED_GRID",
+             f"POINTS {n} double", " ".join(str(0.5 * i) for i in range(3 * n)),
+             f"POINT_DATA {n}", "FIELD FieldData 3",
+             f"type 1 {n} int", " ".join(str(i % 2) for i in range(n)),
+             "METADATA", "INFORMATION 0", "",
+             f"vel 3 {n} double", " ".join(str(0.25 * i) for i in range(3 * n)),
+             "METADATA", "COMPONENT_NAMES", "X", "Y", "Z", "INFORMATION 1",
+             "NAME L2_NORM_RANGE LOCATION vtkDataArray", "DATA 2 0 2.75", "",
+             f"p 1 {n} double", " ".join(str(10.0 * i) for i in range(n))]
+    p = tmp_path / "g.vtk"
+    p.write_text("\n".join(lines) + "\n")
+    got, _ = z.read_vtk(str(p), n, rho0=1000.0)
+    assert np.array_equal(got.type, [i % 2 for i in range(n)])
+    assert np.allclose(got.vel.ravel(), [0.25 * i for i in range(3 * n)])
+    assert np.allclose(got.rhop[:, 1], [10.0 * i for i in range(n)])
+    assert np.allclose(got.pos.ravel(), [0.5 * i for i in range(3 * n)])
+
+
 def test_dam_break_case_round_trips_through_vtk(tmp_path):
     c = cases.small(0.04)
     p = str(tmp_path / "input.vtk")

@@ -178,6 +178,16 @@ int read_vtk_file(const char* path, int n, float rho0, int accept_float, float* 
     const std::string why = read_values(c, binary, ty, count, out);
     return why.empty() ? ZSPH_OK : fail(ZSPH_EIO, "zsph_read_vtk: " + what + ": " + why);
   };
+  // VTK's own legacy writer follows an array with a METADATA block
+  // (COMPONENT_NAMES, INFORMATION n and its entries) that ends at an empty
+  // line, between the arrays of a FIELD too: skipped whole.
+  auto skip_metadata = [&] {
+    c.line();
+    while (c.p < c.s.size()) {
+      const std::string l = c.line();
+      if (l.find_first_not_of(" \t") == std::string::npos) break;
+    }
+  };
   for (;;) {
     const std::string kw = c.token();
     if (kw.empty()) break;
@@ -227,7 +237,11 @@ int read_vtk_file(const char* path, int n, float rho0, int accept_float, float* 
       if (narr < 0) return fail(ZSPH_EIO, "zsph_read_vtk: bad FIELD array count");
       for (long long k = 0; k < narr && rc == ZSPH_OK; ++k) {
         Array a;
-        const std::string name = c.token();
+        std::string name = c.token();
+        while (name == "METADATA") {
+          skip_metadata();
+          name = c.token();
+        }
         const long long comps = parse_count(c.token());
         const long long tuples = parse_count(c.token());
         a.type = c.token();
@@ -238,8 +252,10 @@ int read_vtk_file(const char* path, int n, float rho0, int accept_float, float* 
         rc = values("field " + name, a.type, tuples * comps, a.v);
         arrays.emplace_back(name, std::move(a));
       }
-    } else if (kw == "LOOKUP_TABLE" || kw == "METADATA") {
+    } else if (kw == "LOOKUP_TABLE") {
       c.line();
+    } else if (kw == "METADATA") {
+      skip_metadata();
     } else {
       return fail(ZSPH_EIO, "zsph_read_vtk: unexpected keyword " + kw);
     }
