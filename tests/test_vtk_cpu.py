@@ -199,6 +199,39 @@ def test_field_arrays_with_metadata_blocks(tmp_path):
     assert np.allclose(got.pos.ravel(), [0.5 * i for i in range(3 * n)])
 
 
+@pytest.mark.parametrize("binary", [False, True])
+def test_version_5_1_cells_are_read_past(tmp_path, binary):
+    # version 5.1 files (VTK 9's legacy writer) give CELLS as OFFSETS and
+    # CONNECTIVITY blocks with their own data types; here one vertex cell per
+    # point, offsets in 64-bit and connectivity in 32-bit ints
+    n = 3
+    pos = (np.arange(3 * n) / 4).astype(">f4")
+    types = np.array([1, 0, 1], ">i4")
+    offsets = np.arange(n + 1, dtype=">i8")
+    conn = np.arange(n, dtype=">i4")
+    ctypes_ = np.full(n, 1, ">i4")
+    if binary:
+        blob = (b"# vtk DataFile Version 5.1\nvtk output\nBINARY\nDATASET UNSTRUCTURED_GRID\n"
+                + f"POINTS {n} float\n".encode() + pos.tobytes()
+                + f"\nCELLS {n + 1} {n}\nOFFSETS vtktypeint64\n".encode() + offsets.tobytes()
+                + b"\nCONNECTIVITY vtktypeint32\n" + conn.tobytes()
+                + f"\nCELL_TYPES {n}\n".encode() + ctypes_.tobytes()
+                + f"\nPOINT_DATA {n}\nSCALARS type int 1\nLOOKUP_TABLE default\n".encode() + types.tobytes() + b"\n")
+    else:
+        lines = ["# vtk DataFile Version 5.1", "vtk output", "ASCII", "DATASET UNSTRUCTURED_GRID",
+                 f"POINTS {n} float", " ".join(repr(float(v)) for v in pos),
+                 f"CELLS {n + 1} {n}", "OFFSETS vtktypeint64", " ".join(map(str, offsets)),
+                 "CONNECTIVITY vtktypeint64", " ".join(map(str, conn)),
+                 f"CELL_TYPES {n}", " ".join(map(str, ctypes_)),
+                 f"POINT_DATA {n}", "SCALARS type int 1", "LOOKUP_TABLE default", " ".join(map(str, types))]
+        blob = ("\n".join(lines) + "\n").encode()
+    p = tmp_path / "h.vtk"
+    p.write_bytes(blob)
+    got, _ = z.read_vtk(str(p), n)
+    assert np.array_equal(got.pos.ravel(), pos.astype(np.float32))
+    assert np.array_equal(got.type, types)
+
+
 def test_dam_break_case_round_trips_through_vtk(tmp_path):
     c = cases.small(0.04)
     p = str(tmp_path / "input.vtk")

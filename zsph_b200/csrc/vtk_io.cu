@@ -86,8 +86,8 @@ struct Cursor {
 // Bytes per value of a binary block's data type; 0 for a type this reader
 // does not take.  The reference's writer uses float, double and int.
 size_t binary_width(const std::string& type) {
-  if (type == "double") return 8;
-  if (type == "float" || type == "int") return 4;
+  if (type == "double" || type == "vtktypeint64") return 8;
+  if (type == "float" || type == "int" || type == "vtktypeint32") return 4;
   return 0;
 }
 
@@ -120,9 +120,15 @@ std::string read_values(Cursor& c, bool binary, const std::string& type, long lo
       uint64_t u;
       std::memcpy(&u, q, 8);
       u = bswap64(u);
-      double d;
-      std::memcpy(&d, &u, 8);
-      out[k] = d;
+      if (type == "double") {
+        double d;
+        std::memcpy(&d, &u, 8);
+        out[k] = d;
+      } else {
+        int64_t i;
+        std::memcpy(&i, &u, 8);
+        out[k] = (double)i;
+      }
     } else {
       uint32_t u;
       std::memcpy(&u, q, 4);
@@ -202,11 +208,23 @@ int read_vtk_file(const char* path, int n, float rho0, int accept_float, float* 
         return fail(ZSPH_EINVAL, "zsph_read_vtk: file has " + cnt + " points, ptc_num is " + std::to_string(n));
       rc = values("POINTS", ty, npts * 3, pts);
     } else if (kw == "CELLS" || kw == "CELL_TYPES") {
-      long long cnt = parse_count(c.token());
-      if (kw == "CELLS") cnt = parse_count(c.token());
-      if (cnt < 0) return fail(ZSPH_EIO, "zsph_read_vtk: bad " + kw + " size");
+      // The cells are read past, not kept.  Version 5.1 files give CELLS as
+      // an OFFSETS and a CONNECTIVITY block, each with its own data type;
+      // older ones as one int block.
+      const long long a = parse_count(c.token());
+      const long long b = kw == "CELLS" ? parse_count(c.token()) : a;
+      if (a < 0 || b < 0) return fail(ZSPH_EIO, "zsph_read_vtk: bad " + kw + " size");
       std::vector<double> skip;
-      rc = values(kw, "int", cnt, skip);
+      const size_t at = c.p;
+      if (kw == "CELLS" && c.token() == "OFFSETS") {
+        rc = values("CELLS offsets", c.token(), a, skip);
+        if (rc == ZSPH_OK && c.token() != "CONNECTIVITY")
+          return fail(ZSPH_EIO, "zsph_read_vtk: CELLS: CONNECTIVITY expected after OFFSETS");
+        if (rc == ZSPH_OK) rc = values("CELLS connectivity", c.token(), b, skip);
+      } else {
+        c.p = at;
+        rc = values(kw, "int", b, skip);
+      }
     } else if (kw == "POINT_DATA" || kw == "CELL_DATA") {
       c.token();
     } else if (kw == "SCALARS") {
