@@ -491,21 +491,44 @@ __global__ void k_pack_rows(const float* rows, int n, PackArgs pa, unsigned char
       make_uint4(u[0], u[1], u[2], u[3]);
 }
 
-int g_sms = 0;
-std::once_flag g_init;
-cudaError_t g_init_err = cudaSuccess;
+// The kernels' dynamic shared-memory opt-in and the SM count belong to one
+// device context: they are set up on the first launch in each context of
+// each device (the current one), and again after the context changes
+// (cudaDeviceReset, for example).  A process may use several devices.
+constexpr int kMaxDevices = 64;
+struct DevInit {
+  unsigned long long ctx = 0;  // current_context_id() when set up
+  int sms = 0;
+  bool done = false;
+};
+std::mutex g_init_mu;
+DevInit g_init[kMaxDevices];
 
-cudaError_t init_mlp_kernels() {
-  std::call_once(g_init, [] {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (!e) e = cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+// Sets up the current device's context if needed; *sms receives its SM count.
+cudaError_t init_mlp_kernels(int* sms) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_init_mu);
+  DevInit& d = g_init[dev];
+  const unsigned long long ctx = current_context_id();
+  if (!d.done || ctx == 0 || ctx != d.ctx) {
+    int n = 0;
+    e = cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     if (!e) e = cudaFuncSetAttribute(k_mlp<kPredict>, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem<kPredict>::ALLOC);
     if (!e) e = cudaFuncSetAttribute(k_mlp<kCorrect>, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem<kCorrect>::ALLOC);
     if (!e) e = cudaFuncSetAttribute(k_mlp<kTrain>, cudaFuncAttributeMaxDynamicSharedMemorySize, Smem<kTrain>::ALLOC);
-    g_init_err = e;
-  });
-  return g_init_err;
+    if (e) {
+      d.done = false;
+      return e;
+    }
+    d.sms = n;
+    d.ctx = current_context_id();
+    d.done = true;
+  }
+  *sms = d.sms;
+  return cudaSuccess;
 }
 
 int fail(int code, const std::string& msg) {
@@ -532,7 +555,8 @@ __nv_bfloat16* bf(void* p) { return static_cast<__nv_bfloat16*>(p); }
 namespace zsph {
 
 int mlp_sm_count() {
-  return init_mlp_kernels() ? 0 : g_sms;
+  int sms = 0;
+  return init_mlp_kernels(&sms) ? 0 : sms;
 }
 
 Net mlp_net(const Mlp& m) {
@@ -542,7 +566,8 @@ Net mlp_net(const Mlp& m) {
 // learned-corrector epilogue over the state after the predictor (learn.cu)
 cudaError_t launch_mlp_correct(const Mlp& m, const KParams& kp, const void* tiles, const zsph_ptc_t& ptc,
                                float4* acc, const float4* dprev, float4 oa, float4 ob, int* flags, cudaStream_t st) {
-  cudaError_t e = init_mlp_kernels();
+  int sms = 0;
+  cudaError_t e = init_mlp_kernels(&sms);
   if (e) return e;
   MlpArgs a{};
   a.net = mlp_net(m);
@@ -556,14 +581,15 @@ cudaError_t launch_mlp_correct(const Mlp& m, const KParams& kp, const void* tile
   a.dprev = dprev;
   a.oa = oa;
   a.ob = ob;
-  const int grid = std::min(a.ntiles, 2 * g_sms);
+  const int grid = std::min(a.ntiles, 2 * sms);
   k_mlp<kCorrect><<<grid, 128, Smem<kCorrect>::ALLOC, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_forward(const Mlp& m, const void* tiles, int n, float* out, int* flags,
                                cudaStream_t st) {
-  cudaError_t e = init_mlp_kernels();
+  int sms = 0;
+  cudaError_t e = init_mlp_kernels(&sms);
   if (e) return e;
   MlpArgs a{};
   a.net = mlp_net(m);
@@ -572,14 +598,15 @@ cudaError_t launch_mlp_forward(const Mlp& m, const void* tiles, int n, float* ou
   a.nrows = n;
   a.out = reinterpret_cast<float4*>(out);
   a.flags = flags;
-  const int grid = std::min(a.ntiles, 2 * g_sms);
+  const int grid = std::min(a.ntiles, 2 * sms);
   if (grid > 0) k_mlp<kPredict><<<grid, 128, Smem<kPredict>::ALLOC, st>>>(a);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mlp_grad(const Mlp& m, const void* tiles, const float* y, const float* w, const int* ids,
                             int ntiles, float inv_wsum, float* partial, int* nparts, int* flags, cudaStream_t st) {
-  cudaError_t e = init_mlp_kernels();
+  int sms = 0;
+  cudaError_t e = init_mlp_kernels(&sms);
   if (e) return e;
   MlpArgs a{};
   a.net = mlp_net(m);
@@ -591,7 +618,7 @@ cudaError_t launch_mlp_grad(const Mlp& m, const void* tiles, const float* y, con
   a.inv_wsum = inv_wsum;
   a.partial = partial;
   a.flags = flags;
-  const int grid = std::max(1, std::min(ntiles, g_sms));
+  const int grid = std::max(1, std::min(ntiles, sms));
   k_mlp<kTrain><<<grid, 128, Smem<kTrain>::ALLOC, st>>>(a);
   *nparts = grid;
   return cudaGetLastError();

@@ -35,8 +35,6 @@
 // call's contents.  Each call clears the parts that must start at zero.  Calls
 // whose work overlaps on the GPU (different streams, or different host
 // threads) race on the array and must be serialised by the caller.
-#include <cuda.h>  // CUcontext / CUresult types only; the entry points come from the runtime
-
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -76,36 +74,6 @@ static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocBytes];
 std::mutex g_mu;
 unsigned char* g_base[kMaxDevices] = {};
 unsigned long long g_ctx[kMaxDevices] = {};  // id of the context g_base[dev] was looked up in
-
-using PfnCtxGetCurrent = CUresult (*)(CUcontext*);
-using PfnCtxGetId = CUresult (*)(CUcontext, unsigned long long*);
-PfnCtxGetCurrent g_ctx_get_current = nullptr;
-PfnCtxGetId g_ctx_get_id = nullptr;
-std::once_flag g_entry_once;
-
-// Unique id of the calling thread's current context (never reused within a
-// process), or 0 when there is none yet or the driver does not offer it; with
-// 0 the caller looks the symbol address up again on every call.
-unsigned long long current_context_id() {
-  std::call_once(g_entry_once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      g_ctx_get_current = reinterpret_cast<PfnCtxGetCurrent>(p);
-    p = nullptr;
-    q = cudaDriverEntryPointSymbolNotFound;
-    if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      g_ctx_get_id = reinterpret_cast<PfnCtxGetId>(p);
-  });
-  if (!g_ctx_get_current || !g_ctx_get_id) return 0;
-  CUcontext c = nullptr;
-  if (g_ctx_get_current(&c) != CUDA_SUCCESS || !c) return 0;
-  unsigned long long id = 0;
-  if (g_ctx_get_id(c, &id) != CUDA_SUCCESS) return 0;
-  return id;
-}
 
 // errors are reported through zsph_last_error(NULL, ...)
 int fail(int code, const std::string& m) {

@@ -355,6 +355,12 @@ int mlp_sm_count();
 
 // api.cu: message returned by zsph_last_error(NULL, ...)
 void record_library_error(const std::string& msg);
+// Unique id of the calling thread's current CUDA context (never reused within
+// a process), or 0 when there is none yet or the driver does not offer it
+// (device_context.cu).  Host state that belongs to one context is kept per
+// device with this id and set up again when it differs; with 0 it is set up
+// again on every call.
+unsigned long long current_context_id();
 
 // search.cu
 cudaError_t launch_hash(const KParams& kp, int* flags, const zsph_ptc_t& ptc, const zsph_tmp_t& tmp, cudaStream_t st);
