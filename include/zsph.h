@@ -297,6 +297,36 @@ int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthr
 int zsph_writer_submit(zsph_writer_t* w, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int step, void* stream);
 int zsph_writer_destroy(zsph_writer_t* w);
 
+/* ---- checkpoint and resume ------------------------------------------------- */
+
+/* No counterpart in the reference, whose only resume state is the case
+ * file's start_step/current_step (single_gpu_sph_src/io/read_json.cu:32-35)
+ * with an input.vtk that its own output cannot replace (io/write_vtk.cu:56-128
+ * writes float arrays and no rho; io/read_vkt.cu:27-39 takes double arrays).
+ * A snapshot file holds the non-null arrays of one particle buffer set and of
+ * tmp, bit for bit, with the step number and a checksum per array (host byte
+ * order).  Saving needs pos, vel, rhop, type, table, grid_start and grid_end
+ * (the cell bounds, whose entries from earlier searches can survive a search);
+ * null optional arrays are left out.  Loading needs a file of the same
+ * ptc_num and grid_num (else ZSPH_EINVAL), checks every array's size and
+ * checksum before it writes anything (ZSPH_EIO on a damaged, truncated or
+ * foreign file), fills every non-null destination array (ZSPH_EIO if the file
+ * lacks one) and returns the saved step in *step.  Buffers loaded from a
+ * snapshot of old_ and tmp step on exactly as the saved run does, in the plain
+ * and simple equation forms; the precision form's integer cells, a learned
+ * corrector's previous values and rigid bodies are held by the handle and are
+ * not saved.  zsph_snapshot_save/_load copy device buffers through `stream`
+ * and synchronise it; the _host forms take the same structs holding host
+ * pointers.  Errors: zsph_last_error(NULL, ...). */
+int zsph_snapshot_save(const char* path, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int ptc_num, int grid_num,
+                       int step, void* stream);
+int zsph_snapshot_load(const char* path, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int ptc_num, int grid_num,
+                       int* step, void* stream);
+int zsph_snapshot_save_host(const char* path, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int ptc_num,
+                            int grid_num, int step);
+int zsph_snapshot_load_host(const char* path, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int ptc_num,
+                            int grid_num, int* step);
+
 /* ---- the reference's driver program ---------------------------------------- */
 
 /* single_gpu_sph_src/deltasph/main.cu:8-147 on this library: reads the case

@@ -256,6 +256,10 @@ _sig = {
                                      ctypes.POINTER(ctypes.c_longlong)]),
     "zsph_persistent_info": (_I, [_HP, _IP, _IP]),
     "zsph_persistent_barrier_test": (_I, [_HP, _I, _VP]),
+    "zsph_snapshot_save": (_I, [ctypes.c_char_p, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _I, _VP]),
+    "zsph_snapshot_load": (_I, [ctypes.c_char_p, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _IP, _VP]),
+    "zsph_snapshot_save_host": (_I, [ctypes.c_char_p, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _I]),
+    "zsph_snapshot_load_host": (_I, [ctypes.c_char_p, ctypes.POINTER(Ptc), ctypes.POINTER(Tmp), _I, _I, _IP]),
 }
 
 OUT_P, OUT_TYPE, OUT_VEL, OUT_ACC, OUT_RHO, OUT_HASH, OUT_TABLE = 1, 2, 4, 8, 16, 32, 64
@@ -279,6 +283,53 @@ def read_vtk(path: str, n: int, rho0: float = 1000.0, accept_float: bool = False
     check(lib.zsph_read_vtk(path.encode(), n, float(rho0), 1 if accept_float else 0, _ptr(st.pos), _ptr(st.vel),
                             _ptr(st.rhop), _ptr(acc), _ptr(st.type), _ptr(st.table)))
     return st, acc
+SNAPSHOT_PTC = {"pos": (3, np.float32), "vel": (3, np.float32), "rhop": (2, np.float32),
+                "tmp_pos": (3, np.float32), "tmp_vel": (3, np.float32), "tmp_rhop": (2, np.float32),
+                "type": (1, np.int32), "table": (1, np.int32)}
+SNAPSHOT_TMP = {"acc_drhodt": (4, np.float32), "dofv_grandrho": (4, np.float32), "dofv": (1, np.float32),
+                "index": (1, np.int32), "hash": (1, np.int32), "grid_start": (1, np.int32),
+                "grid_end": (1, np.int32)}
+
+
+def _host_structs(arrays: dict):
+    """Ptc/Tmp structs pointing at the host arrays of `arrays` (absent: NULL)."""
+    p, t = Ptc(), Tmp()
+    for k in SNAPSHOT_PTC:
+        if arrays.get(k) is not None:
+            setattr(p, k, arrays[k].ctypes.data)
+    for k in SNAPSHOT_TMP:
+        if arrays.get(k) is not None:
+            setattr(t, k, arrays[k].ctypes.data)
+    return p, t
+
+
+def snapshot_save_host(path: str, arrays: dict, n: int, grid_num: int, step: int = 0) -> None:
+    """zsph_snapshot_save_host of host arrays keyed by their zsph_ptc_t /
+    zsph_tmp_t member names (missing keys are NULL arrays)."""
+    arrays = {k: np.ascontiguousarray(v, dtype={**SNAPSHOT_PTC, **SNAPSHOT_TMP}[k][1])
+              for k, v in arrays.items() if v is not None}
+    p, t = _host_structs(arrays)
+    check(lib.zsph_snapshot_save_host(path.encode(), ctypes.byref(p), ctypes.byref(t), int(n), int(grid_num),
+                                      int(step)))
+
+
+def snapshot_load_host(path: str, n: int, grid_num: int, names=None) -> tuple[dict, int]:
+    """zsph_snapshot_load_host into fresh host arrays for `names` (default:
+    every array); returns (arrays, step)."""
+    spec = {**SNAPSHOT_PTC, **SNAPSHOT_TMP}
+    names = list(spec) if names is None else list(names)
+    out = {}
+    for k in names:
+        w, dt = spec[k]
+        rows = grid_num if k in ("grid_start", "grid_end") else n
+        out[k] = np.empty((rows, w) if w > 1 else rows, dt)
+    p, t = _host_structs(out)
+    step = ctypes.c_int(-1)
+    check(lib.zsph_snapshot_load_host(path.encode(), ctypes.byref(p), ctypes.byref(t), int(n), int(grid_num),
+                                      ctypes.byref(step)))
+    return out, step.value
+
+
 def last_error(handle=None) -> str:
     buf = ctypes.create_string_buffer(1024)
     lib.zsph_last_error(handle, buf, len(buf))
@@ -478,6 +529,18 @@ class Solver:
         for k, v in arrays.items():
             dt = np.int32 if k in ("index", "hash", "grid_start", "grid_end") else np.float32
             self.copy_to_device(getattr(self.tmp, k), np.ascontiguousarray(v, dtype=dt))
+
+    def save_snapshot(self, path: str, step: int = 0, which: str = "old", stream=None) -> None:
+        """zsph_snapshot_save of one buffer set and tmp (checkpoint)."""
+        check(lib.zsph_snapshot_save(path.encode(), ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), self.n,
+                                     self.G, int(step), stream))
+
+    def load_snapshot(self, path: str, which: str = "old", stream=None) -> int:
+        """zsph_snapshot_load into one buffer set and tmp (resume); returns the saved step."""
+        step = ctypes.c_int(-1)
+        check(lib.zsph_snapshot_load(path.encode(), ctypes.byref(self._buf(which)), ctypes.byref(self.tmp), self.n,
+                                     self.G, ctypes.byref(step), stream))
+        return step.value
 
     # -- entry points ----------------------------------------------------
     def _call(self, fn, *args):
