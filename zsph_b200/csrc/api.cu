@@ -20,6 +20,7 @@
 #include <string>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 using namespace zsph;
@@ -226,9 +227,19 @@ cudaError_t xfer_step(zsph_handle* h, const zsph_ptc_t& o, const zsph_ptc_t& w, 
 // governing + integration of `to` written into `from`.
 cudaError_t substep(zsph_handle* h, const zsph_ptc_t& from, const zsph_ptc_t& to, const zsph_tmp_t& t, int mode,
                     cudaStream_t st, Prof* pf, const FeatOut* feat = nullptr) {
-  cudaError_t e = launch_search(h->kp, h->s, h->tiles, from, to, t, st, pf);
-  if (!e) e = launch_boundary(h->kp, h->s, to, t, st, pf);
-  if (!e) e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf, feat);
+  cudaError_t e;
+  {
+    const TraceRange r("search");
+    e = launch_search(h->kp, h->s, h->tiles, from, to, t, st, pf);
+  }
+  if (!e) {
+    const TraceRange r("boundary");
+    e = launch_boundary(h->kp, h->s, to, t, st, pf);
+  }
+  if (!e) {
+    const TraceRange r("governing");
+    e = launch_governing(h->kp, h->s, to, t, mode, from, st, pf, feat);
+  }
   if (!e && h->rigid && mode != 0) e = rigid_substep(h, from, to, t, mode, st);
   return e;
 }
@@ -526,6 +537,7 @@ int zsph_set_equations(zsph_handle_t* h, int equations) {
 }
 
 #define ENTRY_CHECKS(h)                                         \
+  const zsph::TraceRange trace_range_(__func__);               \
   if (!h) return set_err(nullptr, ZSPH_EINVAL, "null handle"); \
   if (int rc_ = check_device(h)) return rc_;
 

@@ -20,6 +20,7 @@
 #include <string>
 
 #include "../../include/zsph.h"
+#include "trace.h"
 
 namespace {
 
@@ -223,6 +224,7 @@ int read_json_file(const char* path, zsph_json_t* out, char* err, int errlen) {
 }  // namespace
 
 extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int errlen) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!path || !out) { set_err(err, errlen, "null argument"); return ZSPH_EINVAL; }
   // No C++ exception leaves through the C ABI: it becomes an error code.
   try {

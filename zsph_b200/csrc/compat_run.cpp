@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 namespace {
@@ -145,6 +146,7 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
 extern "C" {
 
 int zsph_compat_run(const char* json_path, int mode, int* steps_done) {
+  const zsph::TraceRange trace_range_(__func__);
   if (steps_done) *steps_done = 0;
   if (!json_path) return fail(ZSPH_EINVAL, "null json path");
   // No C++ exception leaves through the C ABI (a std::bad_alloc for the host

@@ -25,6 +25,7 @@
 #include <string>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 namespace zsph {
@@ -318,6 +319,7 @@ int zsph_learn_feature_scales(zsph_handle_t* h, float* scale) {
 
 int zsph_learn_features(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* t,
                         float* features, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (int rc = check_buffers(h, o, w, t, "zsph_learn_features")) return rc;
   if (!features) return set_herr(h, ZSPH_EINVAL, "zsph_learn_features: null features");
   if (reinterpret_cast<uintptr_t>(features) & 15)
@@ -336,6 +338,7 @@ int zsph_learn_features(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t*
 
 int zsph_learn_collect(zsph_handle_t* h, const zsph_ptc_t* o, const zsph_ptc_t* w, const zsph_tmp_t* t, int nsteps,
                        int every, int capacity, int* count, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (int rc = check_buffers(h, o, w, t, "zsph_learn_collect")) return rc;
   if (nsteps < 0 || every <= 0 || capacity <= 0)
     return set_herr(h, ZSPH_EINVAL, "zsph_learn_collect: nsteps >= 0, every > 0 and capacity > 0 required");
@@ -410,6 +413,7 @@ int zsph_learn_clear(zsph_handle_t* h) {
 
 int zsph_learn_train(zsph_handle_t* h, zsph_mlp_t* net, int epochs, int batch_tiles, float lr,
                      unsigned long long seed, float val_frac, zsph_learn_train_stats_t* out, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!h || !net) return set_herr(h, ZSPH_EINVAL, "zsph_learn_train: null argument");
   LearnState* L = h->learn;
   if (!L || L->count < 2) return set_herr(h, ZSPH_EINVAL, "zsph_learn_train: collect at least 2 snapshots first");
@@ -603,6 +607,7 @@ int zsph_run_learned(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, con
 int zsph_run_learned_ex(zsph_handle_t* h, zsph_mlp_t* net, const zsph_ptc_t* o, const zsph_ptc_t* w,
                         const zsph_tmp_t* t, int nsteps, int judge_every, float tol, int corrector,
                         float* err_series, int series_cap, zsph_learn_run_stats_t* out, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (int rc = check_buffers(h, o, w, t, "zsph_run_learned")) return rc;
   const bool network = corrector == ZSPH_CORR_NETWORK;
   if (corrector < ZSPH_CORR_NETWORK || corrector > ZSPH_CORR_REUSE_FRESH)

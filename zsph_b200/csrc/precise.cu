@@ -37,6 +37,7 @@
 #include <string>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 namespace zsph {
@@ -427,6 +428,7 @@ int zsph_set_precision(zsph_handle_t* h, int on) {
 }
 
 int zsph_precise_load(zsph_handle_t* h, const zsph_ptc_t* old_, const double* pos, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!h || !old_ || !pos) return set_herr(h, ZSPH_EINVAL, "zsph_precise_load: null argument");
   if (!h->kp.c3o) return set_herr(h, ZSPH_EINVAL, "zsph_precise_load: precision form is off");
   const int n = h->kp.n;
@@ -469,6 +471,7 @@ int zsph_precise_positions(zsph_handle_t* h, const zsph_ptc_t* old_, double* pos
 }
 
 int zsph_conservation(zsph_handle_t* h, const zsph_ptc_t* old_, zsph_conservation_t* out, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!h || !old_ || !out) return set_herr(h, ZSPH_EINVAL, "zsph_conservation: null argument");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* d = nullptr;
@@ -510,6 +513,7 @@ int zsph_conservation(zsph_handle_t* h, const zsph_ptc_t* old_, zsph_conservatio
 }
 
 int zsph_rigid_attach(zsph_handle_t* h, const zsph_ptc_t* old_, const zsph_rigid_t* body, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!h || !old_ || !body) return set_herr(h, ZSPH_EINVAL, "zsph_rigid_attach: null argument");
   if (body->count <= 0 || body->first < 0 || !(body->mass > 0))
     return set_herr(h, ZSPH_EINVAL, "zsph_rigid_attach: count > 0, first >= 0 and mass > 0 required");

@@ -32,6 +32,7 @@
 #include <string>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 namespace {
@@ -227,6 +228,7 @@ int load(const char* who, const char* path, const zsph_ptc_t* ptc, const zsph_tm
 // No C++ exception (a failed host allocation, for example) leaves through the C ABI.
 template <class F>
 int guarded(const char* who, F&& f) {
+  const zsph::TraceRange trace_range(who);
   try {
     return f();
   } catch (const std::exception& e) {

@@ -31,6 +31,7 @@
 #include <thread>
 #include <vector>
 
+#include "trace.h"
 #include "zsph_internal.cuh"
 
 namespace {
@@ -335,6 +336,7 @@ extern "C" {
 
 int zsph_write_vtk(const char* path, int n, const float* pos, const float* vel, const float* rhop, const int* type,
                    const float* acc, const int* hash, const int* table, int flags) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!path || n < 0 || (n > 0 && !pos)) return fail(ZSPH_EINVAL, "zsph_write_vtk: bad argument");
   // No C++ exception leaves through the C ABI (a std::bad_alloc for a very
   // large n, for example): it becomes an error code.
@@ -397,6 +399,7 @@ int zsph_write_vtk(const char* path, int n, const float* pos, const float* vel, 
 
 int zsph_read_vtk(const char* path, int n, float rho0, int accept_float, float* pos, float* vel, float* rhop,
                   float* acc, int* type, int* table) {
+  const zsph::TraceRange trace_range_(__func__);
   // A malformed file must come back as an error code, never as a C++
   // exception through the C ABI (a std::bad_alloc, for example).
   try {
@@ -502,6 +505,7 @@ int zsph_writer_create(const char* output_path, int ptc_num, int flags, int nthr
 }
 
 int zsph_writer_submit(zsph_writer_t* w, const zsph_ptc_t* ptc, const zsph_tmp_t* tmp, int step, void* stream) {
+  const zsph::TraceRange trace_range_(__func__);
   if (!w || !ptc || !tmp) return fail(ZSPH_EINVAL, "zsph_writer_submit: bad argument");
   int k = -1;
   {
