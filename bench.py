@@ -283,6 +283,17 @@ def cpu_baseline(case, target_s: float) -> dict:
                       f"{dt:.1f} s)"}
 
 
+def guarded_leg(name, fn):
+    """Runs one secondary leg; an exception becomes {"error": ...} in its
+    key (and a note on stderr) instead of ending the run."""
+    try:
+        return fn()
+    except Exception as e:  # noqa: BLE001 - the headline line must still be printed
+        msg = f"{type(e).__name__}: {e}"[:400]
+        print(f"bench: the {name} leg failed: {msg}", file=sys.stderr, flush=True)
+        return {"error": msg}
+
+
 # ---------------------------------------------------------------- learned form
 GROWTH_STEPS = 2000
 
@@ -549,12 +560,15 @@ def run_ours(args, dist: Dist):
                    "read of the 4-byte device status word), zsph_gpu_to_cpu of pos/vel/rhop/type/table; "
                    "host wall clock, max over ranks"}
 
-    learned = None if args.no_learned else learned_leg(args, dist, sol, stream, sptr, n, ms / K)
-    batched = None if args.no_batched else batched_leg(args, dist, stream, sptr)
+    # the other forms' legs and the CPU baseline come after the headline measurement: a failure in one of
+    # them is reported in its key and the line is still printed
+    learned = None if args.no_learned else guarded_leg(
+        "learned", lambda: learned_leg(args, dist, sol, stream, sptr, n, ms / K))
+    batched = None if args.no_batched else guarded_leg("batched", lambda: batched_leg(args, dist, stream, sptr))
 
     cpu = None
     if dist.rank == 0 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(case, args.cpu_seconds)
+        cpu = guarded_leg("cpu_baseline", lambda: cpu_baseline(case, args.cpu_seconds))
 
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": dist.world,

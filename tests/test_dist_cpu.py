@@ -70,3 +70,16 @@ def test_failed_rank_does_not_hang_the_other(tmp_path, monkeypatch):
     outs = _launch(tmp_path, {"FAIL_RANK": "1", "ZSPH_PG_TIMEOUT": "20"}, timeout=300)
     assert outs[1][0] == 3
     assert outs[0][0] != 0
+
+
+def test_a_failing_secondary_leg_is_reported_not_fatal(capsys):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    def boom():
+        raise RuntimeError("leg exploded")
+
+    assert bench.guarded_leg("learned", lambda: {"value": 1.0}) == {"value": 1.0}
+    r = bench.guarded_leg("learned", boom)
+    assert r == {"error": "RuntimeError: leg exploded"}
+    assert "the learned leg failed" in capsys.readouterr().err
