@@ -140,3 +140,19 @@ def test_empty_particle_set(tmp_path):
     z.snapshot_save_host(p, a, 0, 5, step=1)
     b, step = z.snapshot_load_host(p, 0, 5)
     assert step == 1 and all(_same_bits(a[k], b[k]) for k in a)
+
+
+def test_a_failed_save_leaves_the_earlier_snapshot(tmp_path):
+    a = _arrays(9)
+    p = str(tmp_path / "s.zsnap")
+    z.snapshot_save_host(p, a, N, G, step=10)
+    os.mkdir(p + ".part")  # the temporary file of the next save cannot be created
+    with pytest.raises(z.ZsphError) as e:
+        z.snapshot_save_host(p, _arrays(10), N, G, step=20)
+    assert e.value.code == z.ZSPH_EIO
+    b, step = z.snapshot_load_host(p, N, G)
+    assert step == 10 and all(_same_bits(a[k], b[k]) for k in a)
+    os.rmdir(p + ".part")
+    z.snapshot_save_host(p, _arrays(10), N, G, step=20)  # and a later save replaces it whole
+    assert z.snapshot_load_host(p, N, G)[1] == 20
+    assert not os.path.exists(p + ".part")

@@ -122,9 +122,24 @@ int save(const char* who, const char* path, const zsph_ptc_t* ptc, const zsph_tm
     if (s.ptr) used.push_back(s);
     else if (s.required) return fail(ZSPH_EINVAL, std::string(who) + ": array " + s.name + " is null");
   }
+  // written under a temporary name and renamed at the end, so that a failed
+  // save never replaces an earlier good snapshot at `path`
+  const std::string part = std::string(path) + ".part";
   File out;
-  out.f = std::fopen(path, "wb");
-  if (!out.f) return fail(ZSPH_EIO, std::string(who) + ": cannot open " + path);
+  out.f = std::fopen(part.c_str(), "wb");
+  if (!out.f) return fail(ZSPH_EIO, std::string(who) + ": cannot open " + part);
+  struct Cleanup {
+    File& f;
+    const std::string& name;
+    bool keep = false;
+    ~Cleanup() {
+      if (!keep) {
+        if (f.f) std::fclose(f.f);
+        f.f = nullptr;
+        std::remove(name.c_str());
+      }
+    }
+  } cleanup{out, part};
   FileHeader fh{};
   std::memcpy(fh.magic, kMagic, 8);
   fh.version = kVersion;
@@ -159,7 +174,11 @@ int save(const char* who, const char* path, const zsph_ptc_t* ptc, const zsph_tm
         std::fseek(out.f, 0, SEEK_END) != 0)
       return fail(ZSPH_EIO, std::string(who) + ": write failed");
   }
-  if (std::fflush(out.f) != 0) return fail(ZSPH_EIO, std::string(who) + ": write failed");
+  const int closed = std::fclose(out.f);
+  out.f = nullptr;
+  if (closed != 0) return fail(ZSPH_EIO, std::string(who) + ": write failed");
+  if (std::rename(part.c_str(), path) != 0) return fail(ZSPH_EIO, std::string(who) + ": cannot rename to " + path);
+  cleanup.keep = true;
   return ZSPH_OK;
 }
 
