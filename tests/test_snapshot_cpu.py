@@ -156,3 +156,29 @@ def test_a_failed_save_leaves_the_earlier_snapshot(tmp_path):
     z.snapshot_save_host(p, _arrays(10), N, G, step=20)  # and a later save replaces it whole
     assert z.snapshot_load_host(p, N, G)[1] == 20
     assert not os.path.exists(p + ".part")
+
+
+def test_resume_on_the_oracle_is_bit_exact(tmp_path):
+    # the reference's step semantics (the FP32 oracle): the state a step
+    # carries over is old_ plus the cell bounds, so 3 steps, a snapshot
+    # through the file and 3 more steps from a fresh run equal 6 steps
+    from oracle import pyoracle as po
+    from zsph_b200 import cases
+    c = cases.small(0.04)
+    a = po.Oracle(c.json, c.state, np.float32)
+    a.step(3)
+    p = str(tmp_path / "oracle.zsnap")
+    n, G = a.p.ptc_num, a.p.grid_num
+    z.snapshot_save_host(p, {**a.old, **a.tmp}, n, G, step=3)
+    a.step(3)
+    b = po.Oracle(c.json, c.state, np.float32)
+    loaded, step = z.snapshot_load_host(p, n, G, names=list(b.old) + list(b.tmp))
+    assert step == 3
+    for d in (b.old, b.tmp):
+        for k in d:
+            d[k][...] = loaded[k]  # in place: the oracle holds pointers to these arrays
+    b.step(3)
+    for k in ("pos", "vel", "rhop", "type", "table"):
+        assert _same_bits(a.old[k], b.old[k]), k
+    for k in ("hash", "index", "grid_start", "grid_end", "acc_drhodt"):
+        assert _same_bits(a.tmp[k], b.tmp[k]), k
