@@ -68,3 +68,10 @@ def test_negative_particle_count_is_rejected(tmp_path):
         json.dump(j, f)
     assert _run(path, z.COMPAT_FUSED) == (z.ZSPH_EINVAL, 0)
     assert "negative ptc_num" in z.last_error()
+
+
+def test_an_unwritable_metrics_log_is_reported_before_any_step(tmp_path, monkeypatch):
+    path = _case_json_without_input(str(tmp_path))
+    monkeypatch.setenv("ZSPH_METRICS", str(tmp_path / "no_such_dir" / "metrics.jsonl"))
+    assert _run(path, z.COMPAT_FUSED) == (z.ZSPH_EIO, 0)
+    assert "metrics log" in z.last_error()

@@ -74,3 +74,20 @@ def test_compat_run_reports_a_missing_input(tmp_path):
     os.remove(os.path.join(str(tmp_path), "input", "input.vtk"))
     with pytest.raises(z.ZsphError):
         z.compat_run(path)
+
+
+def test_compat_run_metrics_log(tmp_path, monkeypatch):
+    # ZSPH_METRICS: one JSON line per output step with the steps since the
+    # previous line, their wall time and the FP64 conservation sums
+    c = cases.small(0.04)
+    path, out = _write_case(str(tmp_path), c, 12, 5)
+    log = tmp_path / "metrics.jsonl"
+    monkeypatch.setenv("ZSPH_METRICS", str(log))
+    assert z.compat_run(path, z.COMPAT_FUSED) == 12
+    lines = [json.loads(l) for l in log.read_text().splitlines()]
+    assert [l["step"] for l in lines] == [0, 5, 10]
+    assert [l["steps"] for l in lines] == [1, 5, 5]
+    assert all(l["seconds"] > 0 and l["particle_steps_per_s"] > 0 and (l["flags"] & z.FLAG_NAN) == 0 for l in lines)
+    mass = c.n_fluid * float(c.json.rho0) * float(c.json.dx) ** 3
+    assert all(abs(l["mass"] - mass) < 1e-6 * mass for l in lines)  # no fluid particle leaves the tank
+    assert sorted(os.listdir(out)) == sorted(f"zsph{i}.vtk" for i in (0, 5, 10))

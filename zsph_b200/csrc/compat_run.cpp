@@ -18,7 +18,10 @@
 // ZSPH_* status with its message in zsph_last_error(NULL, ...).
 #include <cuda_runtime.h>
 
+#include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -38,6 +41,64 @@ std::string last_error(zsph_handle_t* h) {
   return b;
 }
 
+// The run log the reference prints to stdout as per-step timings
+// (deltasph/main.cu:60-95), as JSON lines in the file that the environment
+// variable ZSPH_METRICS names (no log without it): at every output step, the
+// steps and wall time since the previous line (the stream synchronised first,
+// so the time covers the device work), particle-steps/s, the device status
+// bits and the FP64 conservation sums of the state (zsph_conservation).
+struct MetricsLog {
+  std::FILE* f = nullptr;
+  std::chrono::steady_clock::time_point t0;
+  int steps = 0;
+  ~MetricsLog() {
+    if (f) std::fclose(f);
+  }
+  void start() { t0 = std::chrono::steady_clock::now(); }
+  int line(zsph_handle_t* h, const zsph_ptc_t& o, int step, int n, cudaStream_t st, std::string& what) {
+    cudaError_t ce = cudaStreamSynchronize(st);
+    if (ce) {
+      what = std::string("metrics: ") + cudaGetErrorString(ce);
+      return ZSPH_ECUDA;
+    }
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    zsph_conservation_t c{};
+    int rc = zsph_conservation(h, &o, &c, st);
+    if (rc) {
+      what = "metrics: " + last_error(h);
+      return rc;
+    }
+    int flags = 0;
+    rc = zsph_status(h, &flags, 0);
+    if (rc == ZSPH_ECUDA) {
+      what = "metrics: " + last_error(h);
+      return rc;
+    }
+    // a non-finite sum (a state that blew up) is written as null, so every line stays JSON
+    auto num = [](double x) {
+      char b[32];
+      if (!std::isfinite(x)) return std::string("null");
+      std::snprintf(b, sizeof b, "%.17g", x);
+      return std::string(b);
+    };
+    std::fprintf(f,
+                 "{\"step\": %d, \"steps\": %d, \"seconds\": %.6f, \"particle_steps_per_s\": %.6e, "
+                 "\"flags\": %d, \"mass\": %s, \"volume\": %s, \"momentum\": [%s, %s, %s], "
+                 "\"kinetic\": %s, \"potential\": %s, \"internal\": %s}\n",
+                 step, steps, dt, dt > 0 ? (double)n * steps / dt : 0.0, flags, num(c.mass).c_str(),
+                 num(c.volume).c_str(), num(c.momentum[0]).c_str(), num(c.momentum[1]).c_str(),
+                 num(c.momentum[2]).c_str(), num(c.kinetic).c_str(), num(c.potential).c_str(),
+                 num(c.internal).c_str());
+    if (std::fflush(f) != 0) {
+      what = "metrics: write failed";
+      return ZSPH_EIO;
+    }
+    steps = 0;
+    start();
+    return ZSPH_OK;
+  }
+};
+
 int compat_run(const char* json_path, int mode, int* steps_done) {
   const bool simple = (mode & ZSPH_COMPAT_SIMPLE) != 0;
   mode &= ~ZSPH_COMPAT_SIMPLE;
@@ -51,6 +112,12 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
   if (rc) return fail(rc, "set_cpu_param: " + last_error(nullptr));
   const int n = cp.ptc_num;
   if (n < 0) return fail(ZSPH_EINVAL, "negative ptc_num in the case file");
+  MetricsLog metrics;
+  const char* mpath = std::getenv("ZSPH_METRICS");
+  if (mpath && *mpath) {
+    metrics.f = std::fopen(mpath, "w");
+    if (!metrics.f) return fail(ZSPH_EIO, std::string("cannot open the metrics log ") + mpath);
+  }
   std::vector<float> pos(3 * (size_t)n), vel(3 * (size_t)n), rhop(2 * (size_t)n), acc(4 * (size_t)n);
   std::vector<int> type((size_t)n), table((size_t)n);
   const std::string input = std::string(cp.input_path) + "/input.vtk";
@@ -93,6 +160,7 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
     if (rc) what = "writer: " + last_error(nullptr);
   }
   void* s = st;
+  metrics.start();
   for (int i = cp.start_step; !rc && i < cp.end_step; ++i) {
     if (mode == ZSPH_COMPAT_FUSED) {
       rc = zsph_step(h, &o, &w, &t, s);
@@ -114,9 +182,11 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
       what = "step " + std::to_string(i) + ": " + last_error(h);
       break;
     }
+    ++metrics.steps;
     if (cp.output_step > 0 && i % cp.output_step == 0) {  // main.cu:95-124
       rc = zsph_writer_submit(wr, &o, &t, i, s);
       if (rc) what = "output: " + last_error(nullptr);
+      if (!rc && metrics.f) rc = metrics.line(h, o, i, n, st, what);
     }
     ++done;
   }
