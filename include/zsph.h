@@ -108,6 +108,26 @@ typedef struct zsph_handle zsph_handle_t;
 /* read_json (single_gpu_sph_src/io/read_json.cu:5-51): reads the 33
  * required keys; a missing or mistyped key is ZSPH_EIO with its name in err. */
 int zsph_read_json(const char* path, zsph_json_t* out, char* err, int errlen);
+/* Optional keys of the same case file, which the reference's read_json
+ * ignores (no counterpart in the reference; all may be absent):
+ *   "equations": "delta" (default) or "simple": the equation set, which the
+ *       reference picks when it is built (ZSPH_DELTA / ZSPH_SIMPLE,
+ *       deltasph/CMakeLists.txt:25-31);
+ *   "eos": "linear" (default): the equation of state of the reference's code,
+ *       p = c0^2 (rho - rho0) (lib/time_int.cu:39-40); any other value is
+ *       ZSPH_EINVAL, since no other one is implemented;
+ *   "snapshot_every": k >= 0: zsph_compat_run writes a snapshot of the state
+ *       after every k-th step as output_path/snapshot<s>.zsnap, s being the
+ *       number of the next step to run (0: none);
+ *   "resume": the path of such a snapshot: zsph_compat_run loads it after
+ *       the input and continues from its step.
+ * A mistyped or out-of-range value is ZSPH_EINVAL with its key in err. */
+typedef struct {
+  int equations;      /* ZSPH_EQ_DELTA or ZSPH_EQ_SIMPLE */
+  int snapshot_every; /* 0: no snapshots */
+  char resume[256];   /* empty: start from the input */
+} zsph_case_options_t;
+int zsph_read_case_options(const char* path, zsph_case_options_t* out, char* err, int errlen);
 
 /* set_cpu_param (single_gpu_sph_src/lib/init.cu:153-219), including the
  * check_dt call of init.cu:218: returns ZSPH_EINVAL when dt > dt_max

@@ -75,3 +75,14 @@ def test_an_unwritable_metrics_log_is_reported_before_any_step(tmp_path, monkeyp
     monkeypatch.setenv("ZSPH_METRICS", str(tmp_path / "no_such_dir" / "metrics.jsonl"))
     assert _run(path, z.COMPAT_FUSED) == (z.ZSPH_EIO, 0)
     assert "metrics log" in z.last_error()
+
+
+def test_bad_case_options_are_rejected_before_any_step(tmp_path):
+    path = _case_json_without_input(str(tmp_path))
+    with open(path) as f:
+        j = json.load(f)
+    j["eos"] = "tait"
+    with open(path, "w") as f:
+        json.dump(j, f)
+    assert _run(path, z.COMPAT_FUSED) == (z.ZSPH_EINVAL, 0)
+    assert "case options" in z.last_error() and "eos" in z.last_error()

@@ -194,3 +194,30 @@ def test_set_launch_shapes_rejects_a_null_handle_or_shapes():
     t = z.TuneResult(list_cells_per_cta=2, governing_min_ctas=1, steps_per_graph=1)
     assert z.lib.zsph_set_launch_shapes(None, ctypes.byref(t)) == z.ZSPH_EINVAL
     assert "null handle" in z.last_error()
+
+
+def test_case_options_defaults_and_values(tmp_path):
+    d = case_dict(cases.config0())
+    p = tmp_path / "input.json"
+    p.write_text(json.dumps(d))
+    o = z.read_case_options(str(p))
+    assert (o.equations, o.snapshot_every, o.resume) == (z.EQ_DELTA, 0, b"")
+    d.update(equations="simple", eos="linear", snapshot_every=100, resume="/runs/snapshot300.zsnap")
+    p.write_text(json.dumps(d))
+    o = z.read_case_options(str(p))
+    assert (o.equations, o.snapshot_every, o.resume) == (z.EQ_SIMPLE, 100, b"/runs/snapshot300.zsnap")
+    # the reference's keys still read as before next to the optional ones
+    assert z.read_json(str(p)).ptc_num == d["ptc_num"]
+
+
+@pytest.mark.parametrize("key,value", [("equations", "sph"), ("equations", 1), ("eos", "tait"),
+                                       ("snapshot_every", -1), ("snapshot_every", 2.5), ("resume", 3),
+                                       ("resume", "x" * 300)])
+def test_case_options_errors(tmp_path, key, value):
+    d = case_dict(cases.config0())
+    d[key] = value
+    p = tmp_path / "input.json"
+    p.write_text(json.dumps(d))
+    with pytest.raises(z.ZsphError) as e:
+        z.read_case_options(str(p))
+    assert e.value.code == z.ZSPH_EINVAL and key in str(e.value)

@@ -91,6 +91,11 @@ class JsonCase(ctypes.Structure):
                ("git_hash", ctypes.c_char * 64)]
 
 
+class CaseOptions(ctypes.Structure):
+    """zsph_case_options_t: the optional keys of a case file (no reference counterpart)."""
+    _fields_ = [("equations", _I), ("snapshot_every", _I), ("resume", ctypes.c_char * 256)]
+
+
 class CpuParam(ctypes.Structure):
     """zsph_cpu_param_t: the reference's cpu_param_t (data_structure.cuh:53-105)."""
     _fields_ = [(n, _F) for n in ("g", "m", "rho0", "dx", "h", "r", "eta", "cs", "adh", "delta", "alpha", "dt")] + \
@@ -173,6 +178,7 @@ _HP = ctypes.c_void_p
 _sig = {
     "zsph_read_json": (_I, [ctypes.c_char_p, ctypes.POINTER(JsonCase), ctypes.c_char_p, _I]),
     "zsph_compat_run": (_I, [ctypes.c_char_p, _I, _IP]),
+    "zsph_read_case_options": (_I, [ctypes.c_char_p, ctypes.POINTER(CaseOptions), ctypes.c_char_p, _I]),
     "zsph_set_cpu_param": (_I, [ctypes.POINTER(CpuParam), ctypes.POINTER(JsonCase)]),
     "zsph_set_gpu_param": (_I, [ctypes.POINTER(GpuParam), ctypes.POINTER(CpuParam)]),
     "zsph_check_dt": (_I, [ctypes.POINTER(CpuParam), _FP]),
@@ -364,6 +370,16 @@ def read_json(path: str) -> JsonCase:
     if rc != ZSPH_OK:
         raise ZsphError(rc, err.value.decode())
     return j
+
+
+def read_case_options(path: str) -> CaseOptions:
+    """zsph_read_case_options: the optional keys of a case file."""
+    o = CaseOptions()
+    err = ctypes.create_string_buffer(256)
+    rc = lib.zsph_read_case_options(path.encode(), ctypes.byref(o), err, len(err))
+    if rc != ZSPH_OK:
+        raise ZsphError(rc, err.value.decode(errors="replace"))
+    return o
 
 
 def params_from_json(j: JsonCase) -> tuple[CpuParam, GpuParam]:

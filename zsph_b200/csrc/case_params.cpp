@@ -238,6 +238,66 @@ extern "C" int zsph_read_json(const char* path, zsph_json_t* out, char* err, int
   }
 }
 
+namespace {
+
+int read_options_file(const char* path, zsph_case_options_t* out, char* err, int errlen) {
+  std::ifstream f(path);
+  if (!f) { set_err(err, errlen, std::string("cannot open ") + path); return ZSPH_EIO; }
+  std::stringstream ss;
+  ss << f.rdbuf();
+  const std::string text = ss.str();
+  std::map<std::string, JValue> kv;
+  std::string perr;
+  if (!JParser(text).parse(kv, perr)) { set_err(err, errlen, "JSON parse error: " + perr); return ZSPH_EIO; }
+  std::memset(out, 0, sizeof *out);
+  out->equations = ZSPH_EQ_DELTA;
+  auto bad = [&](const std::string& m) { set_err(err, errlen, m); return ZSPH_EINVAL; };
+  auto it = kv.find("equations");
+  if (it != kv.end()) {
+    if (it->second.kind != JValue::STR) return bad("key is not a string: equations");
+    if (it->second.str == "delta") out->equations = ZSPH_EQ_DELTA;
+    else if (it->second.str == "simple") out->equations = ZSPH_EQ_SIMPLE;
+    else return bad("equations must be \"delta\" or \"simple\", not \"" + it->second.str + "\"");
+  }
+  it = kv.find("eos");
+  if (it != kv.end()) {
+    if (it->second.kind != JValue::STR) return bad("key is not a string: eos");
+    if (it->second.str != "linear")
+      return bad("eos \"" + it->second.str + "\" is not implemented; the reference's code uses \"linear\"");
+  }
+  it = kv.find("snapshot_every");
+  if (it != kv.end()) {
+    const double v = it->second.num;
+    if (it->second.kind != JValue::NUM || !(v >= 0.0 && v < 2147483648.0) || v != (double)(long long)v)
+      return bad("snapshot_every must be a whole number >= 0");
+    out->snapshot_every = (int)v;
+  }
+  it = kv.find("resume");
+  if (it != kv.end()) {
+    if (it->second.kind != JValue::STR) return bad("key is not a string: resume");
+    if (it->second.str.size() >= sizeof out->resume) return bad("resume: path too long");
+    copy_str(out->resume, sizeof out->resume, it->second.str);
+  }
+  set_err(err, errlen, "");
+  return ZSPH_OK;
+}
+
+}  // namespace
+
+extern "C" int zsph_read_case_options(const char* path, zsph_case_options_t* out, char* err, int errlen) {
+  const zsph::TraceRange trace_range_(__func__);
+  if (!path || !out) { set_err(err, errlen, "null argument"); return ZSPH_EINVAL; }
+  try {
+    return read_options_file(path, out, err, errlen);
+  } catch (const std::exception& e) {
+    set_err(err, errlen, std::string("zsph_read_case_options: ") + e.what());
+    return ZSPH_EIO;
+  } catch (...) {
+    set_err(err, errlen, "zsph_read_case_options: unknown error");
+    return ZSPH_EIO;
+  }
+}
+
 extern "C" int zsph_check_dt(const zsph_cpu_param_t* param, float* dt_max_out) {
   if (!param) return ZSPH_EINVAL;
   // check.cu:6: 0.25 is a double literal; sqrt of a float argument.

@@ -100,13 +100,17 @@ struct MetricsLog {
 };
 
 int compat_run(const char* json_path, int mode, int* steps_done) {
-  const bool simple = (mode & ZSPH_COMPAT_SIMPLE) != 0;
+  bool simple = (mode & ZSPH_COMPAT_SIMPLE) != 0;
   mode &= ~ZSPH_COMPAT_SIMPLE;
   if (mode != ZSPH_COMPAT_SEPARATE && mode != ZSPH_COMPAT_FUSED) return fail(ZSPH_EINVAL, "unknown mode");
   zsph_json_t j;
   char err[256] = {0};
   int rc = zsph_read_json(json_path, &j, err, (int)sizeof err);
   if (rc) return fail(rc, std::string("read_json: ") + err);
+  zsph_case_options_t opt;
+  rc = zsph_read_case_options(json_path, &opt, err, (int)sizeof err);
+  if (rc) return fail(rc, std::string("case options: ") + err);
+  if (opt.equations == ZSPH_EQ_SIMPLE) simple = true;
   zsph_cpu_param_t cp;
   rc = zsph_set_cpu_param(&cp, &j);
   if (rc) return fail(rc, "set_cpu_param: " + last_error(nullptr));
@@ -147,6 +151,20 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
     rc = ZSPH_ECUDA;
     what = std::string("stream: ") + cudaGetErrorString(ce);
   }
+  int first = cp.start_step;
+  if (!rc && opt.resume[0]) {  // the state, cell bounds and step of a snapshot replace the input's
+    // the input's upload ran on the legacy stream: let it land before the snapshot overwrites it
+    if ((ce = cudaDeviceSynchronize()) != cudaSuccess) {
+      rc = ZSPH_ECUDA;
+      what = std::string("resume: ") + cudaGetErrorString(ce);
+    }
+    int step = 0;
+    if (!rc) {
+      rc = zsph_snapshot_load(opt.resume, &o, &t, n, cp.grid_num, &step, st);
+      if (rc) what = "resume: " + last_error(nullptr);
+      else first = step;
+    }
+  }
   if (!rc) {
     rc = zsph_create(&gp, cp.grid_num, &h);
     if (rc) what = "create: " + last_error(nullptr);
@@ -161,7 +179,7 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
   }
   void* s = st;
   metrics.start();
-  for (int i = cp.start_step; !rc && i < cp.end_step; ++i) {
+  for (int i = first; !rc && i < cp.end_step; ++i) {
     if (mode == ZSPH_COMPAT_FUSED) {
       rc = zsph_step(h, &o, &w, &t, s);
     } else {  // main.cu:63-88
@@ -187,6 +205,11 @@ int compat_run(const char* json_path, int mode, int* steps_done) {
       rc = zsph_writer_submit(wr, &o, &t, i, s);
       if (rc) what = "output: " + last_error(nullptr);
       if (!rc && metrics.f) rc = metrics.line(h, o, i, n, st, what);
+    }
+    if (!rc && opt.snapshot_every > 0 && (i + 1) % opt.snapshot_every == 0) {  // the state before step i + 1
+      const std::string snap = std::string(cp.output_path) + "/snapshot" + std::to_string(i + 1) + ".zsnap";
+      rc = zsph_snapshot_save(snap.c_str(), &o, &t, n, cp.grid_num, i + 1, st);
+      if (rc) what = "snapshot: " + last_error(nullptr);
     }
     ++done;
   }
