@@ -74,51 +74,3 @@ def test_compat_run_reports_a_missing_input(tmp_path):
     os.remove(os.path.join(str(tmp_path), "input", "input.vtk"))
     with pytest.raises(z.ZsphError):
         z.compat_run(path)
-
-
-def test_compat_run_metrics_log(tmp_path, monkeypatch):
-    # ZSPH_METRICS: one JSON line per output step with the steps since the
-    # previous line, their wall time and the FP64 conservation sums
-    c = cases.small(0.04)
-    path, out = _write_case(str(tmp_path), c, 12, 5)
-    log = tmp_path / "metrics.jsonl"
-    monkeypatch.setenv("ZSPH_METRICS", str(log))
-    assert z.compat_run(path, z.COMPAT_FUSED) == 12
-    lines = [json.loads(l) for l in log.read_text().splitlines()]
-    assert [l["step"] for l in lines] == [0, 5, 10]
-    assert [l["steps"] for l in lines] == [1, 5, 5]
-    assert all(l["seconds"] > 0 and l["particle_steps_per_s"] > 0 and (l["flags"] & z.FLAG_NAN) == 0 for l in lines)
-    mass = c.n_fluid * float(c.json.rho0) * float(c.json.dx) ** 3
-    assert all(abs(l["mass"] - mass) < 1e-6 * mass for l in lines)  # no fluid particle leaves the tank
-    assert sorted(os.listdir(out)) == sorted(f"zsph{i}.vtk" for i in (0, 5, 10))
-
-
-@pytest.mark.parametrize("mode", [z.COMPAT_SEPARATE, z.COMPAT_FUSED])
-def test_compat_run_resumes_from_its_snapshot(tmp_path, mode):
-    # "snapshot_every": 6 writes output/snapshot6.zsnap (the state before step
-    # 6); a second run with "resume" pointing at it runs steps 6..11 and writes
-    # the same zsph10.vtk, byte for byte, as the run that never stopped
-    c = cases.small(0.04)
-    full = tmp_path / "full"
-    full.mkdir()
-    path, out = _write_case(str(full), c, 12, 5)
-    with open(path) as f:
-        j = json.load(f)
-    j["snapshot_every"] = 6
-    with open(path, "w") as f:
-        json.dump(j, f)
-    assert z.compat_run(path, mode) == 12
-    assert sorted(n for n in os.listdir(out) if n.endswith(".zsnap")) == ["snapshot12.zsnap", "snapshot6.zsnap"]
-    part = tmp_path / "resumed"
-    part.mkdir()
-    path2, out2 = _write_case(str(part), c, 12, 5)
-    with open(path2) as f:
-        j2 = json.load(f)
-    j2["resume"] = os.path.join(out, "snapshot6.zsnap")
-    with open(path2, "w") as f:
-        json.dump(j2, f)
-    assert z.compat_run(path2, mode) == 6
-    assert sorted(os.listdir(out2)) == ["zsph10.vtk"]
-    a = open(os.path.join(out, "zsph10.vtk"), "rb").read()
-    b = open(os.path.join(out2, "zsph10.vtk"), "rb").read()
-    assert a == b
