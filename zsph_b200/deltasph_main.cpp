@@ -4,7 +4,10 @@
 // initial particles are read from <input_path>/input.vtk and the outputs go to
 // <output_path>/zsph<step>.vtk.  --fused runs one fused step per step instead
 // of the reference's twelve launches; --simple runs the simple-SPH equations
-// (the reference's simplesph program).
+// (the reference's simplesph program).  Optional case-file keys beyond the
+// reference's: "equations", "eos", "snapshot_every" (snapshots of the state in
+// output_path) and "resume" (continue from such a snapshot); the environment
+// variable ZSPH_METRICS names a JSONL run log (see zsph_compat_run).
 #include <cstdio>
 #include <cstring>
 
