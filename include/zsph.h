@@ -364,8 +364,8 @@ int zsph_snapshot_load_host(const char* path, const zsph_ptc_t* ptc, const zsph_
  * prints per-step timings to stdout, main.cu:60-95): step, steps and wall
  * seconds since the previous line (the stream synchronised), particle-steps/s,
  * the device status bits and the FP64 conservation sums of the state
- * (zsph_conservation); a file that cannot be opened is ZSPH_EIO before any
- * step. */
+ * (zsph_conservation).  The file is rewritten at the start of each run; one
+ * that cannot be opened is ZSPH_EIO before any step. */
 enum { ZSPH_COMPAT_SEPARATE = 0, ZSPH_COMPAT_FUSED = 1, ZSPH_COMPAT_SIMPLE = 2 };
 int zsph_compat_run(const char* json_path, int mode, int* steps_done);
 
