@@ -21,6 +21,7 @@ int main(int argc, char** argv) {
   printf("sizeof zsph_tune_t %zu\n", sizeof(zsph_tune_t));
   printf("sizeof zsph_conservation_t %zu\n", sizeof(zsph_conservation_t));
   printf("sizeof zsph_rigid_t %zu\n", sizeof(zsph_rigid_t));
+  printf("sizeof zsph_case_options_t %zu\n", sizeof(zsph_case_options_t));
   if (argc < 2) return 0;
   zsph_json_t j;
   zsph_cpu_param_t cp;

@@ -20,7 +20,7 @@ MIRRORS = {
     "zsph_json_t": z.JsonCase, "zsph_cpu_param_t": z.CpuParam, "zsph_gpu_param_t": z.GpuParam,
     "zsph_ptc_t": z.Ptc, "zsph_tmp_t": z.Tmp, "zsph_learn_train_stats_t": z.LearnTrainStats,
     "zsph_learn_run_stats_t": z.LearnRunStats, "zsph_tune_t": z.TuneResult,
-    "zsph_conservation_t": z.Conservation, "zsph_rigid_t": z.RigidBody,
+    "zsph_conservation_t": z.Conservation, "zsph_rigid_t": z.RigidBody, "zsph_case_options_t": z.CaseOptions,
 }
 
 
